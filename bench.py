@@ -1,0 +1,317 @@
+"""Benchmark: RK-stage DOF-updates/s of the explicit DG step.
+
+Workload (one GPU): Navier-Stokes Taylor-Green vortex, periodic [0, 2 pi]^3,
+32^3 hexes, p = 3 (64 DOF per element per variable), Re 1600, Ma 0.1, BR2
+viscous terms, RK4 with dt = 0.2 h / ((2p+1)(c + |u|max)), FP64.  Synthetic
+initial data (the analytic TGV field), no dataset.  A "step" is one RK4 time
+step = 4 RK stages; DOF-updates per stage = 5 * 64 * 32^3.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Our arm: the state stays resident in HBM; `value` is device time (CUDA events
+on the handle's stream, max over ranks) of K graph-launched steps; `e2e` is the
+same metric through the C ABI with host buffers (pinned H2D of the state, the
+step, D2H of the state and the residual norm, every step).  Multi-GPU runs
+are independent replicas (weak scaling): the reference's multi-rank mode is a
+domain decomposition this build does not implement.
+
+--impl reference: the reference's own FP64 CPU solver (compiled in place into
+oracle/_ref/) on the host cores, one process per core, each step a bounded
+sample of the same workload (an 8^3 block of the 32^3 TGV mesh; identical
+per-element work), DOF-updates/s summed over processes.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "RK-stage DOF-updates/s (FP64, TGV 32^3 p=3 RK4)"
+UNIT = "DOF-updates/s"
+N_EL = 32
+P_ORD = 3
+L_BOX = 2 * math.pi
+
+
+def tgv_case(n, p):
+    from tests import cases as C
+    nodes = C.box_nodes(n, n, n, 1, L_BOX, L_BOX, L_BOX)
+    prm = C.params(mu=1.0 / 1600.0, c=10.0, u=0.0, v=0.0, w=0.0)
+    U = C.taylor_green(C.node_coords(n, n, n, p, 1, nodes)).reshape(-1)
+    dt = 0.2 * (L_BOX / n) / ((2 * p + 1) * (10.0 + 1.0))
+    return nodes, prm, U, dt
+
+
+def config(extra=None):
+    c = {"workload": "Taylor-Green vortex Re=1600 Ma=0.1, periodic [0,2pi]^3, 32^3 hexes, p=3, BR2, RK4, FP64",
+         "nelem": N_EL ** 3, "p": P_ORD, "dof_per_stage": 5 * (P_ORD + 1) ** 3 * N_EL ** 3,
+         "scheme": "RK4", "l2_between_steps": "inputs larger than L2 (trace buffer 252 MB + 3 state arrays 84 MB each)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------- reference arm
+
+def _ref_worker(args):
+    """One process: the reference solver on an 8^3 block of the TGV mesh."""
+    nsteps, n = args
+    import oracle
+    ref = oracle.reference()
+    nodes, prm, U, dt = tgv_case(n, P_ORD)
+    m = oracle.Mesh(n, n, n, P_ORD, 1, nodes, [-2] * 6)
+    t0 = time.perf_counter()
+    ref.run(m, prm, U, 0, dt, 0)          # geometry precompute only
+    t1 = time.perf_counter()
+    ref.run(m, prm, U, 0, dt, nsteps)     # precompute + nsteps RK4 steps
+    t2 = time.perf_counter()
+    stage_s = max((t2 - t1) - (t1 - t0), 1e-9) / (4 * nsteps)
+    return stage_s
+
+
+def cpu_rate(nsteps, n, procs):
+    """DOF-updates/s of `procs` concurrent reference processes."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        stage_s = pool.map(_ref_worker, [(nsteps, n)] * procs)
+    dof = 5 * (P_ORD + 1) ** 3 * n ** 3
+    return sum(dof / s for s in stage_s), stage_s
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    if oracle.reference() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdgref.so was not built "
+                          "(the reference tree is needed to compile it)"}))
+        return
+    procs = os.cpu_count() or 1
+    n = 8
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, _ = cpu_rate(1, n, procs)
+        if i >= args.warmup:
+            rates.append(r)
+    value = float(np.median(rates))
+    stage_ms = 5 * (P_ORD + 1) ** 3 * N_EL ** 3 / value * 1e3
+    sample = (f"{procs} concurrent single-rank reference processes, each 1 RK4 step of an {n}^3 block "
+              f"(periodic, same p, same per-element work) of the 32^3 TGV; stage time = (wall with the step "
+              f"- wall of geometry setup alone) / 4")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 4 * stage_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config({"sample_block": f"{n}^3"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ------------------------------------------------------------------ our arm
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join("/tmp", f"dgb_clocks_{os.getpid()}_{gpu}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import dgpr_b200 as dg
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    nodes, prm, U0, dt = tgv_case(N_EL, P_ORD)
+    mesh = dg.Mesh(N_EL, N_EL, N_EL, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
+    s = dg.Solver(mesh, dg.Params.from_array(prm))
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.set_state(U0)
+    dof_stage = 5 * (P_ORD + 1) ** 3 * N_EL ** 3
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (also builds the graph)
+    for _ in range(args.warmup):
+        s.step(dg.RK4, dt, 1, norms=False)
+    torch.cuda.synchronize()
+
+    # ---- device-timed: K graph-launched steps, state resident
+    clk = Clocks(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        s.step(dg.RK4, dt, args.steps, norms=True)
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = s.last_launch_count
+    value = world * dof_stage * 4 * args.steps / (ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers
+    Uh = torch.empty(U0.size, dtype=torch.float64).pin_memory()
+    Uh.numpy()[:] = U0
+    Uhost = Uh.numpy()
+    norms_h = torch.empty(1, dtype=torch.float64).pin_memory().numpy()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.set_state(Uhost)
+        dg._check(dg.lib().dgb_step(s.h, dg.RK4, dt, 1, dg._p(norms_h)))
+        dg._check(dg.lib().dgb_get_state(s.h, dg._p(Uhost)))
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * dof_stage * 4 * args.steps / e2e_s
+
+    # ---- per-kernel durations for the roofline (events between launches)
+    s.set_state(U0)
+    kms = s.profile_step(dg.RK4, dt, max(3, min(args.steps, 10)))
+    # launch order per RK4 step: trace0 stage0 norm trace1 stage1 trace2 stage2 trace3 stage3
+    stage_ms = float(np.mean([kms[1], kms[4], kms[6], kms[8]]))
+    trace_ms = float(np.mean([kms[0], kms[3], kms[5], kms[7]]))
+    nb = (P_ORD + 1) ** 3
+    alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    s.close()
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            import oracle
+            if oracle.reference() is not None:
+                procs = os.cpu_count() or 1
+                rate, _ = cpu_rate(1, 8, procs)
+                cpu = {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
+                       "sample": f"{procs} concurrent reference processes, each 1 RK4 step on an 8^3 block "
+                                 f"of the TGV mesh (same per-element work)"}
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get("stage_kernel_bytes_per_launch")
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": U0.size * 8,
+                    "d2h_bytes_per_step": U0.size * 8 + 8},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "stage_kernel<4>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
+                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
+                         if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+            "clocks": clocks,
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    globals()["N_EL"] = args.nel
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

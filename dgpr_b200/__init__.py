@@ -1,0 +1,298 @@
+"""dgpr_b200: Python harness over the dgb200 C ABI (include/dgb200.h).
+
+The product is the native library dgpr_b200/_lib/libdgb200.so (C++ host code
+plus sm_100a CUDA kernels).  This module only binds it with ctypes so tests,
+the benchmark and users in Python can drive it; there is no Python or CPU
+compute path.  Importing fails loudly if the library has not been built
+(`python -m dgpr_b200.build` or `__graft_entry__.build()`).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libdgb200.so")
+
+OK, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_GEOMETRY, ERR_NONFINITE, ERR_IO, ERR_BOUNDARY = range(8)
+INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW, NO_SLIP_WALL = \
+    -1, -2, -3, -4, -5, -6, -7
+RK4, TVDRK3 = 0, 1
+FP64, MIXED_FP32 = 0, 1
+
+BOUNDARY_TYPES = {  # the reference's boundary_types map (boundaries.cpp:37-44)
+    "periodic": PERIODIC, "freestream": FREESTREAM, "inviscid_wall": INVISCID_WALL,
+    "subsonic_inflow": SUBSONIC_INFLOW, "subsonic_outflow": SUBSONIC_OUTFLOW, "no_slip_wall": NO_SLIP_WALL,
+}
+TIME_SCHEMES = {"RK4": RK4, "tvdRK3": TVDRK3}  # multistage_schemes (time.cpp:29-31)
+
+
+class DgbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dgb200 error {code}: {msg}")
+        self.code = code
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("p", ctypes.c_int),
+                ("q", ctypes.c_int), ("nodes", _dp), ("bounds", ctypes.c_longlong * 6)]
+
+
+class Params(ctypes.Structure):
+    """The reference's `parameters` struct (solver_params.cpp:22-36)."""
+    _fields_ = [("gamma", ctypes.c_double), ("R", ctypes.c_double), ("mu", ctypes.c_double),
+                ("c", ctypes.c_double), ("T", ctypes.c_double), ("P", ctypes.c_double),
+                ("Ufr", ctypes.c_double * 5), ("source", ctypes.c_double * 5), ("eta", ctypes.c_double)]
+
+    def as_array(self):
+        """17-vector [gamma R mu c T P Ufr(5) source(5) eta]."""
+        return np.array([self.gamma, self.R, self.mu, self.c, self.T, self.P, *self.Ufr, *self.source, self.eta])
+
+    @classmethod
+    def from_array(cls, a):
+        a = [float(v) for v in a]
+        p = cls()
+        p.gamma, p.R, p.mu, p.c, p.T, p.P = a[:6]
+        for i in range(5):
+            p.Ufr[i] = a[6 + i]
+            p.source[i] = a[11 + i]
+        p.eta = a[16]
+        return p
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m dgpr_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        sig = {
+            "dgb_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+            "dgb_last_error_message": (ctypes.c_char_p, []),
+            "dgb_create": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(Params), ctypes.c_int,
+                                          ctypes.POINTER(vp)]),
+            "dgb_destroy": (ctypes.c_int, [vp]),
+            "dgb_set_stream": (ctypes.c_int, [vp, vp]),
+            "dgb_state_size": (ctypes.c_longlong, [vp]),
+            "dgb_set_state": (ctypes.c_int, [vp, _dp]),
+            "dgb_get_state": (ctypes.c_int, [vp, _dp]),
+            "dgb_state_device_ptr": (ctypes.c_int, [vp, ctypes.POINTER(vp)]),
+            "dgb_residual": (ctypes.c_int, [vp, _dp, _dp, _dp]),
+            "dgb_residual_device": (ctypes.c_int, [vp, vp, vp, vp]),
+            "dgb_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp]),
+            "dgb_last_launch_count": (ctypes.c_longlong, [vp]),
+            "dgb_profile_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
+                                                ctypes.POINTER(ctypes.c_int)]),
+            "dgb_gauss_legendre": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
+            "dgb_lagrange1d": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+            "dgb_lagrange1d_deriv": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+            "dgb_bump_nodes": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.c_double] * 7 + [_dp]),
+            "dgb_make_reference_state": (ctypes.c_int, [ctypes.c_double] * 9 + [_dp, ctypes.POINTER(Params)]),
+            "dgb_write_state": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_ulonglong, ctypes.POINTER(MeshDesc),
+                                               ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                               ctypes.POINTER(_dp)]),
+            "dgb_read_state": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_ulonglong)]
+                               + [ctypes.POINTER(ctypes.c_int)] * 5
+                               + [ctypes.POINTER(ctypes.c_longlong), _dp, ctypes.c_char_p, _dp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        msg = lib().dgb_last_error_message().decode(errors="replace")
+        raise DgbError(rc, f"{lib().dgb_error_string(rc).decode()}: {msg}")
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+# ----------------------------------------------------------------- setup helpers
+
+def make_reference_state(gamma=1.4, gcnst=287.0, mu=1e-3, c=1.0, rho=1.0, u=0.1, v=0.0, w=0.0, eta=6.0,
+                         source=(0.0, 0.0, 0.0, 0.0, 0.0)):
+    """make_reference_state (solver_params.cpp:40-70); defaults are the
+    reference's solver_inputs defaults (input.cpp:46-65)."""
+    out = Params()
+    src = np.ascontiguousarray(source, dtype=np.float64)
+    _check(lib().dgb_make_reference_state(gamma, gcnst, mu, c, rho, u, v, w, eta, _p(src), ctypes.byref(out)))
+    return out
+
+
+def gauss_legendre(n, a=0.0, b=1.0):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    _check(lib().dgb_gauss_legendre(n, a, b, _p(x), _p(w)))
+    return x, w
+
+
+def lagrange1d(i, p, x):
+    return lib().dgb_lagrange1d(i, p, x)
+
+
+def lagrange1d_deriv(i, p, x):
+    return lib().dgb_lagrange1d_deriv(i, p, x)
+
+
+def bump_nodes(nx, ny, nz, q, lx=2.0, ly=1.0, lz=1.0, a=0.0, bmp_height=0.1, bmp_center=1.0, bmp_variance=0.05):
+    """generate_bump_nodes (geometry_common.cpp:494-576); defaults from input.cpp:23-38."""
+    nodes = np.zeros(nx * ny * nz * (q + 1) ** 3 * 3)
+    _check(lib().dgb_bump_nodes(nx, ny, nz, q, lx, ly, lz, a, bmp_height, bmp_center, bmp_variance, _p(nodes)))
+    return nodes
+
+
+def box_nodes(nx, ny, nz, q, lx, ly, lz):
+    return bump_nodes(nx, ny, nz, q, lx, ly, lz, 0.0, 0.0, 1.0, 1.0)
+
+
+class Mesh:
+    def __init__(self, nx, ny, nz, p, q, nodes, bounds):
+        self.nx, self.ny, self.nz, self.p, self.q = int(nx), int(ny), int(nz), int(p), int(q)
+        self.nodes = np.ascontiguousarray(nodes, dtype=np.float64).ravel()
+        self.bounds = [int(b) for b in bounds]
+        if self.nodes.size != self.nelem * (self.q + 1) ** 3 * 3 or len(self.bounds) != 6:
+            raise ValueError("mesh nodes / bounds have the wrong size")
+
+    @property
+    def nelem(self):
+        return self.nx * self.ny * self.nz
+
+    @property
+    def nb(self):
+        return (self.p + 1) ** 3
+
+    @property
+    def state_size(self):
+        return self.nelem * 5 * self.nb
+
+    def desc(self):
+        d = MeshDesc()
+        d.nx, d.ny, d.nz, d.p, d.q = self.nx, self.ny, self.nz, self.p, self.q
+        d.nodes = _p(self.nodes)
+        for i, b in enumerate(self.bounds):
+            d.bounds[i] = b
+        return d
+
+
+def write_state(fname, tstep, mesh, outputs):
+    """.dg writer (io.cpp:33-90); outputs: dict key -> state array."""
+    keys = list(outputs.keys())
+    arrs = [np.ascontiguousarray(outputs[k], dtype=np.float64).ravel() for k in keys]
+    karr = (ctypes.c_char_p * len(keys))(*[k.encode() for k in keys])
+    darr = (_dp * len(keys))(*[_p(a) for a in arrs])
+    d = mesh.desc()
+    _check(lib().dgb_write_state(os.fsencode(fname), tstep, ctypes.byref(d), len(keys), karr, darr))
+
+
+def read_state(fname, key="state"):
+    """.dg reader (io.cpp:92-159): returns (tstep, Mesh, state array or None)."""
+    t = ctypes.c_ulonglong()
+    ints = [ctypes.c_int() for _ in range(5)]
+    b = (ctypes.c_longlong * 6)()
+    _check(lib().dgb_read_state(os.fsencode(fname), ctypes.byref(t), *[ctypes.byref(i) for i in ints], b,
+                                None, None, None))
+    nx, ny, nz, p, q = [i.value for i in ints]
+    nodes = np.zeros(nx * ny * nz * (q + 1) ** 3 * 3)
+    data = np.zeros(nx * ny * nz * 5 * (p + 1) ** 3)
+    _check(lib().dgb_read_state(os.fsencode(fname), None, None, None, None, None, None, None, _p(nodes),
+                                key.encode() if key else None, _p(data) if key else None))
+    return t.value, Mesh(nx, ny, nz, p, q, nodes, list(b)), (data if key else None)
+
+
+# ----------------------------------------------------------------------- solver
+
+class Solver:
+    """One device-resident mesh + state (dgb_create .. dgb_destroy).
+
+    Mirrors the reference's GPU driver objects: the constructor plays
+    cuda_device_geometry + cuda_residual_workspace (solve_cuda.cu:171,303),
+    `residual` plays cuda_residual (solve_cuda.cu:1235) and `step` plays
+    RK4_cuda / tvdRK3_cuda (time_cuda.cu:126-185)."""
+
+    def __init__(self, mesh, params, precision=FP64):
+        self.mesh = mesh
+        self.params = params if isinstance(params, Params) else Params.from_array(params)
+        self._desc = mesh.desc()
+        h = ctypes.c_void_p()
+        _check(lib().dgb_create(ctypes.byref(self._desc), ctypes.byref(self.params), precision, ctypes.byref(h)))
+        self.h = h
+        self.n = lib().dgb_state_size(h)
+
+    def close(self):
+        if self.h:
+            lib().dgb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).ravel()
+        assert U.size == self.n
+        _check(lib().dgb_set_state(self.h, _p(U)))
+
+    def get_state(self):
+        U = np.zeros(self.n)
+        _check(lib().dgb_get_state(self.h, _p(U)))
+        return U
+
+    def residual(self, U):
+        """(R, f) for host state U, f = -Minv R."""
+        U = np.ascontiguousarray(U, dtype=np.float64).ravel()
+        R = np.zeros(self.n)
+        f = np.zeros(self.n)
+        _check(lib().dgb_residual(self.h, _p(U), _p(R), _p(f)))
+        return R, f
+
+    def residual_device(self, U_ptr, R_ptr, f_ptr):
+        """Device pointers (ints, e.g. torch tensor.data_ptr()); asynchronous."""
+        _check(lib().dgb_residual_device(self.h, ctypes.c_void_p(U_ptr), ctypes.c_void_p(R_ptr or 0),
+                                         ctypes.c_void_p(f_ptr)))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().dgb_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def state_device_ptr(self):
+        p = ctypes.c_void_p()
+        _check(lib().dgb_state_device_ptr(self.h, ctypes.byref(p)))
+        return p.value
+
+    def step(self, scheme, dt, nsteps, norms=True):
+        out = np.zeros(max(int(nsteps), 1))
+        _check(lib().dgb_step(self.h, int(scheme), float(dt), int(nsteps), _p(out) if norms else None))
+        return out[:nsteps]
+
+    def profile_step(self, scheme, dt, reps):
+        """Mean per-launch durations (ms) of one RK step, CUDA events on the
+        handle's stream, launch order: per stage trace, stage (+ norm after
+        the first stage)."""
+        out = np.zeros(64)
+        nk = ctypes.c_int(64)
+        _check(lib().dgb_profile_step(self.h, int(scheme), float(dt), int(reps), _p(out), ctypes.byref(nk)))
+        return out[:nk.value]
+
+    @property
+    def last_launch_count(self):
+        return lib().dgb_last_launch_count(self.h)

@@ -1,0 +1,529 @@
+// C ABI (include/dgb200.h): handle life cycle, state transfer, residual,
+// CUDA-graph RK stepping, and the host-only helpers.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dgb200.h"
+#include "host.hpp"
+#include "kernels.hpp"
+#include "mixed.hpp"
+
+using namespace dgb;
+
+struct dgb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int nx = 0, ny = 0, nz = 0, p = 0, q = 0, P = 0, NB = 0, NQF = 0;
+  long E = 0;
+  long long n = 0;  // doubles per state array
+  long long bounds[6] = {0, 0, 0, 0, 0, 0};
+  int precision = DGB_FP64;
+  dgb_params prm{};
+  DevParams dprm{};
+  Ops1D ops;
+  double* d_ops = nullptr;
+  double* d_geo = nullptr;
+  int* d_nbr = nullptr;
+  double* d_U = nullptr;      // resident state
+  double* d_Us = nullptr;     // stage state
+  double* d_acc = nullptr;    // RK4 accumulator
+  double* d_trace = nullptr;  // face traces
+  double* d_in = nullptr;     // residual API input / output
+  double* d_f = nullptr;
+  double* d_R = nullptr;
+  double* d_part = nullptr;
+  double* d_norms = nullptr;
+  int* d_counter = nullptr;
+  int* d_flag = nullptr;
+  unsigned long long norms_cap = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_scheme = -1;
+  double graph_dt = 0.;
+  long long launches_per_step = 0;
+  long long last_launches = 0;
+  MixedState* mixed = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return DGB_ERR_CUDA;
+}
+
+#define CK(call)                                 \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+Fp64Launch fp64_launch(const dgb_handle* h)
+{
+  Fp64Launch L;
+  L.P = h->P;
+  L.E = h->E;
+  L.ops = h->d_ops;
+  L.geo = h->d_geo;
+  L.nbr = h->d_nbr;
+  L.trace = h->d_trace;
+  L.prm = h->dprm;
+  return L;
+}
+
+StageArgs stage_args(int mode, double dt)
+{
+  StageArgs a;
+  memset(&a, 0, sizeof a);
+  a.mode = mode;
+  a.dt = dt;
+  return a;
+}
+
+// one residual of Uin (device) into f / R (device), on the handle's stream
+int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
+{
+  if (h->precision == DGB_MIXED_FP32) return mixed_residual(h->mixed, Uin, R, f, h->stream);
+  const Fp64Launch L = fp64_launch(h);
+  CK(launch_trace(L, Uin, h->stream));
+  StageArgs a = stage_args(MODE_RESIDUAL, 0.);
+  a.fout = f;
+  a.Rout = R;
+  a.flag = h->d_flag;
+  CK(launch_stage(L, Uin, a, h->stream));
+  return DGB_OK;
+}
+
+// one full RK step as a launch sequence (captured into a graph by dgb_step).
+// With ev != null, ev[i] is recorded before launch i and ev[nlaunch] after the
+// last one (per-kernel timing by dgb_profile_step).
+int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr)
+{
+  if (h->precision == DGB_MIXED_FP32)
+    return mixed_step(h->mixed, scheme, dt, h->d_U, h->d_Us, h->d_acc, h->d_part, h->d_norms,
+                      h->d_counter, h->d_flag, h->stream, ev);
+  const Fp64Launch L = fp64_launch(h);
+  const int nst = scheme == DGB_RK4 ? 4 : 3;
+  const int modes4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
+  const int modes3[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
+  int k = 0;
+  for (int s = 0; s < nst; ++s) {
+    const double* in = s == 0 ? h->d_U : h->d_Us;
+    if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+    CK(launch_trace(L, in, h->stream));
+    StageArgs a = stage_args(scheme == DGB_RK4 ? modes4[s] : modes3[s], dt);
+    a.Ubase = h->d_U;
+    a.acc = h->d_acc;
+    a.Uout = s == nst - 1 ? h->d_U : h->d_Us;
+    a.part = s == 0 ? h->d_part : nullptr;
+    a.flag = h->d_flag;
+    if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+    CK(launch_stage(L, in, a, h->stream));
+    if (s == 0) {
+      if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+      CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, h->d_counter, h->d_flag,
+                     h->stream));
+    }
+  }
+  if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+  return DGB_OK;
+}
+
+long long launches_per_step(const dgb_handle* h, int scheme)
+{
+  const int nst = scheme == DGB_RK4 ? 4 : 3;
+  return h->precision == DGB_MIXED_FP32 ? mixed_launches_per_step(h->mixed, nst) : 2 * nst + 1;
+}
+
+void free_all(dgb_handle* h)
+{
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  void* ptrs[] = {h->d_ops, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace, h->d_in,
+                  h->d_f, h->d_R, h->d_part, h->d_norms, h->d_counter, h->d_flag};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->mixed) mixed_destroy(h->mixed);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dgb_error_string(int status)
+{
+  switch (status) {
+    case DGB_OK: return "ok";
+    case DGB_ERR_ARG: return "invalid argument";
+    case DGB_ERR_UNSUPPORTED: return "unsupported input";
+    case DGB_ERR_CUDA: return "CUDA error";
+    case DGB_ERR_GEOMETRY: return "invalid geometry";
+    case DGB_ERR_NONFINITE: return "non-finite residual";
+    case DGB_ERR_IO: return "i/o error";
+    case DGB_ERR_BOUNDARY: return "no subsonic inflow boundary Mach root";
+  }
+  return "unknown status";
+}
+
+const char* dgb_last_error_message(void) { return g_err.c_str(); }
+
+int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precision, dgb_handle** out)
+{
+  if (!mesh || !params || !out) return fail(DGB_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (precision != DGB_FP64 && precision != DGB_MIXED_FP32) return fail(DGB_ERR_ARG, "unknown precision");
+  dgb_handle* h = new dgb_handle();
+  h->nx = mesh->nx;
+  h->ny = mesh->ny;
+  h->nz = mesh->nz;
+  h->p = mesh->p;
+  h->q = mesh->q;
+  h->precision = precision;
+  h->prm = *params;
+  for (int i = 0; i < 6; ++i) h->bounds[i] = mesh->bounds[i];
+  int rc = build_ops(mesh->p, h->ops);
+  if (rc) {
+    delete h;
+    return fail(rc, "solution order outside 0..6");
+  }
+  h->P = h->ops.P;
+  h->NB = h->P * h->P * h->P;
+  h->NQF = h->P * h->P;
+  h->E = (long)mesh->nx * mesh->ny * mesh->nz;
+  h->n = (long long)h->E * 5 * h->NB;
+  std::vector<double> geo;
+  std::vector<int32_t> nbr;
+  std::string why;
+  rc = build_geometry(*mesh, h->ops, geo, nbr, why);
+  if (rc) {
+    delete h;
+    return fail(rc, why);
+  }
+  h->dprm.gamma = params->gamma;
+  h->dprm.R = params->R;
+  h->dprm.mu = params->mu;
+  h->dprm.P = params->P;
+  h->dprm.eta = params->eta;
+  total_conditions(*params, &h->dprm.Tt, &h->dprm.Pt);
+  for (int r = 0; r < 5; ++r) {
+    h->dprm.Ufr[r] = params->Ufr[r];
+    h->dprm.src[r] = params->source[r];
+  }
+
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e != cudaSuccess) {
+    delete h;
+    return cuda_fail(e, "cudaGetDevice");
+  }
+#define CKF(call)                        \
+  do {                                   \
+    cudaError_t e_ = (call);             \
+    if (e_ != cudaSuccess) {             \
+      int rc_ = cuda_fail(e_, #call);    \
+      free_all(h);                       \
+      delete h;                          \
+      return rc_;                        \
+    }                                    \
+  } while (0)
+  CKF(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->own_stream = true;
+  std::vector<double> table(ops_table_size(h->P));
+  pack_ops(h->ops, table.data());
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  CKF(cudaMalloc(&h->d_ops, sizeof(double) * table.size()));
+  CKF(cudaMalloc(&h->d_geo, sizeof(double) * geo.size()));
+  CKF(cudaMalloc(&h->d_nbr, sizeof(int) * nbr.size()));
+  CKF(cudaMalloc(&h->d_U, sb));
+  CKF(cudaMalloc(&h->d_Us, sb));
+  CKF(cudaMalloc(&h->d_acc, sb));
+  CKF(cudaMalloc(&h->d_trace, sizeof(double) * (size_t)h->E * 60 * h->NQF));
+  CKF(cudaMalloc(&h->d_part, sizeof(double) * (size_t)h->E));
+  CKF(cudaMalloc(&h->d_counter, sizeof(int)));
+  CKF(cudaMalloc(&h->d_flag, sizeof(int)));
+  CKF(cudaMemcpy(h->d_ops, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(h->d_geo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice));
+  CKF(cudaMemcpy(h->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
+  CKF(cudaMemset(h->d_U, 0, sb));
+  CKF(cudaMemset(h->d_counter, 0, sizeof(int)));
+  CKF(cudaMemset(h->d_flag, 0, sizeof(int)));
+  if (precision == DGB_MIXED_FP32) {
+    rc = mixed_create(&h->mixed, h->ops, geo, h->d_geo, h->d_nbr, h->E, h->dprm);
+    if (rc) {
+      free_all(h);
+      delete h;
+      return fail(rc, "mixed-precision setup failed");
+    }
+  } else {
+    CKF(prepare_fp64_kernels(h->P));
+  }
+#undef CKF
+  *out = h;
+  return DGB_OK;
+}
+
+int dgb_destroy(dgb_handle* h)
+{
+  if (!h) return DGB_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return DGB_OK;
+}
+
+int dgb_set_stream(dgb_handle* h, void* stream)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (h->own_stream && h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  h->own_stream = false;
+  h->stream = (cudaStream_t)stream;
+  if (!h->stream) {  // graphs need a capturable stream: make our own
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_scheme = -1;
+  }
+  return DGB_OK;
+}
+
+long long dgb_state_size(const dgb_handle* h) { return h ? h->n : -1; }
+
+long long dgb_last_launch_count(const dgb_handle* h) { return h ? h->last_launches : -1; }
+
+int dgb_set_state(dgb_handle* h, const double* U_host)
+{
+  if (!h || !U_host) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->d_U, U_host, sizeof(double) * (size_t)h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_get_state(dgb_handle* h, double* U_host)
+{
+  if (!h || !U_host) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(U_host, h->d_U, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_state_device_ptr(dgb_handle* h, double** U_dev)
+{
+  if (!h || !U_dev) return fail(DGB_ERR_ARG, "null argument");
+  *U_dev = h->d_U;
+  return DGB_OK;
+}
+
+int dgb_residual_device(dgb_handle* h, const double* U_dev, double* R_dev, double* f_dev)
+{
+  if (!h || !U_dev || !f_dev) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  int rc = enqueue_residual(h, U_dev, R_dev, f_dev);
+  h->last_launches = 2;
+  return rc;
+}
+
+int dgb_residual(dgb_handle* h, const double* U_host, double* R_host, double* f_host)
+{
+  if (!h || !U_host || !f_host) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  if (!h->d_in) {
+    CK(cudaMalloc(&h->d_in, sb));
+    CK(cudaMalloc(&h->d_f, sb));
+    CK(cudaMalloc(&h->d_R, sb));
+  }
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  CK(cudaMemcpyAsync(h->d_in, U_host, sb, cudaMemcpyHostToDevice, h->stream));
+  int rc = enqueue_residual(h, h->d_in, h->d_R, h->d_f);
+  if (rc) return rc;
+  h->last_launches = 2;
+  CK(cudaMemcpyAsync(f_host, h->d_f, sb, cudaMemcpyDeviceToHost, h->stream));
+  if (R_host) CK(cudaMemcpyAsync(R_host, h->d_R, sb, cudaMemcpyDeviceToHost, h->stream));
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
+  return DGB_OK;
+}
+
+int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, double* norms_host)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
+  if (!(dt == dt)) return fail(DGB_ERR_ARG, "dt is NaN");
+  CK(cudaSetDevice(h->device));
+  if (nsteps == 0) return DGB_OK;
+  if (nsteps > h->norms_cap) {
+    if (h->d_norms) CK(cudaFree(h->d_norms));
+    h->d_norms = nullptr;
+    CK(cudaMalloc(&h->d_norms, sizeof(double) * nsteps));
+    h->norms_cap = nsteps;
+    if (h->graph) {  // the captured graph holds the old norms pointer
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      h->graph_scheme = -1;
+    }
+  }
+  if (!h->graph || h->graph_scheme != scheme || h->graph_dt != dt) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(h, scheme, dt);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    h->graph_scheme = scheme;
+    h->graph_dt = dt;
+    h->launches_per_step = launches_per_step(h, scheme);
+  }
+  CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  for (unsigned long long s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->graph, h->stream));
+  h->last_launches = (long long)nsteps * h->launches_per_step;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (norms_host)
+    CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
+  return DGB_OK;
+}
+
+int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk)
+{
+  if (!h || !nk || reps < 1) return fail(DGB_ERR_ARG, "bad argument");
+  if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
+  CK(cudaSetDevice(h->device));
+  const int nl = (int)launches_per_step(h, scheme);
+  if (*nk < nl || !ms_out) {
+    *nk = nl;
+    return fail(DGB_ERR_ARG, "ms_out too small");
+  }
+  *nk = nl;
+  if (h->norms_cap < 1) {
+    CK(cudaMalloc(&h->d_norms, sizeof(double)));
+    h->norms_cap = 1;
+  }
+  std::vector<cudaEvent_t> ev((size_t)reps * (nl + 1));
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  int rc = DGB_OK;
+  for (int r = 0; r < reps && rc == DGB_OK; ++r) {
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+    rc = enqueue_step(h, scheme, dt, &ev[(size_t)r * (nl + 1)]);
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < nl; ++k) ms_out[k] = 0.;
+  for (int r = 0; r < reps && rc == DGB_OK; ++r)
+    for (int k = 0; k < nl; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[(size_t)r * (nl + 1) + k], ev[(size_t)r * (nl + 1) + k + 1]));
+      ms_out[k] += ms / reps;
+    }
+  for (auto& e : ev) cudaEventDestroy(e);
+  h->last_launches = (long long)reps * nl;
+  return rc;
+}
+
+// ------------------------------------------------------------ host helpers
+
+int dgb_gauss_legendre(int n, double a, double b, double* x, double* w)
+{
+  if (n < 1 || !x || !w) return fail(DGB_ERR_ARG, "n must be >= 1");
+  gauss_legendre(n, a, b, x, w);
+  return DGB_OK;
+}
+
+double dgb_lagrange1d(int i, int p, double x) { return lagrange1d(i, p, x); }
+double dgb_lagrange1d_deriv(int i, int p, double x) { return lagrange1d_deriv(i, p, x); }
+
+// generate_bump_nodes (geometry_common.cpp:494-576) for a single domain:
+// box elements with optional tanh stretching in y, then the Gaussian bump
+// that lifts the lower wall and relaxes linearly to the upper wall.
+int dgb_bump_nodes(int nx, int ny, int nz, int q, double lx, double ly, double lz, double a,
+                   double bh, double bc, double bv, double* nodes)
+{
+  if (nx <= 0 || ny <= 0 || nz <= 0 || q < 1 || !nodes) return fail(DGB_ERR_ARG, "bad mesh size");
+  const int Q = q + 1;
+  const double elx = lx / nx, ely = ly / ny, elz = lz / nz;
+  const double nsx = elx / q, nsz = elz / q;
+  for (int ez = 0; ez < nz; ++ez)
+    for (int ey = 0; ey < ny; ++ey) {
+      double esy, eey;
+      if (a != 0.) {
+        double xi = -1. + 2. * ((double)ey / ny);
+        double y = 0.5 * std::tanh(xi * std::atanh(a));
+        esy = ly * ((y * (2. / a) + 1.) / 2.);
+        xi = -1. + 2. * ((double)(ey + 1.) / ny);
+        y = 0.5 * std::tanh(xi * std::atanh(a));
+        eey = ly * ((y * (2. / a) + 1.) / 2.);
+      } else {
+        esy = ey * ely;
+        eey = (ey + 1.) * ely;
+      }
+      const double nsy = (eey - esy) / q;
+      for (int ex = 0; ex < nx; ++ex) {
+        const long e = ex + (long)nx * (ey + (long)ny * ez);
+        for (int k = 0; k < Q; ++k)
+          for (int j = 0; j < Q; ++j)
+            for (int i = 0; i < Q; ++i) {
+              double* x = nodes + 3 * (Q * Q * Q * e + i + Q * (j + Q * k));
+              x[0] = ex * elx + nsx * i;
+              x[1] = esy + nsy * j;
+              x[2] = ez * elz + nsz * k;
+              const double f = bh * std::exp(-((x[0] - bc) * (x[0] - bc)) / (2. * bv));
+              x[1] = (x[1] / ly) * (ly - f) + f;
+            }
+      }
+    }
+  return DGB_OK;
+}
+
+int dgb_make_reference_state(double gamma, double gcnst, double mu, double c, double rho, double u,
+                             double v, double w, double eta, const double* source, dgb_params* out)
+{
+  if (!out) return fail(DGB_ERR_ARG, "null output");
+  const double P = c * c * (rho / gamma);
+  out->gamma = gamma;
+  out->R = gcnst;
+  out->mu = mu;
+  out->c = c;
+  out->T = P / (rho * gcnst);
+  out->P = P;
+  out->eta = eta;
+  out->Ufr[0] = rho;
+  out->Ufr[1] = rho * u;
+  out->Ufr[2] = rho * v;
+  out->Ufr[3] = rho * w;
+  out->Ufr[4] = P / (gamma - 1.) + 0.5 * rho * (u * u + v * v + w * w);
+  for (int i = 0; i < 5; ++i) out->source[i] = source ? source[i] : 0.;
+  return DGB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// Pointwise physics shared by the kernels, written for a generic real type T
+// (double in the FP64 path, float in the mixed path).  Formulas follow the
+// reference's flux.cpp and bound_states.cpp; the cited lines name the
+// equations restated here.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace dgb {
+
+struct DevParams {
+  double gamma, R, mu, P, Pt, Tt, eta;
+  double Ufr[5];
+  double src[5];
+};
+
+// F(U) . n for the Euler flux (flux.cpp:24-48).
+template <class T>
+__device__ __forceinline__ void euler_flux_n(const T* U, T gamma, const T* n, T* Fn)
+{
+  const T r = U[0], u = U[1] / r, v = U[2] / r, w = U[3] / r;
+  const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
+  const T un = u * n[0] + v * n[1] + w * n[2];
+  const T H = (U[4] + p) / r;
+  Fn[0] = r * un;
+  Fn[1] = r * u * un + p * n[0];
+  Fn[2] = r * v * un + p * n[1];
+  Fn[3] = r * w * un + p * n[2];
+  Fn[4] = r * H * un;
+}
+
+// Full Euler flux, F[c][r] for direction c (flux.cpp:24-48).
+template <class T>
+__device__ __forceinline__ void euler_flux(const T* U, T gamma, T F[3][5])
+{
+  const T r = U[0], u = U[1] / r, v = U[2] / r, w = U[3] / r;
+  const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
+  const T H = (U[4] + p) / r;
+  const T vel[3] = {u, v, w};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T m = r * vel[c];
+    F[c][0] = m;
+    F[c][1] = m * u;
+    F[c][2] = m * v;
+    F[c][3] = m * w;
+    F[c][4] = m * H;
+    F[c][1 + c] += p;
+  }
+}
+
+// Viscous (Stokes, no heat conduction) flux Q[c][r] = A(S, grad S)
+// (flux.cpp:156-202).  G[c][r] = d S_r / d x_c.
+template <class T>
+__device__ __forceinline__ void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
+{
+  const T lam = -(T(2) / T(3)) * mu;
+  const T r = S[0], u = S[1] / r, v = S[2] / r, w = S[3] / r;
+  T du[3][3];  // du[i][c] = d vel_i / d x_c
+  const T vel[3] = {u, v, w};
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[i][c] = (G[c][1 + i] - G[c][0] * vel[i]) / r;
+  const T dv = du[0][0] + du[1][1] + du[2][2];
+  T tau[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) tau[i][c] = mu * (du[i][c] + du[c][i]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) tau[i][i] = lam * dv + T(2) * mu * du[i][i];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Q[c][0] = T(0);
+    Q[c][1] = tau[0][c];
+    Q[c][2] = tau[1][c];
+    Q[c][3] = tau[2][c];
+    Q[c][4] = u * tau[0][c] + v * tau[1][c] + w * tau[2][c];
+  }
+}
+
+// A(S, d (x) n) . n : viscous flux of a jump d along normal n, projected on n
+// (the BR2 lifting and dual-consistency arguments, solve.cpp:432-444, 516-528).
+template <class T>
+__device__ __forceinline__ void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
+{
+  T G[3][5], Q[3][5];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 5; ++r) G[c][r] = d[r] * n[c];
+  visc_flux(S, G, mu, Q);
+#pragma unroll
+  for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
+}
+
+// Roe flux with the entropy fix at 5% of the Roe sound speed (flux.cpp:56-154).
+template <class T>
+__device__ __forceinline__ void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
+{
+  const T gm1 = g - T(1);
+  const T rl = Ul[0], ul = Ul[1] / rl, vl = Ul[2] / rl, wl = Ul[3] / rl;
+  const T pl = gm1 * (Ul[4] - T(0.5) * rl * (ul * ul + vl * vl + wl * wl));
+  const T Hl = (Ul[4] + pl) / rl;
+  const T rr = Ur[0], ur = Ur[1] / rr, vr = Ur[2] / rr, wr = Ur[3] / rr;
+  const T pr = gm1 * (Ur[4] - T(0.5) * rr * (ur * ur + vr * vr + wr * wr));
+  const T Hr = (Ur[4] + pr) / rr;
+  const T sl = sqrt(rl), sr = sqrt(rr), den = sl + sr;
+  const T u = (sl * ul + sr * ur) / den, v = (sl * vl + sr * vr) / den;
+  const T w = (sl * wl + sr * wr) / den, H = (sl * Hl + sr * Hr) / den;
+  const T dr = rr - rl, dmx = Ur[1] - Ul[1], dmy = Ur[2] - Ul[2], dmz = Ur[3] - Ul[3];
+  const T dE = Ur[4] - Ul[4];
+  const T q2 = u * u + v * v + w * w;
+  const T c = sqrt(gm1 * (H - T(0.5) * q2));
+  const T un = u * n[0] + v * n[1] + w * n[2];
+  const T l1 = un + c, l2 = un - c, l3 = un, eps = T(0.05) * c;
+  T a1 = fabs(l1), a2 = fabs(l2), a3 = fabs(l3);
+  if (a1 < eps) a1 = fabs((eps * eps + l1 * l1) / (T(2) * eps));
+  if (a2 < eps) a2 = fabs((eps * eps + l2 * l2) / (T(2) * eps));
+  if (a3 < eps) a3 = fabs((eps * eps + l3 * l3) / (T(2) * eps));
+  const T s1 = T(0.5) * (a1 + a2), s2 = T(0.5) * (a1 - a2);
+  const T G1 = gm1 * (T(0.5) * q2 * dr - (u * dmx + v * dmy + w * dmz) + dE);
+  const T G2 = -un * dr + (dmx * n[0] + dmy * n[1] + dmz * n[2]);
+  const T C1 = (G1 / (c * c)) * (s1 - a3) + (G2 / c) * s2;
+  const T C2 = (G1 / c) * s2 + (s1 - a3) * G2;
+  const T unl = ul * n[0] + vl * n[1] + wl * n[2];
+  const T unr = ur * n[0] + vr * n[1] + wr * n[2];
+  f[0] = T(0.5) * (rl * unl + rr * unr) - T(0.5) * (a3 * dr + C1);
+  f[1] = T(0.5) * (rl * ul * unl + pl * n[0] + rr * ur * unr + pr * n[0]) -
+         T(0.5) * (a3 * dmx + C1 * u + C2 * n[0]);
+  f[2] = T(0.5) * (rl * vl * unl + pl * n[1] + rr * vr * unr + pr * n[1]) -
+         T(0.5) * (a3 * dmy + C1 * v + C2 * n[1]);
+  f[3] = T(0.5) * (rl * wl * unl + pl * n[2] + rr * wr * unr + pr * n[2]) -
+         T(0.5) * (a3 * dmz + C1 * w + C2 * n[2]);
+  f[4] = T(0.5) * (rl * Hl * unl + rr * Hr * unr) - T(0.5) * (a3 * dE + C1 * H + C2 * un);
+}
+
+// Ghost state for a boundary face (bound_states.cpp:24-130, selected as in
+// solve.cpp:235-252).  Returns 1 when subsonic inflow has no non-negative
+// boundary Mach root (the reference aborts there on the host, :80-83).
+template <class T>
+__device__ __forceinline__ int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm,
+                                              T* Ub)
+{
+  const T gamma = T(prm.gamma), gm1 = gamma - T(1);
+  const T u = UL[1] / UL[0], v = UL[2] / UL[0], w = UL[3] / UL[0];
+  if (bt == -3) {  // freestream
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Ub[r] = T(prm.Ufr[r]);
+    return 0;
+  }
+  if (bt == -4) {  // inviscid wall: remove the normal velocity
+    const T vn = u * n[0] + v * n[1] + w * n[2];
+    Ub[0] = UL[0];
+    Ub[1] = UL[0] * (u - vn * n[0]);
+    Ub[2] = UL[0] * (v - vn * n[1]);
+    Ub[3] = UL[0] * (w - vn * n[2]);
+    Ub[4] = UL[4];
+    return 0;
+  }
+  if (bt == -7) {  // no-slip wall: zero velocity, interior total energy
+    Ub[0] = UL[0];
+    Ub[1] = T(0);
+    Ub[2] = T(0);
+    Ub[3] = T(0);
+    Ub[4] = UL[4];
+    return 0;
+  }
+  const T q2 = u * u + v * v + w * w;
+  const T pp = gm1 * (UL[4] - T(0.5) * UL[0] * q2);
+  const T unp = u * n[0] + v * n[1] + w * n[2];
+  const T cp = sqrt(gamma * pp / UL[0]);
+  const T Jp = unp + T(2) * cp / gm1;
+  if (bt == -5) {  // subsonic inflow: total T and p, outgoing Riemann invariant
+    const T RTt = gamma * T(prm.R) * T(prm.Tt);
+    const T a = RTt - T(0.5) * gm1 * Jp * Jp;
+    const T b = -T(4) * RTt / gm1;
+    const T c = T(4) * RTt / (gm1 * gm1) - Jp * Jp;
+    const T disc = sqrt(b * b - T(4) * a * c);
+    const T s0 = (-b + disc) / (T(2) * a), s1 = (-b - disc) / (T(2) * a);
+    T Mb = T(0);
+    int bad = 0;
+    if (s0 >= T(0) && s1 >= T(0)) Mb = s0 < s1 ? s0 : s1;
+    else if (s0 >= T(0)) Mb = s0;
+    else if (s1 >= T(0)) Mb = s1;
+    else bad = 1;
+    const T Tb = T(prm.Tt) / (T(1) + T(0.5) * gm1 * Mb * Mb);
+    const T Pb = T(prm.Pt) * pow(Tb / T(prm.Tt), gamma / gm1);
+    const T rb = Pb / (T(prm.R) * Tb);
+    const T cb = sqrt(gamma * Pb / rb);
+    const T ub = -Mb * cb * n[0], vb = -Mb * cb * n[1], wb = -Mb * cb * n[2];
+    Ub[0] = rb;
+    Ub[1] = rb * ub;
+    Ub[2] = rb * vb;
+    Ub[3] = rb * wb;
+    Ub[4] = Pb / gm1 + T(0.5) * rb * (ub * ub + vb * vb + wb * wb);
+    return bad;
+  }
+  // subsonic outflow: fixed static pressure, interior entropy and invariant
+  const T Pf = T(prm.P);
+  const T Sp = pp / pow(UL[0], gamma);
+  const T rb = pow(Pf / Sp, T(1) / gamma);
+  const T cb = sqrt(gamma * Pf / rb);
+  const T unb = Jp - T(2) * cb / gm1;
+  const T ub = u - unp * n[0] + unb * n[0], vb = v - unp * n[1] + unb * n[1];
+  const T wb = w - unp * n[2] + unb * n[2];
+  Ub[0] = rb;
+  Ub[1] = rb * ub;
+  Ub[2] = rb * vb;
+  Ub[3] = rb * wb;
+  Ub[4] = Pf / gm1 + T(0.5) * rb * (ub * ub + vb * vb + wb * wb);
+  return 0;
+}
+
+}  // namespace dgb

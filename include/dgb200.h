@@ -1,0 +1,187 @@
+/* dgb200: B200-native explicit DG residual and Runge-Kutta time step for the
+ * 3D compressible Navier-Stokes / Euler equations on structured hex meshes.
+ *
+ * C ABI of the drop-in replacement for the reference's single-GPU path
+ * (solver/solve_cuda.cu + solver/time_cuda.cu, driven by solver/cudg.cu).
+ * Plain C types only: host pointers and sizes, optional device pointers and a
+ * CUDA stream passed as void*.  Every entry point returns a DGB_* status code;
+ * nothing calls exit() (the reference aborts through errout, error.cpp:34-52).
+ *
+ * Data layouts are the reference's:
+ *   state   U[e][r][b]   element-major, 5 conserved variables, (p+1)^3 nodal
+ *                        coefficients ordered [z[y[x]]]  (geometry_common.cpp:467-470)
+ *   nodes   X[e][n][3]   (q+1)^3 geometry nodes per element, [z[y[x]]] order
+ *                        (geometry_common.cpp:44-48)
+ *   element e = i + nx*(j + ny*k)                         (geometry_shared.cpp:171)
+ *   bounds  six btype codes for -x +x -y +y -z +z         (boundaries.cpp:26-35)
+ */
+#ifndef DGB200_H
+#define DGB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+  DGB_OK = 0,
+  DGB_ERR_ARG = 1,          /* bad argument, size or layout */
+  DGB_ERR_UNSUPPORTED = 2,  /* valid input outside what this build implements */
+  DGB_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+  DGB_ERR_GEOMETRY = 4,     /* singular Jacobian / mass matrix, mismatched periodic bounds */
+  DGB_ERR_NONFINITE = 5,    /* a residual or state value became NaN/Inf */
+  DGB_ERR_IO = 6,           /* .dg file could not be read or written */
+  DGB_ERR_BOUNDARY = 7      /* subsonic inflow with no non-negative boundary Mach root */
+};
+
+/* boundary types, same codes as the reference's btype enum (boundaries.cpp:26-35) */
+enum {
+  DGB_BT_INTERIOR = -1,
+  DGB_BT_PERIODIC = -2,
+  DGB_BT_FREESTREAM = -3,
+  DGB_BT_INVISCID_WALL = -4,
+  DGB_BT_SUBSONIC_INFLOW = -5,
+  DGB_BT_SUBSONIC_OUTFLOW = -6,
+  DGB_BT_NO_SLIP_WALL = -7
+};
+
+/* time schemes, same order as the reference's time_scheme enum (time.cpp:23-27) */
+enum { DGB_RK4 = 0, DGB_TVDRK3 = 1 };
+
+/* arithmetic of the residual path */
+enum {
+  DGB_FP64 = 0,        /* everything in FP64 */
+  DGB_MIXED_FP32 = 1   /* FP32 contractions and fluxes, FP64 geometry / inverse mass / RK */
+};
+
+typedef struct dgb_handle dgb_handle;
+
+/* mesh: the fields of the reference's core_geometry that define a mesh
+ * (geometry_common.cpp:25-83) */
+typedef struct {
+  int nx, ny, nz;          /* elements per direction */
+  int p, q;                /* solution and geometry order */
+  const double* nodes;     /* [nx*ny*nz][(q+1)^3][3] */
+  long long bounds[6];     /* btype code per domain side */
+} dgb_mesh_desc;
+
+/* physical and reference parameters: the reference's `parameters` struct
+ * (solver_params.cpp:22-36) */
+typedef struct {
+  double gamma;      /* ratio of specific heats */
+  double R;          /* specific gas constant */
+  double mu;         /* dynamic viscosity */
+  double c;          /* reference speed of sound */
+  double T;          /* reference static temperature */
+  double P;          /* reference static pressure */
+  double Ufr[5];     /* freestream conserved state */
+  double source[5];  /* constant volume source per conserved variable */
+  double eta;        /* BR2 stabilisation constant */
+} dgb_params;
+
+/* Human-readable text for a status code. */
+const char* dgb_error_string(int status);
+
+/* Detail of the last failure on the calling thread (empty if none). */
+const char* dgb_last_error_message(void);
+
+/* Builds the device-resident geometry and workspaces for one mesh.
+ * Replaces cuda_device_geometry::cuda_device_geometry (solve_cuda.cu:171) and
+ * cuda_residual_workspace (solve_cuda.cu:303), plus the host precompute they
+ * consume (core_geometry::precompute, geometry_common.cpp:292;
+ * shared_geometry::precompute_face_geometry, geometry_shared.cpp:156).
+ * Uses the current CUDA device. */
+int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precision,
+               dgb_handle** out);
+
+/* Frees everything dgb_create allocated.  Replaces free_cuda_device_geometry
+ * (solve_cuda.cu:267) and free_cuda_residual_workspace (solve_cuda.cu:323). */
+int dgb_destroy(dgb_handle* h);
+
+/* Orders the handle's work after / on this CUDA stream (cudaStream_t as void*;
+ * NULL = legacy default stream, the reference's only stream). */
+int dgb_set_stream(dgb_handle* h, void* stream);
+
+/* Number of doubles in one state array: nx*ny*nz * 5 * (p+1)^3. */
+long long dgb_state_size(const dgb_handle* h);
+
+/* Host <-> device state copies in the reference layout U[e][r][b].
+ * Replace shuffle_state + cudaMemcpy (cudg.cu:97-106) and the reverse
+ * (cudg.cu:117-122). */
+int dgb_set_state(dgb_handle* h, const double* U_host);
+int dgb_get_state(dgb_handle* h, double* U_host);
+
+/* Device pointer of the handle's resident state (for callers that keep data
+ * on the GPU). */
+int dgb_state_device_ptr(dgb_handle* h, double** U_dev);
+
+/* One residual evaluation of U: R = un-inverted residual (may be NULL) and
+ * f = dU/dt = -Minv R.  Host pointers; copies in and out.
+ * Replaces cuda_residual (solve_cuda.cu:1235) / residual (solve.cpp:150). */
+int dgb_residual(dgb_handle* h, const double* U_host, double* R_host, double* f_host);
+
+/* Same on device pointers, on the handle's stream, no host synchronisation. */
+int dgb_residual_device(dgb_handle* h, const double* U_dev, double* R_dev, double* f_dev);
+
+/* Advances the resident state nsteps steps of size dt with RK4 or TVD-RK3.
+ * norms_host (may be NULL) receives, per step, sqrt(sum R^2 / size) of the
+ * first stage's residual, the number the reference prints each step
+ * (time_cuda.cu:36-47, time_distributed.cpp:23-44).
+ * Replaces RK4_cuda / tvdRK3_cuda (time_cuda.cu:126-185) and
+ * RK4_distributed / tvdRK3_distributed (time_distributed.cpp:46-102).
+ * Returns DGB_ERR_NONFINITE if a residual norm became NaN/Inf (the reference
+ * aborts on a NaN norm, time_distributed.cpp:41-42). */
+int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps,
+             double* norms_host);
+
+/* Kernel launches issued by the last dgb_step / dgb_residual call. */
+long long dgb_last_launch_count(const dgb_handle* h);
+
+/* Measurement hook: runs `reps` RK steps of the resident state launch by
+ * launch (no graph) with a CUDA event between consecutive launches on the
+ * handle's stream; ms_out[k] is the mean duration of launch k of one step.
+ * *nk: capacity of ms_out in, launches per step out.  Advances the state like
+ * dgb_step. */
+int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk);
+
+/* ---------------------------------------------------------------- host side
+ * Host-only helpers (no GPU needed) that mirror the reference's setup
+ * functions, for drivers and for checks. */
+
+/* n-point Gauss-Legendre rule on [a,b] (quadrature.cpp:84-205). */
+int dgb_gauss_legendre(int n, double a, double b, double* x, double* w);
+
+/* Equispaced Lagrange basis on [0,1] and its derivative (basis.cpp:91-148). */
+double dgb_lagrange1d(int i, int p, double x);
+double dgb_lagrange1d_deriv(int i, int p, double x);
+
+/* Geometry nodes of the reference's bump / stretched channel generator
+ * (generate_bump_nodes, geometry_common.cpp:494-576, as called by
+ * bump_shared, geometry_shared.cpp:275-292).  nodes: [nx*ny*nz][(q+1)^3][3]. */
+int dgb_bump_nodes(int nx, int ny, int nz, int q, double lx, double ly, double lz,
+                   double a, double bmp_height, double bmp_center, double bmp_variance,
+                   double* nodes);
+
+/* make_reference_state (solver_params.cpp:40-70). */
+int dgb_make_reference_state(double gamma, double gcnst, double mu, double c, double rho,
+                             double u, double v, double w, double eta,
+                             const double* source, dgb_params* out);
+
+/* Writes a .dg file byte-compatible with the reference's write_state
+ * (io.cpp:33-90): outputs appear in the reference's hash-map order
+ * (djb2 mod 256, data_structures.cpp:538-583). */
+int dgb_write_state(const char* fname, unsigned long long tstep, const dgb_mesh_desc* mesh,
+                    int noutput, const char* const* keys, const double* const* data);
+
+/* Reads a .dg header (io.cpp:92-124): sizes and bounds; nodes and the state
+ * named `key` are copied when their pointers are non-NULL.  Returns
+ * DGB_ERR_IO on a short or malformed file. */
+int dgb_read_state(const char* fname, unsigned long long* tstep, int* nx, int* ny, int* nz,
+                   int* p, int* q, long long* bounds, double* nodes, const char* key,
+                   double* data);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGB200_H */
