@@ -383,12 +383,7 @@ stage_kernel(long E, const double* Us, const double* __restrict__ Tr,
           jmp[r] = Uo[r] - Un[r];
         }
         if (mu != 0.) {
-          double G[3][5];
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int r = 0; r < 5; ++r) G[c][r] = dd[r] * n[c];
-          visc_flux(Uo, G, mu, dc);
+          visc_rank1(Uo, dd, n, mu, dc);
           // BR2 lifting sources of both sides, weighted by their inverse-mass factor
           double ro[5], rn[5];
           visc_jump_n(Uo, jmp, n, mu, ro);
@@ -417,12 +412,7 @@ stage_kernel(long E, const double* Us, const double* __restrict__ Tr,
 #pragma unroll
         for (int r = 0; r < 5; ++r) dd[r] = Uo[r] - Ub[r];
         if (mu != 0.) {
-          double G[3][5];
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int r = 0; r < 5; ++r) G[c][r] = dd[r] * n[c];
-          visc_flux(Uo, G, mu, dc);
+          visc_rank1(Uo, dd, n, mu, dc);
           double rb[5];
           visc_jump_n(Ub, dd, n, mu, rb);
           const double co = so[C::oC + end] / detJ;

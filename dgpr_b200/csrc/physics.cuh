@@ -18,10 +18,10 @@ struct DevParams {
 template <class T>
 __device__ __forceinline__ void euler_flux_n(const T* U, T gamma, const T* n, T* Fn)
 {
-  const T r = U[0], u = U[1] / r, v = U[2] / r, w = U[3] / r;
+  const T r = U[0], ir = T(1) / r, u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
   const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
   const T un = u * n[0] + v * n[1] + w * n[2];
-  const T H = (U[4] + p) / r;
+  const T H = (U[4] + p) * ir;
   Fn[0] = r * un;
   Fn[1] = r * u * un + p * n[0];
   Fn[2] = r * v * un + p * n[1];
@@ -33,9 +33,9 @@ __device__ __forceinline__ void euler_flux_n(const T* U, T gamma, const T* n, T*
 template <class T>
 __device__ __forceinline__ void euler_flux(const T* U, T gamma, T F[3][5])
 {
-  const T r = U[0], u = U[1] / r, v = U[2] / r, w = U[3] / r;
+  const T r = U[0], ir = T(1) / r, u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
   const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
-  const T H = (U[4] + p) / r;
+  const T H = (U[4] + p) * ir;
   const T vel[3] = {u, v, w};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -55,13 +55,14 @@ template <class T>
 __device__ __forceinline__ void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
 {
   const T lam = -(T(2) / T(3)) * mu;
-  const T r = S[0], u = S[1] / r, v = S[2] / r, w = S[3] / r;
+  const T ir = T(1) / S[0];
+  const T u = S[1] * ir, v = S[2] * ir, w = S[3] * ir;
   T du[3][3];  // du[i][c] = d vel_i / d x_c
   const T vel[3] = {u, v, w};
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) du[i][c] = (G[c][1 + i] - G[c][0] * vel[i]) / r;
+    for (int c = 0; c < 3; ++c) du[i][c] = (G[c][1 + i] - G[c][0] * vel[i]) * ir;
   const T dv = du[0][0] + du[1][1] + du[2][2];
   T tau[3][3];
 #pragma unroll
@@ -80,19 +81,56 @@ __device__ __forceinline__ void visc_flux(const T* S, const T G[3][5], T mu, T Q
   }
 }
 
-// A(S, d (x) n) . n : viscous flux of a jump d along normal n, projected on n
-// (the BR2 lifting and dual-consistency arguments, solve.cpp:432-444, 516-528).
+// A(S, d (x) n): the viscous flux of a rank-one "gradient" d n^T, the argument
+// of the BR2 lifting and dual-consistency terms (solve.cpp:432-444, 516-528,
+// 657-667).  With a_i = (d_{1+i} - d_0 vel_i) / rho the velocity gradient is
+// a n^T, so tau = mu (a n^T + n a^T) + lam (a.n) I.
+template <class T>
+__device__ __forceinline__ void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5])
+{
+  const T lam = -(T(2) / T(3)) * mu;
+  const T ir = T(1) / S[0];
+  const T vel[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
+  T a[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) a[i] = (d[1 + i] - d[0] * vel[i]) * ir;
+  const T an = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    T e = T(0);
+    Q[c][0] = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      T t = mu * (a[i] * n[c] + a[c] * n[i]);
+      if (i == c) t += lam * an;
+      Q[c][1 + i] = t;
+      e += vel[i] * t;
+    }
+    Q[c][4] = e;
+  }
+}
+
+// A(S, d (x) n) . n, the normal component only.
 template <class T>
 __device__ __forceinline__ void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
 {
-  T G[3][5], Q[3][5];
+  const T lam = -(T(2) / T(3)) * mu;
+  const T ir = T(1) / S[0];
+  const T vel[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
+  T a[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
+  for (int i = 0; i < 3; ++i) a[i] = (d[1 + i] - d[0] * vel[i]) * ir;
+  const T an = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+  const T nn = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+  Qn[0] = T(0);
+  T e = T(0);
 #pragma unroll
-    for (int r = 0; r < 5; ++r) G[c][r] = d[r] * n[c];
-  visc_flux(S, G, mu, Q);
-#pragma unroll
-  for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
+  for (int i = 0; i < 3; ++i) {
+    const T t = mu * (a[i] * nn + an * n[i]) + lam * an * n[i];
+    Qn[1 + i] = t;
+    e += vel[i] * t;
+  }
+  Qn[4] = e;
 }
 
 // Roe flux with the entropy fix at 5% of the Roe sound speed (flux.cpp:56-154).
@@ -100,30 +138,34 @@ template <class T>
 __device__ __forceinline__ void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
 {
   const T gm1 = g - T(1);
-  const T rl = Ul[0], ul = Ul[1] / rl, vl = Ul[2] / rl, wl = Ul[3] / rl;
+  const T rl = Ul[0], irl = T(1) / rl, ul = Ul[1] * irl, vl = Ul[2] * irl, wl = Ul[3] * irl;
   const T pl = gm1 * (Ul[4] - T(0.5) * rl * (ul * ul + vl * vl + wl * wl));
-  const T Hl = (Ul[4] + pl) / rl;
-  const T rr = Ur[0], ur = Ur[1] / rr, vr = Ur[2] / rr, wr = Ur[3] / rr;
+  const T Hl = (Ul[4] + pl) * irl;
+  const T rr = Ur[0], irr = T(1) / rr, ur = Ur[1] * irr, vr = Ur[2] * irr, wr = Ur[3] * irr;
   const T pr = gm1 * (Ur[4] - T(0.5) * rr * (ur * ur + vr * vr + wr * wr));
-  const T Hr = (Ur[4] + pr) / rr;
-  const T sl = sqrt(rl), sr = sqrt(rr), den = sl + sr;
-  const T u = (sl * ul + sr * ur) / den, v = (sl * vl + sr * vr) / den;
-  const T w = (sl * wl + sr * wr) / den, H = (sl * Hl + sr * Hr) / den;
+  const T Hr = (Ur[4] + pr) * irr;
+  const T sl = sqrt(rl), sr = sqrt(rr), iden = T(1) / (sl + sr);
+  const T u = (sl * ul + sr * ur) * iden, v = (sl * vl + sr * vr) * iden;
+  const T w = (sl * wl + sr * wr) * iden, H = (sl * Hl + sr * Hr) * iden;
   const T dr = rr - rl, dmx = Ur[1] - Ul[1], dmy = Ur[2] - Ul[2], dmz = Ur[3] - Ul[3];
   const T dE = Ur[4] - Ul[4];
   const T q2 = u * u + v * v + w * w;
   const T c = sqrt(gm1 * (H - T(0.5) * q2));
+  const T ic = T(1) / c;
   const T un = u * n[0] + v * n[1] + w * n[2];
   const T l1 = un + c, l2 = un - c, l3 = un, eps = T(0.05) * c;
   T a1 = fabs(l1), a2 = fabs(l2), a3 = fabs(l3);
-  if (a1 < eps) a1 = fabs((eps * eps + l1 * l1) / (T(2) * eps));
-  if (a2 < eps) a2 = fabs((eps * eps + l2 * l2) / (T(2) * eps));
-  if (a3 < eps) a3 = fabs((eps * eps + l3 * l3) / (T(2) * eps));
+  if (a1 < eps || a2 < eps || a3 < eps) {  // entropy fix, rarely taken
+    const T i2e = T(1) / (T(2) * eps);
+    if (a1 < eps) a1 = fabs((eps * eps + l1 * l1) * i2e);
+    if (a2 < eps) a2 = fabs((eps * eps + l2 * l2) * i2e);
+    if (a3 < eps) a3 = fabs((eps * eps + l3 * l3) * i2e);
+  }
   const T s1 = T(0.5) * (a1 + a2), s2 = T(0.5) * (a1 - a2);
   const T G1 = gm1 * (T(0.5) * q2 * dr - (u * dmx + v * dmy + w * dmz) + dE);
   const T G2 = -un * dr + (dmx * n[0] + dmy * n[1] + dmz * n[2]);
-  const T C1 = (G1 / (c * c)) * (s1 - a3) + (G2 / c) * s2;
-  const T C2 = (G1 / c) * s2 + (s1 - a3) * G2;
+  const T C1 = (G1 * ic * ic) * (s1 - a3) + (G2 * ic) * s2;
+  const T C2 = (G1 * ic) * s2 + (s1 - a3) * G2;
   const T unl = ul * n[0] + vl * n[1] + wl * n[2];
   const T unr = ur * n[0] + vr * n[1] + wr * n[2];
   f[0] = T(0.5) * (rl * unl + rr * unr) - T(0.5) * (a3 * dr + C1);
