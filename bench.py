@@ -184,16 +184,22 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    # warm-up (also builds the graph)
-    for _ in range(args.warmup):
+    # warm-up: at least W steps and at least half a second of GPU work, so the
+    # clocks have settled; the clock sampler runs from here to the end of the
+    # timed region
+    clk = Clocks(local_rank)
+    clk.start()
+    t_w = time.perf_counter()
+    warm = 0
+    while warm < args.warmup or time.perf_counter() - t_w < 0.5:
         s.step(dg.RK4, dt, 1, norms=False)
+        warm += 1
     torch.cuda.synchronize()
+    args.warmup = warm
 
     # ---- device-timed: K graph-launched steps, state resident
-    clk = Clocks(local_rank)
     barrier()
     torch.cuda.synchronize()
-    clk.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
@@ -234,9 +240,9 @@ def run_ours(args, rank, world, local_rank):
     # ---- per-kernel durations for the roofline (events between launches)
     s.set_state(U0)
     kms = s.profile_step(dg.RK4, dt, max(3, min(args.steps, 10)))
-    # launch order per RK4 step: trace0 stage0 norm trace1 stage1 trace2 stage2 trace3 stage3
-    stage_ms = float(np.mean([kms[1], kms[4], kms[6], kms[8]]))
-    trace_ms = float(np.mean([kms[0], kms[3], kms[5], kms[7]]))
+    # launch order: initial traces, then one RK4 step: stage0 norm stage1 stage2 stage3
+    stage_ms = float(np.mean([kms[1], kms[3], kms[4], kms[5]]))
+    trace_ms = float(kms[0])
     nb = (P_ORD + 1) ** 3
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
@@ -285,7 +291,7 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libdgb200.so")
+# DGB200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("DGB200_LIB") or os.path.join(HERE, "_lib", "libdgb200.so")
 
 OK, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_GEOMETRY, ERR_NONFINITE, ERR_IO, ERR_BOUNDARY = range(8)
 INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW, NO_SLIP_WALL = \

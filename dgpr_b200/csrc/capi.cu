@@ -33,7 +33,7 @@ struct dgb_handle {
   double* d_U = nullptr;      // resident state
   double* d_Us = nullptr;     // stage state
   double* d_acc = nullptr;    // RK4 accumulator
-  double* d_trace = nullptr;  // face traces
+  double* d_trace[3] = {nullptr, nullptr, nullptr};  // face traces, rotated between stages
   double* d_in = nullptr;     // residual API input / output
   double* d_f = nullptr;
   double* d_R = nullptr;
@@ -80,7 +80,6 @@ Fp64Launch fp64_launch(const dgb_handle* h)
   L.ops = h->d_ops;
   L.geo = h->d_geo;
   L.nbr = h->d_nbr;
-  L.trace = h->d_trace;
   L.prm = h->dprm;
   return L;
 }
@@ -99,16 +98,30 @@ int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
 {
   if (h->precision == DGB_MIXED_FP32) return mixed_residual(h->mixed, Uin, R, f, h->stream);
   const Fp64Launch L = fp64_launch(h);
-  CK(launch_trace(L, Uin, h->stream));
+  CK(launch_trace(L, Uin, h->d_trace[0], h->stream));
   StageArgs a = stage_args(MODE_RESIDUAL, 0.);
   a.fout = f;
   a.Rout = R;
   a.flag = h->d_flag;
-  CK(launch_stage(L, Uin, a, h->stream));
+  CK(launch_stage(L, Uin, h->d_trace[0], a, h->stream));
   return DGB_OK;
 }
 
-// one full RK step as a launch sequence (captured into a graph by dgb_step).
+// Traces of the resident state, read by the first stage of the next step.
+// Every dgb_step call starts with this one launch; later stages and steps get
+// their traces from the epilogue of the stage before.
+int enqueue_initial_traces(dgb_handle* h)
+{
+  if (h->precision == DGB_MIXED_FP32) return mixed_initial_traces(h->mixed, h->d_U, h->stream);
+  CK(launch_trace(fp64_launch(h), h->d_U, h->d_trace[0], h->stream));
+  return DGB_OK;
+}
+
+// One full RK step as a launch sequence (captured into a graph by dgb_step):
+// the stage kernels, plus the residual-norm kernel after the first stage.
+// Traces rotate so a stage never writes the buffer it reads:
+//   RK4      T0 -> T1 -> T0 -> T1 -> T0
+//   TVD-RK3  T0 -> T1 -> T2 -> T0
 // With ev != null, ev[i] is recorded before launch i and ev[nlaunch] after the
 // last one (per-kernel timing by dgb_profile_step).
 int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr)
@@ -120,19 +133,21 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
   const int nst = scheme == DGB_RK4 ? 4 : 3;
   const int modes4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
   const int modes3[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
+  const int tin4[4] = {0, 1, 0, 1}, tout4[4] = {1, 0, 1, 0};
+  const int tin3[3] = {0, 1, 2}, tout3[3] = {1, 2, 0};
   int k = 0;
   for (int s = 0; s < nst; ++s) {
     const double* in = s == 0 ? h->d_U : h->d_Us;
-    if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-    CK(launch_trace(L, in, h->stream));
     StageArgs a = stage_args(scheme == DGB_RK4 ? modes4[s] : modes3[s], dt);
     a.Ubase = h->d_U;
     a.acc = h->d_acc;
     a.Uout = s == nst - 1 ? h->d_U : h->d_Us;
     a.part = s == 0 ? h->d_part : nullptr;
     a.flag = h->d_flag;
+    a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
+    const double* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-    CK(launch_stage(L, in, a, h->stream));
+    CK(launch_stage(L, in, tin, a, h->stream));
     if (s == 0) {
       if (ev) CK(cudaEventRecord(ev[k++], h->stream));
       CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, h->d_counter, h->d_flag,
@@ -146,14 +161,14 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
 long long launches_per_step(const dgb_handle* h, int scheme)
 {
   const int nst = scheme == DGB_RK4 ? 4 : 3;
-  return h->precision == DGB_MIXED_FP32 ? mixed_launches_per_step(h->mixed, nst) : 2 * nst + 1;
+  return h->precision == DGB_MIXED_FP32 ? mixed_launches_per_step(h->mixed, nst) : nst + 1;
 }
 
 void free_all(dgb_handle* h)
 {
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->d_ops, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace, h->d_in,
-                  h->d_f, h->d_R, h->d_part, h->d_norms, h->d_counter, h->d_flag};
+  void* ptrs[] = {h->d_ops, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0], h->d_trace[1],
+                  h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms, h->d_counter, h->d_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->mixed) mixed_destroy(h->mixed);
@@ -250,7 +265,7 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMalloc(&h->d_U, sb));
   CKF(cudaMalloc(&h->d_Us, sb));
   CKF(cudaMalloc(&h->d_acc, sb));
-  CKF(cudaMalloc(&h->d_trace, sizeof(double) * (size_t)h->E * 60 * h->NQF));
+  for (int t = 0; t < 3; ++t) CKF(cudaMalloc(&h->d_trace[t], sizeof(double) * (size_t)h->E * 60 * h->NQF));
   CKF(cudaMalloc(&h->d_part, sizeof(double) * (size_t)h->E));
   CKF(cudaMalloc(&h->d_counter, sizeof(int)));
   CKF(cudaMalloc(&h->d_flag, sizeof(int)));
@@ -404,8 +419,10 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
   }
   CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  int rc = enqueue_initial_traces(h);
+  if (rc) return rc;
   for (unsigned long long s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->graph, h->stream));
-  h->last_launches = (long long)nsteps * h->launches_per_step;
+  h->last_launches = 1 + (long long)nsteps * h->launches_per_step;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (norms_host)
@@ -421,7 +438,8 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
   if (!h || !nk || reps < 1) return fail(DGB_ERR_ARG, "bad argument");
   if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
   CK(cudaSetDevice(h->device));
-  const int nl = (int)launches_per_step(h, scheme);
+  // launch 0 is the initial trace kernel, then one step's launches
+  const int nl = 1 + (int)launches_per_step(h, scheme);
   if (*nk < nl || !ms_out) {
     *nk = nl;
     return fail(DGB_ERR_ARG, "ms_out too small");
@@ -435,8 +453,11 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
   for (auto& e : ev) CK(cudaEventCreate(&e));
   int rc = DGB_OK;
   for (int r = 0; r < reps && rc == DGB_OK; ++r) {
+    cudaEvent_t* er = &ev[(size_t)r * (nl + 1)];
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-    rc = enqueue_step(h, scheme, dt, &ev[(size_t)r * (nl + 1)]);
+    CK(cudaEventRecord(er[0], h->stream));
+    rc = enqueue_initial_traces(h);
+    if (rc == DGB_OK) rc = enqueue_step(h, scheme, dt, er + 1);
   }
   CK(cudaStreamSynchronize(h->stream));
   for (int k = 0; k < nl; ++k) ms_out[k] = 0.;

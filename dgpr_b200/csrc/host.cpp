@@ -267,13 +267,17 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
   }
   const int npts = (int)pts.size() / 3;
 
+  // the Jacobian is taken at the element centre: for an affine element it is
+  // the same everywhere, and there the q = 1 basis gradients are +-1/4, so
+  // equal elements get bit-identical Jacobians
+  const double centre[3] = {0.5, 0.5, 0.5};
   for (long e = 0; e < E; ++e) {
     const double* X = m.nodes + (size_t)e * nq * 3;
     double J0[9], J[9];
-    jacobian(X, q, &pts[0], J0);
+    jacobian(X, q, centre, J0);
     double scale = 0.;
     for (int i = 0; i < 9; ++i) scale = std::fmax(scale, std::fabs(J0[i]));
-    for (int s = 1; s < npts; ++s) {
+    for (int s = 0; s < npts; ++s) {
       jacobian(X, q, &pts[3 * s], J);
       for (int i = 0; i < 9; ++i)
         if (std::fabs(J[i] - J0[i]) > 1e-11 * scale) {

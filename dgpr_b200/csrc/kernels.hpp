@@ -28,8 +28,9 @@ struct StageArgs {
   double* Uout;
   double* fout;
   double* Rout;
-  double* part;  // per-element sum of R^2 (stage 1 of a step), or null
-  int* flag;     // bit 1: non-finite norm, bit 2: inflow without a Mach root
+  double* part;   // per-element sum of R^2 (stage 1 of a step), or null
+  int* flag;      // bit 1: non-finite norm, bit 2: inflow without a Mach root
+  double* Tnext;  // face traces of Uout for the next stage, or null
 };
 
 // everything the FP64 kernels read that does not change between stages
@@ -39,7 +40,6 @@ struct Fp64Launch {
   const double* ops;   // packed 1D operator table (pack_ops)
   const double* geo;   // [E][kGeoStride]
   const int* nbr;      // [E][6]
-  double* trace;       // [E][6][10][P*P]
   DevParams prm;
 };
 
@@ -48,8 +48,11 @@ void pack_ops(const Ops1D& o, double* table);
 size_t stage_smem_bytes(int P);
 
 cudaError_t prepare_fp64_kernels(int P);
-cudaError_t launch_trace(const Fp64Launch& L, const double* U, cudaStream_t st);
-cudaError_t launch_stage(const Fp64Launch& L, const double* Us, const StageArgs& sa, cudaStream_t st);
+// face traces T[E][6][10][P*P] of U
+cudaError_t launch_trace(const Fp64Launch& L, const double* U, double* Tout, cudaStream_t st);
+// one stage: residual of Us with traces Tin, then sa.mode's update
+cudaError_t launch_stage(const Fp64Launch& L, const double* Us, const double* Tin, const StageArgs& sa,
+                         cudaStream_t st);
 cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, int* counter,
                         int* flag, cudaStream_t st);
 

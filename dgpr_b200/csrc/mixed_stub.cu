@@ -19,6 +19,7 @@ int mixed_step(MixedState*, int, double, double*, double*, double*, double*, dou
 {
   return DGB_ERR_UNSUPPORTED;
 }
+int mixed_initial_traces(MixedState*, const double*, cudaStream_t) { return DGB_ERR_UNSUPPORTED; }
 long long mixed_launches_per_step(const MixedState*, int) { return 0; }
 
 }  // namespace dgb
