@@ -164,6 +164,37 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def _timed_steps(dg, torch, s, stream, dt, steps):
+    """Device time (ms) of `steps` graph-launched RK4 steps on the handle's stream."""
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        s.step(dg.RK4, dt, steps, norms=True)
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1)
+
+
+def _warm(dg, torch, s, dt, min_steps, min_seconds=0.5):
+    t_w = time.perf_counter()
+    warm = 0
+    while warm < min_steps or time.perf_counter() - t_w < min_seconds:
+        s.step(dg.RK4, dt, 1, norms=False)
+        warm += 1
+    torch.cuda.synchronize()
+    return warm
+
+
+def _stage_kernel_ms(dg, s, U0, dt, reps):
+    """Mean per-launch durations (CUDA events on the launching stream) of the
+    stage kernel and of the trace kernel; launch order of one profiled step:
+    initial traces, stage0, norm, stage1, stage2, stage3."""
+    s.set_state(U0)
+    kms = s.profile_step(dg.RK4, dt, reps)
+    return float(np.mean([kms[1], kms[3], kms[4], kms[5]])), float(kms[0])
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import dgpr_b200 as dg
@@ -174,50 +205,39 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
     nodes, prm, U0, dt = tgv_case(N_EL, P_ORD)
     mesh = dg.Mesh(N_EL, N_EL, N_EL, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
-    s = dg.Solver(mesh, dg.Params.from_array(prm))
     stream = torch.cuda.Stream()
-    s.set_stream(stream.cuda_stream)
-    s.set_state(U0)
     dof_stage = 5 * (P_ORD + 1) ** 3 * N_EL ** 3
+    nb = (P_ORD + 1) ** 3
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # warm-up: at least W steps and at least half a second of GPU work, so the
-    # clocks have settled; the clock sampler runs from here to the end of the
-    # timed region
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- FP64 form: warm-up (>= W steps and >= 0.5 s, clocks sampled from
+    # here), then K graph-launched steps with the state resident in HBM
+    s = dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64)
+    s.set_stream(stream.cuda_stream)
+    s.set_state(U0)
     clk = Clocks(local_rank)
     clk.start()
-    t_w = time.perf_counter()
-    warm = 0
-    while warm < args.warmup or time.perf_counter() - t_w < 0.5:
-        s.step(dg.RK4, dt, 1, norms=False)
-        warm += 1
-    torch.cuda.synchronize()
-    args.warmup = warm
-
-    # ---- device-timed: K graph-launched steps, state resident
+    args.warmup = _warm(dg, torch, s, dt, args.warmup)
     barrier()
     torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        ev0.record(stream)
-        s.step(dg.RK4, dt, args.steps, norms=True)
-        ev1.record(stream)
-    torch.cuda.synchronize()
+    ms = max_over_ranks(_timed_steps(dg, torch, s, stream, dt, args.steps))
     barrier()
     clocks = clk.stop()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     launches = s.last_launch_count
     value = world * dof_stage * 4 * args.steps / (ms * 1e-3)
 
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers: every step copies the
+    # state in from pinned host memory and the state and norm back out
     Uh = torch.empty(U0.size, dtype=torch.float64).pin_memory()
     Uh.numpy()[:] = U0
     Uhost = Uh.numpy()
@@ -230,20 +250,37 @@ def run_ours(args, rank, world, local_rank):
         dg._check(dg.lib().dgb_step(s.h, dg.RK4, dt, 1, dg._p(norms_h)))
         dg._check(dg.lib().dgb_get_state(s.h, dg._p(Uhost)))
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * dof_stage * 4 * args.steps / e2e_s
 
-    # ---- per-kernel durations for the roofline (events between launches)
-    s.set_state(U0)
-    kms = s.profile_step(dg.RK4, dt, max(3, min(args.steps, 10)))
-    # launch order: initial traces, then one RK4 step: stage0 norm stage1 stage2 stage3
-    stage_ms = float(np.mean([kms[1], kms[3], kms[4], kms[5]]))
-    trace_ms = float(kms[0])
-    nb = (P_ORD + 1) ** 3
+    reps = max(3, min(args.steps, 10))
+    stage_ms, trace_ms = _stage_kernel_ms(dg, s, U0, dt, reps)
+    s.close()
+
+    # ---- mixed form, same workload
+    sm = dg.Solver(mesh, dg.Params.from_array(prm), dg.MIXED_FP32)
+    sm.set_stream(stream.cuda_stream)
+    sm.set_state(U0)
+    _warm(dg, torch, sm, dt, 3)
+    barrier()
+    torch.cuda.synchronize()
+    ms_mixed = max_over_ranks(_timed_steps(dg, torch, sm, stream, dt, args.steps))
+    value_mixed = world * dof_stage * 4 * args.steps / (ms_mixed * 1e-3)
+    stage_ms_mixed, trace_ms_mixed = _stage_kernel_ms(dg, sm, U0, dt, reps)
+    sm.close()
+
+    # ---- accuracy of the mixed form against the FP64 form after many steps
+    acc = None
+    if rank == 0 and args.accuracy_steps > 0:
+        out = {}
+        for prec in (dg.FP64, dg.MIXED_FP32):
+            with dg.Solver(mesh, dg.Params.from_array(prm), prec) as sa:
+                sa.set_state(U0)
+                sa.step(dg.RK4, dt, args.accuracy_steps, norms=False)
+                out[prec] = sa.get_state()
+        err = float(np.linalg.norm(out[dg.MIXED_FP32] - out[dg.FP64]) / np.linalg.norm(out[dg.FP64]))
+        acc = {"steps": args.accuracy_steps, "rel_l2_mixed_vs_fp64": err}
+
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
     try:
@@ -252,7 +289,7 @@ def run_ours(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
-    s.close()
+    barrier()
 
     if rank == 0:
         cpu = None
@@ -278,9 +315,14 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "stage_kernel<4>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
+                         "kernel": "stage_kernel<4,double>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+            "mixed": {"value": value_mixed, "unit": UNIT, "ms_per_step": ms_mixed / args.steps,
+                      "speedup_vs_fp64": value_mixed / value, "stage_kernel_ms": stage_ms_mixed,
+                      "trace_kernel_ms": trace_ms_mixed,
+                      "dtype": "f32 contractions/fluxes, f64 geometry/inverse mass/RK state",
+                      "accuracy": acc},
             "clocks": clocks,
         }
         if cpu:
@@ -296,6 +338,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 accuracy check (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     globals()["N_EL"] = args.nel

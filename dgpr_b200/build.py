@@ -11,7 +11,7 @@ LIB = os.path.join(HERE, "_lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "--expt-relaxed-constexpr"]
-SOURCES = ["host.cpp", "io.cpp", "capi.cu", "kernels_fp64.cu", "mixed.cu"]
+SOURCES = ["host.cpp", "io.cpp", "capi.cu", "kernels_fp64.cu", "kernels_fp32.cu"]
 
 
 def _nvcc():
@@ -22,13 +22,7 @@ def _nvcc():
 
 
 def sources():
-    out = []
-    for s in SOURCES:
-        path = os.path.join(CSRC, s)
-        if not os.path.exists(path) and s == "mixed.cu":
-            path = os.path.join(CSRC, "mixed_stub.cu")
-        out.append(path)
-    return out
+    return [os.path.join(CSRC, s) for s in SOURCES]
 
 
 def build(verbose=False, jobs=None):

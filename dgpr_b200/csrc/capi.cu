@@ -11,7 +11,6 @@
 #include "../../include/dgb200.h"
 #include "host.hpp"
 #include "kernels.hpp"
-#include "mixed.hpp"
 
 using namespace dgb;
 
@@ -28,12 +27,13 @@ struct dgb_handle {
   DevParams dprm{};
   Ops1D ops;
   double* d_ops = nullptr;
+  float* d_opsf = nullptr;    // operator table for the mixed form
   double* d_geo = nullptr;
   int* d_nbr = nullptr;
   double* d_U = nullptr;      // resident state
   double* d_Us = nullptr;     // stage state
   double* d_acc = nullptr;    // RK4 accumulator
-  double* d_trace[3] = {nullptr, nullptr, nullptr};  // face traces, rotated between stages
+  void* d_trace[3] = {nullptr, nullptr, nullptr};  // face traces (compute type), rotated between stages
   double* d_in = nullptr;     // residual API input / output
   double* d_f = nullptr;
   double* d_R = nullptr;
@@ -47,7 +47,6 @@ struct dgb_handle {
   double graph_dt = 0.;
   long long launches_per_step = 0;
   long long last_launches = 0;
-  MixedState* mixed = nullptr;
 };
 
 namespace {
@@ -72,12 +71,14 @@ int cuda_fail(cudaError_t e, const char* what)
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
 
-Fp64Launch fp64_launch(const dgb_handle* h)
+KLaunch klaunch(const dgb_handle* h)
 {
-  Fp64Launch L;
+  KLaunch L;
   L.P = h->P;
+  L.precision = h->precision;
   L.E = h->E;
-  L.ops = h->d_ops;
+  L.ops = h->precision == DGB_MIXED_FP32 ? (const void*)h->d_opsf : (const void*)h->d_ops;
+  L.opsd = h->d_ops;
   L.geo = h->d_geo;
   L.nbr = h->d_nbr;
   L.prm = h->dprm;
@@ -96,8 +97,7 @@ StageArgs stage_args(int mode, double dt)
 // one residual of Uin (device) into f / R (device), on the handle's stream
 int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
 {
-  if (h->precision == DGB_MIXED_FP32) return mixed_residual(h->mixed, Uin, R, f, h->stream);
-  const Fp64Launch L = fp64_launch(h);
+  const KLaunch L = klaunch(h);
   CK(launch_trace(L, Uin, h->d_trace[0], h->stream));
   StageArgs a = stage_args(MODE_RESIDUAL, 0.);
   a.fout = f;
@@ -112,8 +112,7 @@ int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
 // their traces from the epilogue of the stage before.
 int enqueue_initial_traces(dgb_handle* h)
 {
-  if (h->precision == DGB_MIXED_FP32) return mixed_initial_traces(h->mixed, h->d_U, h->stream);
-  CK(launch_trace(fp64_launch(h), h->d_U, h->d_trace[0], h->stream));
+  CK(launch_trace(klaunch(h), h->d_U, h->d_trace[0], h->stream));
   return DGB_OK;
 }
 
@@ -126,10 +125,7 @@ int enqueue_initial_traces(dgb_handle* h)
 // last one (per-kernel timing by dgb_profile_step).
 int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr)
 {
-  if (h->precision == DGB_MIXED_FP32)
-    return mixed_step(h->mixed, scheme, dt, h->d_U, h->d_Us, h->d_acc, h->d_part, h->d_norms,
-                      h->d_counter, h->d_flag, h->stream, ev);
-  const Fp64Launch L = fp64_launch(h);
+  const KLaunch L = klaunch(h);
   const int nst = scheme == DGB_RK4 ? 4 : 3;
   const int modes4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
   const int modes3[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
@@ -145,7 +141,7 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     a.part = s == 0 ? h->d_part : nullptr;
     a.flag = h->d_flag;
     a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
-    const double* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
+    const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
     CK(launch_stage(L, in, tin, a, h->stream));
     if (s == 0) {
@@ -158,20 +154,16 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
   return DGB_OK;
 }
 
-long long launches_per_step(const dgb_handle* h, int scheme)
-{
-  const int nst = scheme == DGB_RK4 ? 4 : 3;
-  return h->precision == DGB_MIXED_FP32 ? mixed_launches_per_step(h->mixed, nst) : nst + 1;
-}
+long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == DGB_RK4 ? 4 : 3) + 1; }
 
 void free_all(dgb_handle* h)
 {
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->d_ops, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0], h->d_trace[1],
-                  h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms, h->d_counter, h->d_flag};
+  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
+                  h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
+                  h->d_counter, h->d_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  if (h->mixed) mixed_destroy(h->mixed);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -265,7 +257,8 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMalloc(&h->d_U, sb));
   CKF(cudaMalloc(&h->d_Us, sb));
   CKF(cudaMalloc(&h->d_acc, sb));
-  for (int t = 0; t < 3; ++t) CKF(cudaMalloc(&h->d_trace[t], sizeof(double) * (size_t)h->E * 60 * h->NQF));
+  for (int t = 0; t < 3; ++t)
+    CKF(cudaMalloc(&h->d_trace[t], trace_elem_bytes(precision) * (size_t)h->E * 60 * h->NQF));
   CKF(cudaMalloc(&h->d_part, sizeof(double) * (size_t)h->E));
   CKF(cudaMalloc(&h->d_counter, sizeof(int)));
   CKF(cudaMalloc(&h->d_flag, sizeof(int)));
@@ -276,15 +269,11 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMemset(h->d_counter, 0, sizeof(int)));
   CKF(cudaMemset(h->d_flag, 0, sizeof(int)));
   if (precision == DGB_MIXED_FP32) {
-    rc = mixed_create(&h->mixed, h->ops, geo, h->d_geo, h->d_nbr, h->E, h->dprm);
-    if (rc) {
-      free_all(h);
-      delete h;
-      return fail(rc, "mixed-precision setup failed");
-    }
-  } else {
-    CKF(prepare_fp64_kernels(h->P));
+    std::vector<float> tf(table.begin(), table.end());
+    CKF(cudaMalloc(&h->d_opsf, sizeof(float) * tf.size()));
+    CKF(cudaMemcpy(h->d_opsf, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
   }
+  CKF(prepare_kernels(h->P, precision));
 #undef CKF
   *out = h;
   return DGB_OK;

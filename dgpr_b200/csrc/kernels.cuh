@@ -1,0 +1,749 @@
+// Residual / RK-stage kernels for affine hexahedral elements, templated on the
+// polynomial size P = p + 1 and on the compute type T of the residual:
+//   T = double : the plain FP64 form
+//   T = float  : the mixed form -- contractions, traces and the pointwise
+//                Roe / viscous fluxes in FP32; the inverse mass matrix, the RK
+//                update and the state in HBM stay FP64
+//
+// One CTA per element.  The tensor-product structure of the basis (equispaced
+// Lagrange, basis.cpp:64-170) and of the quadrature (P Gauss points per
+// direction, geometry_common.cpp:176-177) is used throughout: every
+// interpolation / projection is a sequence of 1D P x P contractions on
+// shared-memory element tiles (sum factorisation), never the dense nb x nqv
+// tables the reference streams from HBM.
+//
+// Pipeline (state layout U[e][r][b], the reference's):
+//   trace_kernel : U -> face traces T[e][lf][10][P*P] (5 conserved values and
+//                  the viscous normal flux A(U, grad U).n_out at every face
+//                  quadrature point); once per dgb_step call
+//   stage_kernel : U_s, T_s -> R (volume + source + faces), f = -Minv R, the
+//                  RK update U_{s+1}, and in its epilogue the traces T_{s+1}
+//                  of U_{s+1} for the next stage; one launch per RK stage
+// The face kernel of the reference (solve.cpp:393-794) is folded into the
+// stage kernel: each element evaluates its own six faces from its own traces
+// and its neighbours' traces, so no per-face residual slots are written
+// (the reference's FACERESID gather, solve_cuda.cu:1192-1210).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+#include "physics.cuh"
+
+#ifndef DGB_STAGE_REGS
+#define DGB_STAGE_REGS 96
+#endif
+
+namespace dgb {
+
+// ------------------------------------------------------------ configuration
+
+template <int P>
+struct Cfg {
+  static constexpr int NB = P * P * P;  // nodes = volume quadrature points
+  static constexpr int NQF = P * P;     // face quadrature points
+  static constexpr int NH = 3 * NQF;    // face points of half an element (3 faces)
+  static constexpr int NT = (((NB > NH ? NB : NH) + 31) / 32) * 32;
+  // resident CTAs per SM the stage kernel is compiled for: caps registers at
+  // about DGB_STAGE_REGS per thread so occupancy is not register-limited
+  static constexpr int MINB_RAW = 65536 / (NT * DGB_STAGE_REGS);
+  static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW);
+  // operator table: B Bd Dq M1i K (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2]
+  static constexpr int oB = 0, oBd = P * P, oDq = 2 * P * P, oMi = 3 * P * P, oK = 4 * P * P;
+  static constexpr int oE = 5 * P * P, oD = oE + 2 * P, oWb = oD + 2 * P, oW = oWb + P;
+  static constexpr int oC = oW + P;
+  static constexpr int OPS = oC + 2;
+};
+
+constexpr int align16(int bytes) { return (bytes + 15) & ~15; }
+
+// ------------------------------------------------------------ index helpers
+
+// node index from the coordinate along face axis a and the two tangential
+// coordinates (t1 < t2 in axis order: x faces (y,z), y faces (x,z), z faces (x,y))
+template <int P>
+__device__ __forceinline__ int face_node(int a, int ia, int t1, int t2)
+{
+  return a == 0 ? ia + P * (t1 + P * t2) : a == 1 ? t1 + P * (ia + P * t2) : t1 + P * (t2 + P * ia);
+}
+
+// one output point o of a 1D contraction along axis AX for all 5 variables:
+//   out[r][o] (+)= scale * sum_k M(a, k) in[r][o with coordinate AX replaced by k]
+// M(a,k) = Mat[a*P+k], or Mat[k*P+a] when TR.
+template <int P, int AX, bool TR, bool ACC, class T>
+__device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in, T* out, int o,
+                                         T scale = T(1))
+{
+  constexpr int NB = P * P * P;
+  constexpr int S = AX == 0 ? 1 : (AX == 1 ? P : P * P);
+  const int a = (o / S) % P;
+  const int base = o - a * S;
+  T m[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    T s = T(0);
+#pragma unroll
+    for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
+    s *= scale;
+    out[r * NB + o] = ACC ? out[r * NB + o] + s : s;
+  }
+}
+
+// same, result returned in registers
+template <int P, int AX, bool TR, class T>
+__device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T* in, int o, T* res)
+{
+  constexpr int NB = P * P * P;
+  constexpr int S = AX == 0 ? 1 : (AX == 1 ? P : P * P);
+  const int a = (o / S) % P;
+  const int base = o - a * S;
+  T m[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    T s = T(0);
+#pragma unroll
+    for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
+    res[r] = s;
+  }
+}
+
+// Dual-consistency test coefficients of one face point: with
+// dc = A(S, d n^T) (solve.cpp:509-546, 720-741) the face term -grad(phi) . dc fJ w
+// becomes sum_i d(phi)/d(xi_i) b_i with b_i = -fw sum_c Jinv[i][c] dc[c].
+// Written for variables 1..4 (dc has no mass component): fb[(i*4 + r-1)*stride].
+template <class T>
+__device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, const T* n, T mu, const T* Ji,
+                                                     T fw, T* fb, int stride)
+{
+  const T lam = -(T(2) / T(3)) * mu;
+  const T ir = T(1) / S[0];
+  const T vel[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
+  T a[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) a[i] = (d[1 + i] - d[0] * vel[i]) * ir;
+  const T an = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+  T tau[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) tau[k][c] = mu * (a[k] * n[c] + a[c] * n[k]) + (k == c ? lam * an : T(0));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T en = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T m = Ji[3 * i] * tau[k][0] + Ji[3 * i + 1] * tau[k][1] + Ji[3 * i + 2] * tau[k][2];
+      fb[(i * 4 + k) * stride] = -fw * m;
+      en += vel[k] * m;
+    }
+    fb[(i * 4 + 3) * stride] = -fw * en;
+  }
+}
+
+// ------------------------------------------------------------- face traces
+
+// Traces of a nodal state sUx[5][NB] (shared memory) on the three faces
+// lf = 3*half + j, j < 3: at every face quadrature point the 5 conserved values
+// and the viscous normal flux A(U, grad U).n_out, written to
+// Te[(lf*10 + r)*NQF + fq] (Te = this element's slice of the trace buffer).
+// Threads tid < 3*NQF each own one face point.  Scratch: sN[3][10][NQF],
+// sY[3][15][NQF].  Both the trace kernel and the stage kernel's epilogue call
+// this, so a trace is bit-identical whichever of them produced it.
+// sg: element geometry record in T (Jinv, detJ, normals, surface Jacobians).
+template <int P, class T>
+__device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY, const T* so, const T* sg,
+                                           T mu, T* __restrict__ Te)
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NH;
+  const int tid = threadIdx.x;
+  const T* B = so + C::oB;
+  const T* Bd = so + C::oBd;
+  if (tid < NH) {  // along the face normal: value and normal derivative
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P;
+    const int a = lf >> 1, end = lf & 1;
+    const T* Ev = so + C::oE + end * P;
+    const T* Dv = so + C::oD + end * P;
+    T* out = sN + j * 10 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      T v = T(0), dn = T(0);
+#pragma unroll
+      for (int ia = 0; ia < P; ++ia) {
+        const T u = sUx[r * NB + face_node<P>(a, ia, t1, t2)];
+        v = fma(Ev[ia], u, v);
+        dn = fma(Dv[ia], u, dn);
+      }
+      out[r * NQF + fq] = v;
+      out[(5 + r) * NQF + fq] = dn;
+    }
+  }
+  __syncthreads();
+  if (tid < NH) {  // first tangential direction (index q1 = fq % P)
+    const int j = tid / NQF, fq = tid % NQF, q1 = fq % P, t2 = fq / P;
+    const T* in = sN + j * 10 * NQF;
+    T* out = sY + j * 15 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      T yv = T(0), yd = T(0), yn = T(0);
+#pragma unroll
+      for (int t1 = 0; t1 < P; ++t1) {
+        const T v = in[r * NQF + t1 + P * t2];
+        yv = fma(B[q1 * P + t1], v, yv);
+        yd = fma(Bd[q1 * P + t1], v, yd);
+        yn = fma(B[q1 * P + t1], in[(5 + r) * NQF + t1 + P * t2], yn);
+      }
+      out[r * NQF + fq] = yv;
+      out[(5 + r) * NQF + fq] = yd;
+      out[(10 + r) * NQF + fq] = yn;
+    }
+  }
+  __syncthreads();
+  if (tid < NH) {  // second tangential direction, physical gradient, A(U, grad U).n
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+    const T* in = sY + j * 15 * NQF;
+    T S[5], g[3][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      T v = T(0), d1 = T(0), d2 = T(0), dn = T(0);
+#pragma unroll
+      for (int t2 = 0; t2 < P; ++t2) {
+        const T bv = B[q2 * P + t2], bd = Bd[q2 * P + t2];
+        const T yv = in[r * NQF + q1 + P * t2];
+        v = fma(bv, yv, v);
+        d2 = fma(bd, yv, d2);
+        d1 = fma(bv, in[(5 + r) * NQF + q1 + P * t2], d1);
+        dn = fma(bv, in[(10 + r) * NQF + q1 + P * t2], dn);
+      }
+      S[r] = v;
+      g[0][r] = a == 0 ? dn : d1;
+      g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
+      g[2][r] = a == 2 ? dn : d2;
+    }
+    T Qn[5] = {T(0), T(0), T(0), T(0), T(0)};
+    if (mu != T(0)) {
+      const T* Ji = sg + kGeoJinv;
+      T G[3][5], Q[3][5];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) G[c][r] = Ji[c] * g[0][r] + Ji[3 + c] * g[1][r] + Ji[6 + c] * g[2][r];
+      visc_flux(S, G, mu, Q);
+      const T* n = sg + kGeoN + 3 * lf;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
+    }
+    T* Tq = Te + lf * 10 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      Tq[r * NQF + fq] = S[r];
+      Tq[(5 + r) * NQF + fq] = Qn[r];
+    }
+  }
+}
+
+template <int P, class T>
+struct TraceSmem {
+  using C = Cfg<P>;
+  static constexpr int oOps = 0;
+  static constexpr int oGeo = align16(C::OPS * (int)sizeof(T));
+  static constexpr int oU = oGeo + align16(kGeoStride * (int)sizeof(T));
+  static constexpr int oN = oU + align16(5 * C::NB * (int)sizeof(T));
+  static constexpr int oY = oN + align16(30 * C::NQF * (int)sizeof(T));
+  static constexpr int TOTAL = oY + align16(45 * C::NQF * (int)sizeof(T));
+};
+
+// Face traces of U (FP64 in HBM) into Tr[e][lf][10][P*P] (type T).
+template <int P, class T>
+__global__ void __launch_bounds__(Cfg<P>::NT)
+trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, const double* __restrict__ geo,
+             T* __restrict__ Tr, DevParams prm)
+{
+  using C = Cfg<P>;
+  using L = TraceSmem<P, T>;
+  constexpr int NB = C::NB, NQF = C::NQF;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw + L::oOps);
+  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
+  T* sU = reinterpret_cast<T*>(smraw + L::oU);
+  T* sN = reinterpret_cast<T*>(smraw + L::oN);
+  T* sY = reinterpret_cast<T*>(smraw + L::oY);
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
+  const double* Ue = U + e * 5 * NB;
+  for (int i = tid; i < 5 * NB; i += blockDim.x) sU[i] = T(Ue[i]);
+  __syncthreads();
+  T* Te = Tr + e * 60 * NQF;
+  trace_half<P, T>(0, sU, sN, sY, so, sg, T(prm.mu), Te);
+  trace_half<P, T>(1, sU, sN, sY, so, sg, T(prm.mu), Te);
+}
+
+// ------------------------------------------------------------- stage kernel
+//
+// Shared memory: [operators (T) | inverse 1D mass matrix (FP64) | element
+// geometry (T) | misc] followed by one scratch region reused by the phases:
+//   volume  V0[5NB] V1[5NB] G[3][5][NB]                               (T)
+//   faces   (three faces at a time)                                    (T)
+//           Fa[3][5][NQF]   face flux coefficient of phi (then times fJ w)
+//           Fb[3][12][NQF]  reference-space coefficient of grad phi, vars 1..4
+//           Fz[3][4][NQF]   BR2 lifting source, vars 1..4 (var 0 has no viscous flux)
+//           Fz2[3][4][NQF]  after the first lifting direction
+//           Su[3][13][NQF]  test functions after the first tangential direction
+//           Sc[3][9][NQF]   after the second (aliases Fb)
+//   minv    M0[5NB] M1[5NB]                                            (FP64)
+//   traces  sN[3][10][NQF] sY[3][15][NQF] of the new state, which sits at oTrU (T)
+// The residual of the thread's own node stays in registers until the inverse
+// mass matrix is applied.
+template <int P, class T>
+struct StageSmem {
+  using C = Cfg<P>;
+  static constexpr int NB = C::NB, NQF = C::NQF;
+  static constexpr int ST = (int)sizeof(T), SD = (int)sizeof(double);
+  static constexpr int oOps = 0;
+  static constexpr int oMi = align16(C::OPS * ST);
+  static constexpr int oGeo = oMi + align16(P * P * SD);
+  static constexpr int oMisc = oGeo + align16(kGeoStride * ST);
+  static constexpr int oX = oMisc + align16(8 * ST);
+  static constexpr int VOL = 25 * NB * ST;
+  static constexpr int FACE = 3 * (5 + 12 + 4 + 4 + 13) * NQF * ST;
+  static constexpr int MINV = 10 * NB * SD;
+  static constexpr int RED = C::NT * SD;
+  // byte offset of the new state inside the scratch: after the trace buffers
+  // and clear of M0/M1, which are still being read when it is written
+  static constexpr int oTrU = align16(75 * NQF * ST) > MINV ? align16(75 * NQF * ST) : MINV;
+  static constexpr int TRACE = oTrU + 5 * NB * ST;
+  static constexpr int X0 = VOL > FACE ? VOL : FACE;
+  static constexpr int X1 = MINV > RED ? MINV : RED;
+  static constexpr int X2 = X0 > X1 ? X0 : X1;
+  static constexpr int X = X2 > TRACE ? X2 : TRACE;
+  static constexpr int TOTAL = oX + align16(X);
+  static_assert(oTrU >= MINV, "epilogue state must not overlap the inverse-mass buffers");
+};
+
+template <int P, class T>
+__global__ void __launch_bounds__(Cfg<P>::NT, Cfg<P>::MINB)
+stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __restrict__ opsg,
+             const double* __restrict__ opsd, const double* __restrict__ geo, const int* __restrict__ nbr,
+             DevParams prm, StageArgs sa)
+{
+  using C = Cfg<P>;
+  using L = StageSmem<P, T>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NH;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw + L::oOps);
+  double* sMi = reinterpret_cast<double*>(smraw + L::oMi);
+  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
+  T* sMisc = reinterpret_cast<T*>(smraw + L::oMisc);
+  unsigned char* sXb = smraw + L::oX;
+  T* sX = reinterpret_cast<T*>(sXb);
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  const bool node = tid < NB;  // thread owns node / volume point `tid`
+
+  T* V0 = sX;
+  T* V1 = sX + 5 * NB;
+  T* G = sX + 10 * NB;
+  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
+  for (int i = tid; i < P * P; i += blockDim.x) sMi[i] = opsd[C::oMi + i];
+  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
+  const double* Ue = Us + e * 5 * NB;
+  for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = T(Ue[i]);
+  __syncthreads();
+
+  const T* B = so + C::oB;
+  const T* Bd = so + C::oBd;
+  const T* Dq = so + C::oDq;
+  const double detJd = geo[e * kGeoStride + kGeoDetJ];
+  const T detJ = sg[kGeoDetJ];
+  const T* Ji = sg + kGeoJinv;
+  const T gamma = T(prm.gamma), mu = T(prm.mu);
+  T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // residual of node tid
+
+  // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
+  if (node) contract<P, 0, false, false>(B, V0, V1, tid);
+  __syncthreads();
+  if (node) contract<P, 1, false, false>(B, V1, V0, tid);
+  __syncthreads();
+  if (node) contract<P, 2, false, false>(B, V0, V1, tid);  // V1: values at quadrature points
+  __syncthreads();
+  if (node) {
+    contract<P, 0, false, false>(Dq, V1, G, tid);
+    contract<P, 1, false, false>(Dq, V1, G + 5 * NB, tid);
+    contract<P, 2, false, false>(Dq, V1, G + 10 * NB, tid);
+  }
+  __syncthreads();
+  if (node) {  // pointwise flux at quadrature point tid
+    const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+    const T* w = so + C::oW;
+    const T wJ = w[qx] * w[qy] * w[qz] * detJ;
+    T S[5], Gp[3][5], H[3][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      S[r] = V1[r * NB + tid];
+      const T g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Gp[c][r] = Ji[c] * g0 + Ji[3 + c] * g1 + Ji[6 + c] * g2;
+    }
+    euler_flux(S, gamma, H);
+    if (mu != T(0)) {
+      T Q[3][5];
+      visc_flux(S, Gp, mu, Q);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
+    }
+    // contravariant components scaled by the quadrature weight
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+        G[i * 5 * NB + r * NB + tid] = wJ * (Ji[3 * i] * H[0][r] + Ji[3 * i + 1] * H[1][r] + Ji[3 * i + 2] * H[2][r]);
+  }
+  __syncthreads();
+  if (node) {  // sum_i Dq_i^T Ghat_i
+    contract<P, 0, true, false>(Dq, G, V0, tid);
+    contract<P, 1, true, true>(Dq, G + 5 * NB, V0, tid);
+    contract<P, 2, true, true>(Dq, G + 10 * NB, V0, tid);
+  }
+  __syncthreads();
+  if (node) contract<P, 0, true, false>(B, V0, V1, tid);
+  __syncthreads();
+  if (node) contract<P, 1, true, false>(B, V1, V0, tid);
+  __syncthreads();
+  if (node) {
+    contract_reg<P, 2, true>(B, V0, tid, Rv);
+    const T* Wb = so + C::oWb;
+    const int ix = tid % P, iy = (tid / P) % P, iz = tid / (P * P);
+    const T ws = Wb[ix] * Wb[iy] * Wb[iz] * detJ;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Rv[r] -= T(prm.src[r]) * ws;
+  }
+  __syncthreads();
+
+  // ---------------- faces (solve.cpp:393-794), three at a time
+  T* Fa = sX;
+  T* Fb = Fa + 15 * NQF;
+  T* Fz = Fb + 36 * NQF;
+  T* Fz2 = Fz + 12 * NQF;
+  T* Su = Fz2 + 12 * NQF;
+  T* Sc = Fb;
+  const T* K = so + C::oK;
+  const T* w1 = so + C::oW;
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) {
+    if (tid < NH) {
+      const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
+      const T* n = sg + kGeoN + 3 * lf;
+      const T fw = sg[kGeoFJ + lf] * w1[q1] * w1[q2];
+      const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
+      T Uo[5], Qo[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        Uo[r] = To[r * NQF + fq];
+        Qo[r] = To[(5 + r) * NQF + fq];
+      }
+      const int nb = nbr[e * 6 + lf];
+      T* fa = Fa + j * 5 * NQF + fq;
+      T* fb = Fb + j * 12 * NQF + fq;
+      T* fz = Fz + j * 4 * NQF + fq;
+      if (nb >= 0) {
+        const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+        T Un[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
+        {
+          // Roe flux in one orientation for both sides: the element that sees
+          // the face on its high side is "left"
+          T F[5];
+          if (end) {
+            roe_flux(Uo, Un, n, gamma, F);
+          } else {
+            const T nn[3] = {-n[0], -n[1], -n[2]};
+            roe_flux(Un, Uo, nn, gamma, F);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) F[r] = -F[r];
+          }
+#pragma unroll
+          for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
+        }
+        if (mu != T(0)) {
+          T d[5];
+#pragma unroll
+          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - T(0.5) * (Uo[r] + Un[r]);  // Uo - Uhat
+          dual_consistency_ref(Uo, d, n, mu, Ji, fw, fb, NQF);
+#pragma unroll
+          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
+          T ro[5], rn[5];
+          visc_jump_n(Uo, d, n, mu, ro);  // BR2 lifting sources of both sides
+          visc_jump_n(Un, d, n, mu, rn);
+          const T co = T(0.5) * fw * so[C::oC + end] / detJ;
+          const T cn = T(0.5) * fw * so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+#pragma unroll
+          for (int r = 1; r < 5; ++r) fz[(r - 1) * NQF] = co * ro[r] + cn * rn[r];
+        }
+        if (fq == 0) sMisc[j] = T(0.5);
+      } else {
+        T Ub[5];
+        const int bad = boundary_state(nb, Uo, n, prm, Ub);
+        if (bad && sa.flag) atomicOr(sa.flag, 2);
+        {
+          T F[5];
+          euler_flux_n(Ub, gamma, n, F);
+#pragma unroll
+          for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - Qo[r];
+        }
+        if (mu != T(0)) {
+          T d[5], rb[5];
+#pragma unroll
+          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ub[r];
+          dual_consistency_ref(Uo, d, n, mu, Ji, fw, fb, NQF);
+          visc_jump_n(Ub, d, n, mu, rb);
+          const T co = fw * so[C::oC + end] / detJ;
+#pragma unroll
+          for (int r = 1; r < 5; ++r) fz[(r - 1) * NQF] = co * rb[r];
+        }
+        if (fq == 0) sMisc[j] = T(1);
+      }
+      if (mu == T(0)) {
+#pragma unroll
+        for (int i = 0; i < 12; ++i) fb[i * NQF] = T(0);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) fz[r * NQF] = T(0);
+      }
+    }
+    __syncthreads();
+    if (tid < NH) {  // lifting operator, first face direction
+      const int j = tid / NQF, fq = tid % NQF, q1 = fq % P, q2 = fq / P;
+      const T* fz = Fz + j * 4 * NQF;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < P; ++k) s = fma(K[q1 * P + k], fz[v * NQF + k + P * q2], s);
+        Fz2[(j * 4 + v) * NQF + fq] = s;
+      }
+    }
+    __syncthreads();
+    if (tid < NH) {  // second direction; a = (F - Qhat.n) fJ w
+      const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P;
+      const T fw = sg[kGeoFJ + lf] * w1[q1] * w1[q2];
+      const T ef = T(prm.eta) * sMisc[j];
+      T* fa = Fa + j * 5 * NQF;
+      const T* fz2 = Fz2 + j * 4 * NQF;
+      fa[fq] *= fw;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < P; ++k) s = fma(K[q2 * P + k], fz2[v * NQF + q1 + P * k], s);
+        fa[(v + 1) * NQF + fq] = (fa[(v + 1) * NQF + fq] + ef * s) * fw;
+      }
+    }
+    __syncthreads();
+    if (tid < NH) {  // test functions, first tangential direction: items (j, t1, q2)
+      const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, t1 = fq % P, q2 = fq / P, a = lf >> 1;
+      const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+      const T* fa = Fa + j * 5 * NQF;
+      const T* fb = Fb + j * 12 * NQF;
+      T u1[5], u2[4], un[4];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) u1[r] = T(0);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) u2[r] = un[r] = T(0);
+#pragma unroll
+      for (int q1 = 0; q1 < P; ++q1) {
+        const int q = q1 + P * q2;
+        const T b = B[q1 * P + t1], bd = Bd[q1 * P + t1];
+        u1[0] = fma(b, fa[q], u1[0]);
+#pragma unroll
+        for (int r = 1; r < 5; ++r) {
+          u1[r] = fma(b, fa[r * NQF + q], u1[r]);
+          u1[r] = fma(bd, fb[(ax1 * 4 + r - 1) * NQF + q], u1[r]);
+          u2[r - 1] = fma(b, fb[(ax2 * 4 + r - 1) * NQF + q], u2[r - 1]);
+          un[r - 1] = fma(b, fb[(a * 4 + r - 1) * NQF + q], un[r - 1]);
+        }
+      }
+      T* su = Su + j * 13 * NQF;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) su[r * NQF + fq] = u1[r];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        su[(5 + r) * NQF + fq] = u2[r];
+        su[(9 + r) * NQF + fq] = un[r];
+      }
+    }
+    __syncthreads();
+    if (tid < NH) {  // second tangential direction: items (j, t1, t2)
+      const int j = tid / NQF, fq = tid % NQF, t1 = fq % P, t2 = fq / P;
+      const T* su = Su + j * 13 * NQF;
+      T c0[5], cn[4];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) c0[r] = T(0);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) cn[r] = T(0);
+#pragma unroll
+      for (int q2 = 0; q2 < P; ++q2) {
+        const int q = t1 + P * q2;
+        const T b = B[q2 * P + t2], bd = Bd[q2 * P + t2];
+        c0[0] = fma(b, su[q], c0[0]);
+#pragma unroll
+        for (int r = 1; r < 5; ++r) {
+          c0[r] = fma(b, su[r * NQF + q], c0[r]);
+          c0[r] = fma(bd, su[(4 + r) * NQF + q], c0[r]);
+          cn[r - 1] = fma(b, su[(8 + r) * NQF + q], cn[r - 1]);
+        }
+      }
+      T* sc = Sc + j * 9 * NQF;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) sc[r * NQF + fq] = c0[r];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) sc[(5 + r) * NQF + fq] = cn[r];
+    }
+    __syncthreads();
+    if (node) {  // scatter to the node through the normal-direction factors
+      const int ix = tid % P, iy = (tid / P) % P, iz = tid / (P * P);
+      const T* Ev = so + C::oE;
+      const T* Dv = so + C::oD;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int lf = 3 * half + j, a = lf >> 1, end = lf & 1;
+        const int ia = a == 0 ? ix : a == 1 ? iy : iz;
+        const int t1 = a == 0 ? iy : ix, t2 = a == 2 ? iy : iz;
+        const T ev = Ev[end * P + ia], dv = Dv[end * P + ia];
+        const T* sc = Sc + j * 9 * NQF + t1 + P * t2;
+        Rv[0] += ev * sc[0];
+#pragma unroll
+        for (int r = 1; r < 5; ++r) Rv[r] += ev * sc[r * NQF] + dv * sc[(4 + r) * NQF];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---------------- norm partial, f = -Minv R (solve.cpp:800-804) in FP64, RK update
+  if (sa.part) {  // sum of R^2 over the element, fixed order
+    double s = 0.;
+    if (node) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r) s += double(Rv[r]) * double(Rv[r]);
+    }
+    double* red = reinterpret_cast<double*>(sXb);
+    red[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.;
+      for (int i = 0; i < C::NT; ++i) t += red[i];
+      sa.part[e] = t;
+    }
+    __syncthreads();
+  }
+  double* M0 = reinterpret_cast<double*>(sXb);
+  double* M1 = M0 + 5 * NB;
+  if (node) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) M0[r * NB + tid] = double(Rv[r]);
+  }
+  __syncthreads();
+  if (node) contract<P, 0, false, false>(sMi, M0, M1, tid);
+  __syncthreads();
+  if (node) contract<P, 1, false, false>(sMi, M1, M0, tid);
+  __syncthreads();
+  T* sUn = reinterpret_cast<T*>(sXb + L::oTrU);  // new state for the epilogue traces
+  if (node) {
+    double f[5];
+    contract_reg<P, 2, false>(sMi, M0, tid, f);
+    const double sc = -1.0 / detJd;
+    const long base = e * 5 * NB;
+    const double dt = sa.dt;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const long i = base + r * NB + tid;
+      const double fr = f[r] * sc;
+      double un = 0.;
+      switch (sa.mode) {
+        case MODE_RESIDUAL:
+          sa.fout[i] = fr;
+          if (sa.Rout) sa.Rout[i] = double(Rv[r]);
+          break;
+        case MODE_RK4_0:
+          sa.acc[i] = fr;
+          un = sa.Ubase[i] + dt * fr * 0.5;
+          break;
+        case MODE_RK4_1:
+          sa.acc[i] = sa.acc[i] + 2. * fr;
+          un = sa.Ubase[i] + dt * fr * 0.5;
+          break;
+        case MODE_RK4_2:
+          sa.acc[i] = sa.acc[i] + 2. * fr;
+          un = sa.Ubase[i] + dt * fr;
+          break;
+        case MODE_RK4_3:
+          un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
+          break;
+        case MODE_TVD_0:
+          un = sa.Ubase[i] + dt * fr;
+          break;
+        case MODE_TVD_1:
+          un = 0.75 * sa.Ubase[i] + 0.25 * Ue[r * NB + tid] + 0.25 * dt * fr;
+          break;
+        case MODE_TVD_2:
+          un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * Ue[r * NB + tid] + (2. / 3.) * dt * fr;
+          break;
+      }
+      if (sa.mode != MODE_RESIDUAL) {
+        sa.Uout[i] = un;
+        sUn[r * NB + tid] = T(un);
+      }
+    }
+  }
+  // ---------------- face traces of the new state for the next stage
+  if (sa.Tnext) {
+    __syncthreads();
+    T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
+    trace_half<P, T>(0, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
+    trace_half<P, T>(1, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
+  }
+}
+
+// ------------------------------------------------------------ host launchers
+
+template <int P, class T>
+cudaError_t prepare_p()
+{
+  cudaError_t e = cudaFuncSetAttribute(trace_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TraceSmem<P, T>::TOTAL);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              StageSmem<P, T>::TOTAL);
+}
+
+template <int P, class T>
+cudaError_t launch_trace_p(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
+{
+  trace_kernel<P, T><<<(unsigned)L.E, Cfg<P>::NT, TraceSmem<P, T>::TOTAL, st>>>(
+      L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, reinterpret_cast<T*>(Tout), L.prm);
+  return cudaGetLastError();
+}
+
+template <int P, class T>
+cudaError_t launch_stage_p(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                           cudaStream_t st)
+{
+  stage_kernel<P, T><<<(unsigned)L.E, Cfg<P>::NT, StageSmem<P, T>::TOTAL, st>>>(
+      L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.nbr, L.prm,
+      sa);
+  return cudaGetLastError();
+}
+
+}  // namespace dgb

@@ -28,16 +28,18 @@ struct StageArgs {
   double* Uout;
   double* fout;
   double* Rout;
-  double* part;   // per-element sum of R^2 (stage 1 of a step), or null
-  int* flag;      // bit 1: non-finite norm, bit 2: inflow without a Mach root
-  double* Tnext;  // face traces of Uout for the next stage, or null
+  double* part;  // per-element sum of R^2 (stage 1 of a step), or null
+  int* flag;     // bit 1: non-finite norm, bit 2: inflow without a Mach root
+  void* Tnext;   // face traces of Uout for the next stage (compute type), or null
 };
 
-// everything the FP64 kernels read that does not change between stages
-struct Fp64Launch {
+// everything the kernels read that does not change between stages
+struct KLaunch {
   int P;
+  int precision;       // DGB_FP64 or DGB_MIXED_FP32
   long E;
-  const double* ops;   // packed 1D operator table (pack_ops)
+  const void* ops;     // packed 1D operator table in the compute type (pack_ops)
+  const double* opsd;  // the same table in FP64 (inverse mass matrix)
   const double* geo;   // [E][kGeoStride]
   const int* nbr;      // [E][6]
   DevParams prm;
@@ -45,15 +47,25 @@ struct Fp64Launch {
 
 int ops_table_size(int P);
 void pack_ops(const Ops1D& o, double* table);
-size_t stage_smem_bytes(int P);
+size_t trace_elem_bytes(int precision);  // bytes of one trace value
 
-cudaError_t prepare_fp64_kernels(int P);
+cudaError_t prepare_kernels(int P, int precision);
 // face traces T[E][6][10][P*P] of U
-cudaError_t launch_trace(const Fp64Launch& L, const double* U, double* Tout, cudaStream_t st);
+cudaError_t launch_trace(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
 // one stage: residual of Us with traces Tin, then sa.mode's update
-cudaError_t launch_stage(const Fp64Launch& L, const double* Us, const double* Tin, const StageArgs& sa,
+cudaError_t launch_stage(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                          cudaStream_t st);
 cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, int* counter,
                         int* flag, cudaStream_t st);
+
+// per compute type (kernels_fp64.cu / kernels_fp32.cu)
+cudaError_t prepare_fp64(int P);
+cudaError_t launch_trace_fp64(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
+cudaError_t launch_stage_fp64(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                              cudaStream_t st);
+cudaError_t prepare_fp32(int P);
+cudaError_t launch_trace_fp32(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
+cudaError_t launch_stage_fp32(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                              cudaStream_t st);
 
 }  // namespace dgb
