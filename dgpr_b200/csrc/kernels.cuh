@@ -33,6 +33,9 @@
 #ifndef DGB_STAGE_REGS
 #define DGB_STAGE_REGS 96
 #endif
+#ifndef DGB_STAGE_REGS_F32
+#define DGB_STAGE_REGS_F32 64
+#endif
 
 namespace dgb {
 
@@ -44,10 +47,6 @@ struct Cfg {
   static constexpr int NQF = P * P;     // face quadrature points
   static constexpr int NH = 3 * NQF;    // face points of half an element (3 faces)
   static constexpr int NT = (((NB > NH ? NB : NH) + 31) / 32) * 32;
-  // resident CTAs per SM the stage kernel is compiled for: caps registers at
-  // about DGB_STAGE_REGS per thread so occupancy is not register-limited
-  static constexpr int MINB_RAW = 65536 / (NT * DGB_STAGE_REGS);
-  static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW);
   // operator table: B Bd Dq M1i K (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2]
   static constexpr int oB = 0, oBd = P * P, oDq = 2 * P * P, oMi = 3 * P * P, oK = 4 * P * P;
   static constexpr int oE = 5 * P * P, oD = oE + 2 * P, oWb = oD + 2 * P, oW = oWb + P;
@@ -56,6 +55,16 @@ struct Cfg {
 };
 
 constexpr int align16(int bytes) { return (bytes + 15) & ~15; }
+
+// Resident CTAs per SM the stage kernel is compiled for: caps registers at
+// about DGB_STAGE_REGS (FP64) / DGB_STAGE_REGS_F32 (FP32) per thread so
+// occupancy is not register-limited.
+template <int P, class T>
+struct MinBlocks {
+  static constexpr int REGS = sizeof(T) == 8 ? DGB_STAGE_REGS : DGB_STAGE_REGS_F32;
+  static constexpr int RAW = 65536 / (Cfg<P>::NT * REGS);
+  static constexpr int value = RAW < 1 ? 1 : (RAW > 16 ? 16 : RAW);
+};
 
 // ------------------------------------------------------------ index helpers
 
@@ -280,8 +289,8 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
   for (int i = tid; i < 5 * NB; i += blockDim.x) sU[i] = T(Ue[i]);
   __syncthreads();
   T* Te = Tr + e * 60 * NQF;
-  trace_half<P, T>(0, sU, sN, sY, so, sg, T(prm.mu), Te);
-  trace_half<P, T>(1, sU, sN, sY, so, sg, T(prm.mu), Te);
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) trace_half<P, T>(half, sU, sN, sY, so, sg, T(prm.mu), Te);
 }
 
 // ------------------------------------------------------------- stage kernel
@@ -327,7 +336,7 @@ struct StageSmem {
 };
 
 template <int P, class T>
-__global__ void __launch_bounds__(Cfg<P>::NT, Cfg<P>::MINB)
+__global__ void __launch_bounds__(Cfg<P>::NT, (MinBlocks<P, T>::value))
 stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __restrict__ opsg,
              const double* __restrict__ opsd, const double* __restrict__ geo, const int* __restrict__ nbr,
              DevParams prm, StageArgs sa)
@@ -465,18 +474,18 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
         for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
         {
           // Roe flux in one orientation for both sides: the element that sees
-          // the face on its high side is "left"
-          T F[5];
-          if (end) {
-            roe_flux(Uo, Un, n, gamma, F);
-          } else {
-            const T nn[3] = {-n[0], -n[1], -n[2]};
-            roe_flux(Un, Uo, nn, gamma, F);
+          // the face on its high side is "left"; the other side negates it
+          T UL[5], UR[5], F[5];
+          const T sgn = end ? T(1) : T(-1);
 #pragma unroll
-            for (int r = 0; r < 5; ++r) F[r] = -F[r];
+          for (int r = 0; r < 5; ++r) {
+            UL[r] = end ? Uo[r] : Un[r];
+            UR[r] = end ? Un[r] : Uo[r];
           }
+          const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
+          roe_flux(UL, UR, nn, gamma, F);
 #pragma unroll
-          for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
+          for (int r = 0; r < 5; ++r) fa[r * NQF] = sgn * F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
         }
         if (mu != T(0)) {
           T d[5];
@@ -711,8 +720,8 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   if (sa.Tnext) {
     __syncthreads();
     T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
-    trace_half<P, T>(0, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
-    trace_half<P, T>(1, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) trace_half<P, T>(half, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
   }
 }
 

@@ -182,8 +182,7 @@ __device__ __forceinline__ void roe_flux(const T* Ul, const T* Ur, const T* n, T
 // solve.cpp:235-252).  Returns 1 when subsonic inflow has no non-negative
 // boundary Mach root (the reference aborts there on the host, :80-83).
 template <class T>
-__device__ __forceinline__ int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm,
-                                              T* Ub)
+__device__ __forceinline__ int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm, T* Ub)
 {
   const T gamma = T(prm.gamma), gm1 = gamma - T(1);
   const T u = UL[1] / UL[0], v = UL[2] / UL[0], w = UL[3] / UL[0];
