@@ -169,6 +169,8 @@ void free_all(dgb_handle* h)
 
 }  // namespace
 
+int dgb::set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
 extern "C" {
 
 const char* dgb_error_string(int status)

@@ -60,4 +60,7 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
 // Total conditions used by the subsonic inflow state (solve.cpp:167-175).
 void total_conditions(const dgb_params& prm, double* Tt, double* Pt);
 
+// Records msg as the calling thread's dgb_last_error_message and returns code.
+int set_last_error(int code, const std::string& msg);
+
 }  // namespace dgb

@@ -144,6 +144,25 @@ long long dgb_last_launch_count(const dgb_handle* h);
  * dgb_step. */
 int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk);
 
+/* One FP64 residual f = -Minv R of a device-resident state U_dev into f_dev
+ * (both caller-owned device arrays, layout U[e][r][b]), for callers that may
+ * not allocate GPU memory -- e.g. a host application that owns the device
+ * memory pool, or a solver that has claimed all of HBM for its own state.
+ * It calls no cudaMalloc / cudaFree: every intermediate (operator tables,
+ * element geometry, neighbour table, face traces, status word) lives in one
+ * file-scope device array of 32 MiB built into the library, which every GPU
+ * that loads the library holds until the process exits.  Meshes needing more
+ * scratch than that (about 4,000 elements at p = 3) are rejected with
+ * DGB_ERR_ARG and a message giving the size needed.
+ * The first call on each device looks up the array's device address (set-up);
+ * make that first call before any stream capture.  All calls share the array
+ * and it keeps the last call's contents: calls whose GPU work could overlap
+ * (different streams or host threads) race -- order them.  Synchronises
+ * `stream` (cudaStream_t as void*, NULL = legacy default) before returning.
+ * This entry point has no counterpart in the reference. */
+int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params* params, const double* U_dev,
+                         double* f_dev, void* stream);
+
 /* ---------------------------------------------------------------- host side
  * Host-only helpers (no GPU needed) that mirror the reference's setup
  * functions, for drivers and for checks. */
