@@ -6,6 +6,12 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
+// host + device: the kernels use these, and the host-side check hooks run the
+// same code on the CPU
+#define DGB_HD __host__ __device__ __forceinline__
+
 namespace dgb {
 
 struct DevParams {
@@ -16,7 +22,7 @@ struct DevParams {
 
 // F(U) . n for the Euler flux (flux.cpp:24-48).
 template <class T>
-__device__ __forceinline__ void euler_flux_n(const T* U, T gamma, const T* n, T* Fn)
+DGB_HD void euler_flux_n(const T* U, T gamma, const T* n, T* Fn)
 {
   const T r = U[0], ir = T(1) / r, u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
   const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
@@ -31,7 +37,7 @@ __device__ __forceinline__ void euler_flux_n(const T* U, T gamma, const T* n, T*
 
 // Full Euler flux, F[c][r] for direction c (flux.cpp:24-48).
 template <class T>
-__device__ __forceinline__ void euler_flux(const T* U, T gamma, T F[3][5])
+DGB_HD void euler_flux(const T* U, T gamma, T F[3][5])
 {
   const T r = U[0], ir = T(1) / r, u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
   const T p = (gamma - T(1)) * (U[4] - T(0.5) * r * (u * u + v * v + w * w));
@@ -52,7 +58,7 @@ __device__ __forceinline__ void euler_flux(const T* U, T gamma, T F[3][5])
 // Viscous (Stokes, no heat conduction) flux Q[c][r] = A(S, grad S)
 // (flux.cpp:156-202).  G[c][r] = d S_r / d x_c.
 template <class T>
-__device__ __forceinline__ void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
+DGB_HD void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -86,7 +92,7 @@ __device__ __forceinline__ void visc_flux(const T* S, const T G[3][5], T mu, T Q
 // 657-667).  With a_i = (d_{1+i} - d_0 vel_i) / rho the velocity gradient is
 // a n^T, so tau = mu (a n^T + n a^T) + lam (a.n) I.
 template <class T>
-__device__ __forceinline__ void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5])
+DGB_HD void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5])
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -112,7 +118,7 @@ __device__ __forceinline__ void visc_rank1(const T* S, const T* d, const T* n, T
 
 // A(S, d (x) n) . n, the normal component only.
 template <class T>
-__device__ __forceinline__ void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
+DGB_HD void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -135,7 +141,7 @@ __device__ __forceinline__ void visc_jump_n(const T* S, const T* d, const T* n, 
 
 // Roe flux with the entropy fix at 5% of the Roe sound speed (flux.cpp:56-154).
 template <class T>
-__device__ __forceinline__ void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
+DGB_HD void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
 {
   const T gm1 = g - T(1);
   const T rl = Ul[0], irl = T(1) / rl, ul = Ul[1] * irl, vl = Ul[2] * irl, wl = Ul[3] * irl;
@@ -182,7 +188,7 @@ __device__ __forceinline__ void roe_flux(const T* Ul, const T* Ur, const T* n, T
 // solve.cpp:235-252).  Returns 1 when subsonic inflow has no non-negative
 // boundary Mach root (the reference aborts there on the host, :80-83).
 template <class T>
-__device__ __forceinline__ int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm, T* Ub)
+DGB_HD int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm, T* Ub)
 {
   const T gamma = T(prm.gamma), gm1 = gamma - T(1);
   const T u = UL[1] / UL[0], v = UL[2] / UL[0], w = UL[3] / UL[0];

@@ -1,0 +1,130 @@
+"""The hand-written reverse mode of every pointwise function in the residual
+(Euler flux, viscous flux and its rank-one forms, Roe flux with entropy fix,
+wall ghost states) against central finite differences, on the CPU through the
+check hooks (include/dgb200_check.h).  Also pins the forward functions to the
+reference's own implementations where it is built here.
+
+Check: <ybar, (y(x + h v) - y(x - h v)) / 2h>  vs  <xbar, v>  with random v,
+ybar; relative tolerance 1e-7 (central differences at h = 1e-6 in FP64)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import dgpr_b200 as dg
+import oracle
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _fn():
+    f = dg.lib().dgb_check_pointwise
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+    return f
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+NOUT = {0: 15, 1: 5, 2: 15, 3: 15, 4: 5, 5: 5, 6: 5}
+NIN = {0: 5, 1: 5, 2: 20, 3: 10, 4: 10, 5: 10, 6: 5}
+
+
+def call(which, x, aux, ybar=None):
+    x = np.ascontiguousarray(x, np.float64)
+    aux = np.ascontiguousarray(aux, np.float64)
+    y = np.zeros(NOUT[which])
+    xbar = np.zeros(NIN[which])
+    rc = _fn()(which, _p(x), _p(np.ascontiguousarray(ybar, np.float64)) if ybar is not None else None, _p(aux),
+               _p(y), _p(xbar) if ybar is not None else None)
+    assert rc == 0, rc
+    return y, xbar
+
+
+def state(rng, rho=1.0, vel=0.3, p=0.8, g=1.4):
+    r = rho * (1 + 0.1 * rng.standard_normal())
+    v = vel * rng.standard_normal(3)
+    pp = p * (1 + 0.1 * rng.standard_normal())
+    return np.array([r, *(r * v), pp / (g - 1) + 0.5 * r * v @ v])
+
+
+def unit(rng):
+    n = rng.standard_normal(3)
+    return n / np.linalg.norm(n)
+
+
+def fd_check(which, x, aux, rng, h=1e-6, tol=1e-7):
+    ybar = rng.standard_normal(NOUT[which])
+    v = rng.standard_normal(NIN[which])
+    _, xbar = call(which, x, aux, ybar)
+    yp, _ = call(which, x + h * v, aux)
+    ym, _ = call(which, x - h * v, aux)
+    fd = ybar @ (yp - ym) / (2 * h)
+    an = xbar @ v
+    assert abs(fd - an) <= tol * max(1.0, abs(an), np.abs(ybar).max() * np.abs(yp - ym).max() / (2 * h)), (fd, an)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_euler_flux_vjp(seed):
+    rng = np.random.default_rng(seed)
+    fd_check(0, state(rng), [1.4], rng)
+    fd_check(1, state(rng), [1.4, *unit(rng)], rng)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_viscous_flux_vjp(seed):
+    rng = np.random.default_rng(100 + seed)
+    x = np.concatenate([state(rng), 0.5 * rng.standard_normal(15)])
+    fd_check(2, x, [0.01 + 0.01 * seed], rng)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_rank_one_viscous_vjps(seed):
+    rng = np.random.default_rng(200 + seed)
+    x = np.concatenate([state(rng), 0.1 * rng.standard_normal(5)])
+    aux = [0.02, *unit(rng)]
+    fd_check(3, x, aux, rng)
+    fd_check(4, x, aux, rng)
+
+
+@pytest.mark.parametrize("seed", range(16))
+def test_roe_vjp(seed):
+    rng = np.random.default_rng(300 + seed)
+    UL, UR = state(rng), state(rng)
+    if seed % 4 == 1:  # near-stagnant normal speed: the entropy fix on the contact wave
+        UL[1:4] *= 0.01
+        UR[1:4] *= 0.01
+    if seed % 4 == 2:  # supersonic
+        UL[1:4] *= 8.0
+        UR[1:4] *= 8.0
+        UL[4] += 0.5 * (UL[1:4] @ UL[1:4]) / UL[0] * 0.9
+        UR[4] += 0.5 * (UR[1:4] @ UR[1:4]) / UR[0] * 0.9
+    fd_check(5, np.concatenate([UL, UR]), [1.4, *unit(rng)], rng, h=1e-7, tol=2e-6)
+
+
+@pytest.mark.parametrize("bt", [-3, -4, -7])
+def test_wall_and_freestream_state_vjp(bt):
+    rng = np.random.default_rng(17)
+    aux = [bt, *unit(rng), 1.4, 287.0, 0.7, 0.9, 0.003, 1.0, 0.1, 0.0, 0.0, 1.8]
+    for _ in range(4):
+        fd_check(6, state(rng), aux, rng)
+
+
+def test_forward_pointwise_matches_reference():
+    ref = oracle.reference()
+    if ref is None:
+        pytest.skip("reference not built here")
+    rng = np.random.default_rng(5)
+    for _ in range(50):
+        UL, UR, n = state(rng), state(rng), unit(rng)
+        f, _ = call(5, np.concatenate([UL, UR]), [1.4, *n])
+        fr, _ = ref.roe(UL, UR, n, 1.4)
+        assert np.max(np.abs(f - fr)) <= 1e-14 * max(1, np.max(np.abs(fr)))
+        F, _ = call(0, UL, [1.4])
+        assert np.max(np.abs(F.reshape(3, 5) - ref.analytical_flux(UL, 1.4))) <= 1e-14 * np.max(np.abs(F))
+        G = 0.3 * rng.standard_normal(15)
+        Q, _ = call(2, np.concatenate([UL, G]), [0.02])
+        Qr = ref.A(UL, G[:5], G[5:10], G[10:], 0.02)
+        assert np.max(np.abs(Q.reshape(3, 5) - Qr)) <= 1e-14 * max(1, np.max(np.abs(Qr)))
