@@ -91,6 +91,22 @@ def lib():
             "dgb_last_launch_count": (ctypes.c_longlong, [vp]),
             "dgb_profile_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
                                                 ctypes.POINTER(ctypes.c_int)]),
+            "dgb_synchronize": (ctypes.c_int, [vp]),
+            "dgb_set_state_device": (ctypes.c_int, [vp, vp]),
+            "dgb_get_state_device": (ctypes.c_int, [vp, vp]),
+            "dgb_residual_vjp": (ctypes.c_int, [vp, _dp, _dp, _dp]),
+            "dgb_residual_vjp_device": (ctypes.c_int, [vp, vp, vp, vp]),
+            "dgb_step_vjp_device": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp]),
+            "dgb_forward_record": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong,
+                                                  ctypes.c_int, _dp]),
+            "dgb_backward": (ctypes.c_int, [vp, _dp, _dp]),
+            "dgb_backward_device": (ctypes.c_int, [vp, vp, vp]),
+            "dgb_adjoint_stats": (ctypes.c_int, [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3),
+            "dgb_checkpoint_plan": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int,
+                                                   ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong,
+                                                   ctypes.POINTER(ctypes.c_longlong),
+                                                   ctypes.POINTER(ctypes.c_longlong),
+                                                   ctypes.POINTER(ctypes.c_int)]),
             "dgb_gauss_legendre": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double, _dp, _dp]),
             "dgb_lagrange1d": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
             "dgb_lagrange1d_deriv": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
@@ -122,6 +138,24 @@ def _p(a):
 
 
 # ----------------------------------------------------------------- setup helpers
+
+
+def checkpoint_plan(nsteps, slots):
+    """The binomial checkpoint plan of dgb_forward_record / dgb_backward:
+    (ops, forward_steps, peak_slots) with ops a list of (kind, arg), kind
+    "forward" (arg steps), "store" / "restore" (arg buffer), "reverse" (arg
+    step index).  Host only."""
+    n = ctypes.c_longlong()
+    fw = ctypes.c_longlong()
+    pk = ctypes.c_int()
+    _check(lib().dgb_checkpoint_plan(int(nsteps), int(slots), None, 0, ctypes.byref(n), ctypes.byref(fw),
+                                     ctypes.byref(pk)))
+    buf = (ctypes.c_longlong * (2 * n.value))()
+    _check(lib().dgb_checkpoint_plan(int(nsteps), int(slots), buf, 2 * n.value, ctypes.byref(n),
+                                     ctypes.byref(fw), ctypes.byref(pk)))
+    kinds = ("forward", "store", "restore", "reverse")
+    ops = [(kinds[buf[2 * k]], buf[2 * k + 1]) for k in range(n.value)]
+    return ops, fw.value, pk.value
 
 def make_reference_state(gamma=1.4, gcnst=287.0, mu=1e-3, c=1.0, rho=1.0, u=0.1, v=0.0, w=0.0, eta=6.0,
                          source=(0.0, 0.0, 0.0, 0.0, 0.0)):
@@ -297,3 +331,55 @@ class Solver:
     @property
     def last_launch_count(self):
         return lib().dgb_last_launch_count(self.h)
+
+    def synchronize(self):
+        _check(lib().dgb_synchronize(self.h))
+
+    def set_state_device(self, U_ptr):
+        _check(lib().dgb_set_state_device(self.h, ctypes.c_void_p(U_ptr)))
+
+    def get_state_device(self, U_ptr):
+        _check(lib().dgb_get_state_device(self.h, ctypes.c_void_p(U_ptr)))
+
+    # ---- adjoint (no counterpart in the reference)
+
+    def residual_vjp(self, U, lam):
+        """(df/dU)^T lam at host state U, f = -Minv R(U)."""
+        U = np.ascontiguousarray(U, dtype=np.float64).ravel()
+        lam = np.ascontiguousarray(lam, dtype=np.float64).ravel()
+        out = np.zeros(self.n)
+        _check(lib().dgb_residual_vjp(self.h, _p(U), _p(lam), _p(out)))
+        return out
+
+    def residual_vjp_device(self, U_ptr, lam_ptr, out_ptr):
+        _check(lib().dgb_residual_vjp_device(self.h, ctypes.c_void_p(U_ptr), ctypes.c_void_p(lam_ptr),
+                                             ctypes.c_void_p(out_ptr)))
+
+    def step_vjp_device(self, scheme, dt, U_ptr, lam_ptr):
+        """Reverse of one RK step at device state U: lam (device) is the
+        adjoint of the stepped state on entry and of U on return."""
+        _check(lib().dgb_step_vjp_device(self.h, int(scheme), float(dt), ctypes.c_void_p(U_ptr),
+                                         ctypes.c_void_p(lam_ptr)))
+
+    def forward_record(self, scheme, dt, nsteps, slots, norms=True):
+        self.record_id = getattr(self, "record_id", 0) + 1
+        out = np.zeros(max(int(nsteps), 1))
+        _check(lib().dgb_forward_record(self.h, int(scheme), float(dt), int(nsteps), int(slots),
+                                        _p(out) if norms else None))
+        return out[:nsteps]
+
+    def backward(self, lamN):
+        lamN = np.ascontiguousarray(lamN, dtype=np.float64).ravel()
+        out = np.zeros(self.n)
+        _check(lib().dgb_backward(self.h, _p(lamN), _p(out)))
+        return out
+
+    def backward_device(self, lamN_ptr, out_ptr):
+        _check(lib().dgb_backward_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr)))
+
+    def adjoint_stats(self):
+        """(steps recomputed, steps reversed) by the last backward sweep and
+        the forward steps of the whole checkpoint plan."""
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().dgb_adjoint_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value

@@ -1,0 +1,86 @@
+"""torch.autograd wrappers over the adjoint entry points of the C ABI.
+
+`integrate(U0, solver, scheme, dt, nsteps, slots)` advances a device state
+(torch float64 CUDA tensor in the reference layout U[e][r][b]) by nsteps RK
+steps through dgb_forward_record; its backward is dgb_backward_device, the
+hand-written discrete adjoint with binomial checkpointing.  `residual(U,
+solver)` is f = -Minv R(U) with dgb_residual_vjp_device as its backward.
+
+Both run the native library only; there is no torch compute path.  A solver
+handle holds one recorded run at a time: calling `integrate` again on the same
+solver before the first result's backward makes that backward raise.
+"""
+import torch
+
+from . import DgbError, ERR_ARG
+
+__all__ = ["integrate", "residual"]
+
+
+def _dev_f64(t, n, what):
+    if not (t.is_cuda and t.dtype == torch.float64):
+        raise TypeError(f"{what} must be a float64 CUDA tensor")
+    if t.numel() != n:
+        raise ValueError(f"{what} has {t.numel()} values, the solver's state has {n}")
+    return t.contiguous()
+
+
+class _Integrate(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U0, solver, scheme, dt, nsteps, slots):
+        U0 = _dev_f64(U0, solver.n, "U0")
+        torch.cuda.current_stream().synchronize()
+        solver.set_state_device(U0.data_ptr())
+        solver.forward_record(scheme, dt, nsteps, slots, norms=False)
+        UN = torch.empty_like(U0)
+        solver.get_state_device(UN.data_ptr())
+        ctx.solver = solver
+        ctx.record_id = solver.record_id
+        return UN
+
+    @staticmethod
+    def backward(ctx, gUN):
+        solver = ctx.solver
+        if getattr(solver, "record_id", None) != ctx.record_id:
+            raise DgbError(ERR_ARG, "the solver recorded another run since this one; its adjoint is gone")
+        gUN = _dev_f64(gUN, solver.n, "grad")
+        torch.cuda.current_stream().synchronize()
+        g0 = torch.empty_like(gUN)
+        solver.backward_device(gUN.data_ptr(), g0.data_ptr())
+        return g0, None, None, None, None, None
+
+
+class _Residual(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U, solver):
+        U = _dev_f64(U, solver.n, "U")
+        torch.cuda.current_stream().synchronize()
+        f = torch.empty_like(U)
+        solver.residual_device(U.data_ptr(), 0, f.data_ptr())
+        solver.synchronize()
+        ctx.solver = solver
+        ctx.save_for_backward(U)
+        return f
+
+    @staticmethod
+    def backward(ctx, g):
+        (U,) = ctx.saved_tensors
+        solver = ctx.solver
+        g = _dev_f64(g, solver.n, "grad")
+        torch.cuda.current_stream().synchronize()
+        out = torch.empty_like(U)
+        solver.residual_vjp_device(U.data_ptr(), g.data_ptr(), out.data_ptr())
+        solver.synchronize()
+        return out, None
+
+
+def integrate(U0, solver, scheme, dt, nsteps, slots=None):
+    """U_N after nsteps RK steps from U0, differentiable in U0.  slots: number
+    of state checkpoints held on the device (default: every state)."""
+    return _Integrate.apply(U0, solver, int(scheme), float(dt), int(nsteps),
+                            int(slots if slots is not None else nsteps))
+
+
+def residual(U, solver):
+    """f = -Minv R(U), differentiable in U."""
+    return _Residual.apply(U, solver)

@@ -1,0 +1,382 @@
+// Adjoint entry points of the C ABI (include/dgb200.h): residual VJP, the
+// reverse of one RK step, and the recorded forward / backward pair with
+// binomial checkpointing.  The reference has no adjoint; these follow its
+// forward discretisation (solve.cpp:150-807, time_distributed.cpp:46-110).
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/dgb200.h"
+#include "adjoint.hpp"
+#include "handle.hpp"
+
+using namespace dgb;
+
+namespace {
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_status(e_, #call); \
+  } while (0)
+
+int fail(int code, const char* msg) { return set_last_error(code, msg); }
+
+// boundary states whose adjoint exists (freestream, walls); periodic sides
+// have none
+int check_bounds(const dgb_handle* h)
+{
+  for (int s = 0; s < 6; ++s)
+    if (h->bounds[s] == DGB_BT_SUBSONIC_INFLOW || h->bounds[s] == DGB_BT_SUBSONIC_OUTFLOW)
+      return fail(DGB_ERR_UNSUPPORTED, "the adjoint covers periodic, freestream and wall boundaries only");
+  return DGB_OK;
+}
+
+int ensure_adjoint(dgb_handle* h)
+{
+  if (h->d_adj_ta) return DGB_OK;
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  const size_t tr = sizeof(double) * (size_t)h->E * 60 * h->NQF;
+  cudaError_t e = cudaSuccess;
+  for (int b = 0; b < dgb_handle::ADJ_NBUF && e == cudaSuccess; ++b) e = cudaMalloc(&h->d_adj[b], sb);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_adj_tr, tr);
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_adj_ta, 2 * tr);
+  if (e == cudaSuccess) e = prepare_adjoint(h->P);
+  if (e != cudaSuccess) {
+    free_adjoint(h);
+    return cuda_status(e, "adjoint buffers");
+  }
+  return DGB_OK;
+}
+
+VjpScratch scratch(dgb_handle* h) { return {h->d_adj_tr, h->d_adj_ta, h->d_adj[dgb_handle::ADJ_PART], h->d_flag}; }
+
+VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const double* Y = nullptr,
+            double cz = 0., const double* Z = nullptr)
+{
+  VjpArgs v;
+  v.U = U;
+  v.X = X;
+  v.Y = Y;
+  v.Z = Z;
+  v.cx = cx;
+  v.cy = cy;
+  v.cz = cz;
+  v.a_out = nullptr;
+  v.acc_in = nullptr;
+  v.acc_out = nullptr;
+  return v;
+}
+
+// Reverse of one RK step from U_i (device, unchanged) with lam = adjoint of
+// U_{i+1} in, adjoint of U_i out (in place).  The stage states are recomputed
+// in the handle's precision, then one residual VJP per stage runs backwards.
+// With f = -Minv R, J_s = df/dU at stage state S_s and a_s = J_s^T (...):
+//   RK4   U1 = U + dt/2 k1, U2 = U + dt/2 k2, U3 = U + dt k3,
+//         U' = U + dt/6 (k1 + 2 k2 + 2 k3 + k4)
+//         a3 = J3^T (dt/6 lam)        a2 = J2^T (dt/3 lam + dt a3)
+//         a1 = J1^T (dt/3 lam + dt/2 a2)   a0 = J0^T (dt/6 lam + dt/2 a1)
+//   TVD   U1 = U + dt f(U), U2 = 3/4 U + 1/4 U1 + dt/4 f(U1),
+//         U' = 1/3 U + 2/3 U2 + 2/3 dt f(U2)  (time_distributed.cpp:79-110)
+//         a2 = J2^T (2/3 dt lam)      a1 = J1^T (dt/6 lam + dt/4 a2)
+//         a0 = J0^T (dt/6 lam + dt/4 a2 + dt a1)
+//   and in both  lam_i = lam + a0 + a1 + a2 (+ a3).
+// 3 (RK4) or 2 (TVD) stage launches + 1 trace launch, then 3 launches per VJP.
+int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl)
+{
+  const KLaunch L = klaunch(h);
+  double* S0 = h->d_adj[dgb_handle::ADJ_S0];
+  double* S1 = h->d_adj[dgb_handle::ADJ_S1];
+  double* S2 = h->d_adj[dgb_handle::ADJ_S2];
+  double* A0 = h->d_adj[dgb_handle::ADJ_A0];
+  double* A1 = h->d_adj[dgb_handle::ADJ_A1];
+  double* ACC = h->d_adj[dgb_handle::ADJ_ACC];
+  const VjpScratch sc = scratch(h);
+  CK(launch_trace(L, Ui, h->d_trace[0], h->stream));
+  if (scheme == DGB_RK4) {
+    const int modes[3] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2};
+    const double* in[3] = {Ui, S0, S1};
+    double* out[3] = {S0, S1, S2};
+    const int tin[3] = {0, 1, 0}, tout[3] = {1, 0, -1};
+    for (int s = 0; s < 3; ++s) {
+      StageArgs a = stage_args(modes[s], dt);
+      a.Ubase = Ui;
+      a.acc = h->d_acc;
+      a.Uout = out[s];
+      a.flag = h->d_flag;
+      a.Tnext = tout[s] >= 0 ? h->d_trace[tout[s]] : nullptr;
+      CK(launch_stage(L, in[s], h->d_trace[tin[s]], a, h->stream));
+    }
+    VjpArgs v = vjp(S2, dt / 6., lam);
+    v.a_out = A0;
+    v.acc_in = lam;
+    v.acc_out = ACC;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    v = vjp(S1, dt / 3., lam, dt, A0);
+    v.a_out = A0;
+    v.acc_in = ACC;
+    v.acc_out = ACC;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    v = vjp(S0, dt / 3., lam, dt / 2., A0);
+    v.a_out = A0;
+    v.acc_in = ACC;
+    v.acc_out = ACC;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    v = vjp(Ui, dt / 6., lam, dt / 2., A0);
+    v.acc_in = ACC;
+    v.acc_out = lam;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if (nl) *nl += 4 + 4 * 3;
+  } else {
+    const int modes[2] = {MODE_TVD_0, MODE_TVD_1};
+    const double* in[2] = {Ui, S0};
+    double* out[2] = {S0, S1};
+    for (int s = 0; s < 2; ++s) {
+      StageArgs a = stage_args(modes[s], dt);
+      a.Ubase = Ui;
+      a.Uout = out[s];
+      a.flag = h->d_flag;
+      a.Tnext = s == 0 ? h->d_trace[1] : nullptr;
+      CK(launch_stage(L, in[s], h->d_trace[s], a, h->stream));
+    }
+    VjpArgs v = vjp(S1, 2. * dt / 3., lam);
+    v.a_out = A0;
+    v.acc_in = lam;
+    v.acc_out = ACC;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    v = vjp(S0, dt / 6., lam, dt / 4., A0);
+    v.a_out = A1;
+    v.acc_in = ACC;
+    v.acc_out = ACC;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    v = vjp(Ui, dt / 6., lam, dt / 4., A0, dt, A1);
+    v.acc_in = ACC;
+    v.acc_out = lam;
+    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if (nl) *nl += 3 + 3 * 3;
+  }
+  return DGB_OK;
+}
+
+int read_flag(dgb_handle* h)
+{
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag & 8) return fail(DGB_ERR_UNSUPPORTED, "boundary state without an adjoint");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
+  return DGB_OK;
+}
+
+int copy_state(dgb_handle* h, double* dst, const double* src)
+{
+  if (dst == src) return DGB_OK;
+  CK(cudaMemcpyAsync(dst, src, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToDevice, h->stream));
+  return DGB_OK;
+}
+
+int check_scheme(int scheme, double dt)
+{
+  if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
+  if (!(dt == dt)) return fail(DGB_ERR_ARG, "dt is NaN");
+  return DGB_OK;
+}
+
+}  // namespace
+
+void dgb::free_adjoint(dgb_handle* h)
+{
+  for (double*& p : h->d_adj) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+  if (h->d_adj_tr) cudaFree(h->d_adj_tr);
+  if (h->d_adj_ta) cudaFree(h->d_adj_ta);
+  h->d_adj_tr = h->d_adj_ta = nullptr;
+  for (double* p : h->d_slots)
+    if (p) cudaFree(p);
+  h->d_slots.clear();
+  h->recorded = false;
+}
+
+extern "C" {
+
+int dgb_residual_vjp_device(dgb_handle* h, const double* U_dev, const double* lam_dev, double* Ubar_dev)
+{
+  if (!h || !U_dev || !lam_dev || !Ubar_dev) return fail(DGB_ERR_ARG, "null argument");
+  if (Ubar_dev == U_dev || Ubar_dev == lam_dev) return fail(DGB_ERR_ARG, "Ubar must not alias U or lam");
+  int rc = check_bounds(h);
+  if (rc) return rc;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_adjoint(h))) return rc;
+  VjpArgs v = vjp(U_dev, 1., lam_dev);
+  v.a_out = Ubar_dev;
+  CK(launch_residual_vjp(klaunch(h), v, scratch(h), h->stream));
+  h->last_launches = 3;
+  return DGB_OK;
+}
+
+int dgb_residual_vjp(dgb_handle* h, const double* U_host, const double* lam_host, double* Ubar_host)
+{
+  if (!h || !U_host || !lam_host || !Ubar_host) return fail(DGB_ERR_ARG, "null argument");
+  int rc = check_bounds(h);
+  if (rc) return rc;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_adjoint(h))) return rc;
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  double* in = h->d_adj[dgb_handle::ADJ_IN];
+  double* out = h->d_adj[dgb_handle::ADJ_OUT];
+  double* lam = h->d_adj[dgb_handle::ADJ_LAM];
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  CK(cudaMemcpyAsync(in, U_host, sb, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(lam, lam_host, sb, cudaMemcpyHostToDevice, h->stream));
+  VjpArgs v = vjp(in, 1., lam);
+  v.a_out = out;
+  CK(launch_residual_vjp(klaunch(h), v, scratch(h), h->stream));
+  h->last_launches = 3;
+  CK(cudaMemcpyAsync(Ubar_host, out, sb, cudaMemcpyDeviceToHost, h->stream));
+  return read_flag(h);
+}
+
+int dgb_step_vjp_device(dgb_handle* h, int scheme, double dt, const double* U_dev, double* lam_dev)
+{
+  if (!h || !U_dev || !lam_dev) return fail(DGB_ERR_ARG, "null argument");
+  if ((const double*)lam_dev == U_dev) return fail(DGB_ERR_ARG, "lam must not alias U");
+  int rc = check_scheme(scheme, dt);
+  if (rc) return rc;
+  if ((rc = check_bounds(h))) return rc;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_adjoint(h))) return rc;
+  for (int b = 0; b < dgb_handle::ADJ_NBUF; ++b)
+    if (U_dev == h->d_adj[b] || lam_dev == h->d_adj[b]) return fail(DGB_ERR_ARG, "argument aliases scratch");
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  long long nl = 0;
+  if ((rc = enqueue_reverse_step(h, scheme, dt, U_dev, lam_dev, &nl))) return rc;
+  h->last_launches = nl;
+  return read_flag(h);
+}
+
+int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, int slots,
+                       double* norms_host)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  int rc = check_scheme(scheme, dt);
+  if (rc) return rc;
+  if (nsteps < 1 || slots < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1 and slots >= 1");
+  if ((rc = check_bounds(h))) return rc;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_adjoint(h))) return rc;
+  h->recorded = false;
+  if (make_checkpoint_plan((long long)nsteps, slots, h->plan)) return fail(DGB_ERR_ARG, "bad checkpoint plan");
+  const int need = h->plan.slots;
+  while ((int)h->d_slots.size() > need) {
+    cudaFree(h->d_slots.back());
+    h->d_slots.pop_back();
+  }
+  while ((int)h->d_slots.size() < need) {
+    double* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(double) * (size_t)h->n));
+    h->d_slots.push_back(p);
+  }
+  unsigned long long done = 0;
+  long long launches = 0;
+  for (size_t k = 0; k < h->plan.first_reverse; ++k) {
+    const CkOp& op = h->plan.ops[k];
+    if (op.kind == CK_STORE) {
+      if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+    } else if (op.kind == CK_FORWARD) {
+      rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, norms_host ? norms_host + done : nullptr);
+      if (rc) return rc;
+      launches += h->last_launches;
+      done += (unsigned long long)op.arg;
+    } else {
+      return fail(DGB_ERR_ARG, "checkpoint plan restores during the forward run");
+    }
+  }
+  // work state is U_{N-1}: keep it, take the last step on the resident state
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_WORK], h->d_U))) return rc;
+  rc = dgb_step(h, scheme, dt, 1, norms_host ? norms_host + done : nullptr);
+  if (rc) return rc;
+  launches += h->last_launches;
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], h->d_U))) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  h->plan_pos = h->plan.first_reverse;
+  h->recorded = true;
+  h->rec_scheme = scheme;
+  h->rec_dt = dt;
+  h->rec_steps = nsteps;
+  h->last_launches = launches;
+  return DGB_OK;
+}
+
+int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
+{
+  if (!h || !lamN_dev || !lam0_dev) return fail(DGB_ERR_ARG, "null argument");
+  if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
+  CK(cudaSetDevice(h->device));
+  const int scheme = h->rec_scheme;
+  const double dt = h->rec_dt;
+  double* lam = h->d_adj[dgb_handle::ADJ_LAM];
+  int rc;
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  if ((rc = copy_state(h, lam, lamN_dev))) return rc;
+  if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
+  long long nl = 0, fwd = 0, rev = 0;
+  for (size_t k = h->plan_pos; k < h->plan.ops.size(); ++k) {
+    const CkOp& op = h->plan.ops[k];
+    switch (op.kind) {
+      case CK_REVERSE:
+        if ((rc = enqueue_reverse_step(h, scheme, dt, h->d_U, lam, &nl))) return rc;
+        ++rev;
+        break;
+      case CK_RESTORE:
+        if ((rc = copy_state(h, h->d_U, h->d_slots[op.arg]))) return rc;
+        break;
+      case CK_STORE:
+        if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+        break;
+      case CK_FORWARD:
+        // dgb_step clears the status word: keep what the reverse steps raised
+        if ((rc = read_flag(h))) return rc;
+        if ((rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, nullptr))) return rc;
+        nl += h->last_launches;
+        fwd += op.arg;
+        break;
+    }
+  }
+  if ((rc = copy_state(h, lam0_dev, lam))) return rc;
+  if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_FINAL]))) return rc;
+  h->last_launches = nl;
+  h->adj_forward_steps = fwd;
+  h->adj_reverse_steps = rev;
+  return read_flag(h);
+}
+
+int dgb_backward(dgb_handle* h, const double* lamN_host, double* lam0_host)
+{
+  if (!h || !lamN_host || !lam0_host) return fail(DGB_ERR_ARG, "null argument");
+  if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
+  CK(cudaSetDevice(h->device));
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  double* in = h->d_adj[dgb_handle::ADJ_IN];
+  double* out = h->d_adj[dgb_handle::ADJ_OUT];
+  CK(cudaMemcpyAsync(in, lamN_host, sb, cudaMemcpyHostToDevice, h->stream));
+  int rc = dgb_backward_device(h, in, out);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(lam0_host, out, sb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_adjoint_stats(const dgb_handle* h, long long* forward_steps, long long* reverse_steps,
+                      long long* planned_forward_steps)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (forward_steps) *forward_steps = h->adj_forward_steps;
+  if (reverse_steps) *reverse_steps = h->adj_reverse_steps;
+  if (planned_forward_steps) *planned_forward_steps = h->plan.forward_steps;
+  return DGB_OK;
+}
+
+}  // extern "C"

@@ -9,45 +9,11 @@
 #include <vector>
 
 #include "../../include/dgb200.h"
+#include "handle.hpp"
 #include "host.hpp"
 #include "kernels.hpp"
 
 using namespace dgb;
-
-struct dgb_handle {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int nx = 0, ny = 0, nz = 0, p = 0, q = 0, P = 0, NB = 0, NQF = 0;
-  long E = 0;
-  long long n = 0;  // doubles per state array
-  long long bounds[6] = {0, 0, 0, 0, 0, 0};
-  int precision = DGB_FP64;
-  dgb_params prm{};
-  DevParams dprm{};
-  Ops1D ops;
-  double* d_ops = nullptr;
-  float* d_opsf = nullptr;    // operator table for the mixed form
-  double* d_geo = nullptr;
-  int* d_nbr = nullptr;
-  double* d_U = nullptr;      // resident state
-  double* d_Us = nullptr;     // stage state
-  double* d_acc = nullptr;    // RK4 accumulator
-  void* d_trace[3] = {nullptr, nullptr, nullptr};  // face traces (compute type), rotated between stages
-  double* d_in = nullptr;     // residual API input / output
-  double* d_f = nullptr;
-  double* d_R = nullptr;
-  double* d_part = nullptr;
-  double* d_norms = nullptr;
-  int* d_counter = nullptr;
-  int* d_flag = nullptr;
-  unsigned long long norms_cap = 0;
-  cudaGraphExec_t graph = nullptr;
-  int graph_scheme = -1;
-  double graph_dt = 0.;
-  long long launches_per_step = 0;
-  long long last_launches = 0;
-};
 
 namespace {
 
@@ -70,29 +36,6 @@ int cuda_fail(cudaError_t e, const char* what)
     cudaError_t e_ = (call);                     \
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
-
-KLaunch klaunch(const dgb_handle* h)
-{
-  KLaunch L;
-  L.P = h->P;
-  L.precision = h->precision;
-  L.E = h->E;
-  L.ops = h->precision == DGB_MIXED_FP32 ? (const void*)h->d_opsf : (const void*)h->d_ops;
-  L.opsd = h->d_ops;
-  L.geo = h->d_geo;
-  L.nbr = h->d_nbr;
-  L.prm = h->dprm;
-  return L;
-}
-
-StageArgs stage_args(int mode, double dt)
-{
-  StageArgs a;
-  memset(&a, 0, sizeof a);
-  a.mode = mode;
-  a.dt = dt;
-  return a;
-}
 
 // one residual of Uin (device) into f / R (device), on the handle's stream
 int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
@@ -164,6 +107,7 @@ void free_all(dgb_handle* h)
                   h->d_counter, h->d_flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  free_adjoint(h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -312,6 +256,14 @@ int dgb_set_stream(dgb_handle* h, void* stream)
   return DGB_OK;
 }
 
+int dgb_synchronize(dgb_handle* h)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
 long long dgb_state_size(const dgb_handle* h) { return h ? h->n : -1; }
 
 long long dgb_last_launch_count(const dgb_handle* h) { return h ? h->last_launches : -1; }
@@ -330,6 +282,24 @@ int dgb_get_state(dgb_handle* h, double* U_host)
   if (!h || !U_host) return fail(DGB_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(U_host, h->d_U, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_set_state_device(dgb_handle* h, const double* U_dev)
+{
+  if (!h || !U_dev) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->d_U, U_dev, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_get_state_device(dgb_handle* h, double* U_dev)
+{
+  if (!h || !U_dev) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(U_dev, h->d_U, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return DGB_OK;
 }

@@ -1,0 +1,103 @@
+// The solver handle behind the opaque dgb_handle of the C ABI, shared by the
+// forward entry points (capi.cu) and the adjoint ones (adjoint_capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dgb200.h"
+#include "checkpoint.hpp"
+#include "host.hpp"
+#include "kernels.hpp"
+
+struct dgb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int nx = 0, ny = 0, nz = 0, p = 0, q = 0, P = 0, NB = 0, NQF = 0;
+  long E = 0;
+  long long n = 0;  // doubles per state array
+  long long bounds[6] = {0, 0, 0, 0, 0, 0};
+  int precision = DGB_FP64;
+  dgb_params prm{};
+  dgb::DevParams dprm{};
+  dgb::Ops1D ops;
+  double* d_ops = nullptr;
+  float* d_opsf = nullptr;    // operator table for the mixed form
+  double* d_geo = nullptr;
+  int* d_nbr = nullptr;
+  double* d_U = nullptr;      // resident state
+  double* d_Us = nullptr;     // stage state
+  double* d_acc = nullptr;    // RK4 accumulator
+  void* d_trace[3] = {nullptr, nullptr, nullptr};  // face traces (compute type), rotated between stages
+  double* d_in = nullptr;     // residual API input / output
+  double* d_f = nullptr;
+  double* d_R = nullptr;
+  double* d_part = nullptr;
+  double* d_norms = nullptr;
+  int* d_counter = nullptr;
+  int* d_flag = nullptr;
+  unsigned long long norms_cap = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_scheme = -1;
+  double graph_dt = 0.;
+  long long launches_per_step = 0;
+  long long last_launches = 0;
+
+  // ---- adjoint (allocated on first use, adjoint_capi.cu)
+  // state-sized buffers: stage states S0..S2, stage adjoints A0 A1, the
+  // adjoint accumulator, the volume part of a VJP, the adjoint being carried
+  // backwards, the state before the last recorded step and after it, and the
+  // residual-VJP API's input / output
+  enum { ADJ_S0, ADJ_S1, ADJ_S2, ADJ_A0, ADJ_A1, ADJ_ACC, ADJ_PART, ADJ_LAM, ADJ_WORK, ADJ_FINAL, ADJ_IN,
+         ADJ_OUT, ADJ_NBUF };
+  double* d_adj[ADJ_NBUF] = {};
+  double* d_adj_tr = nullptr;  // FP64 face traces [E][6][10][NQF]
+  double* d_adj_ta = nullptr;  // face-trace adjoints [E][6][20][NQF]
+  std::vector<double*> d_slots;  // checkpoints
+  dgb::CheckpointPlan plan;    // the recorded forward's plan
+  size_t plan_pos = 0;         // first op of the backward part
+  bool recorded = false;
+  int rec_scheme = DGB_RK4;
+  double rec_dt = 0.;
+  unsigned long long rec_steps = 0;
+  long long adj_forward_steps = 0;  // steps recomputed by the last dgb_backward
+  long long adj_reverse_steps = 0;
+};
+
+namespace dgb {
+
+inline KLaunch klaunch(const dgb_handle* h)
+{
+  KLaunch L;
+  L.P = h->P;
+  L.precision = h->precision;
+  L.E = h->E;
+  L.ops = h->precision == DGB_MIXED_FP32 ? (const void*)h->d_opsf : (const void*)h->d_ops;
+  L.opsd = h->d_ops;
+  L.geo = h->d_geo;
+  L.nbr = h->d_nbr;
+  L.prm = h->dprm;
+  return L;
+}
+
+inline StageArgs stage_args(int mode, double dt)
+{
+  StageArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.mode = mode;
+  a.dt = dt;
+  return a;
+}
+
+inline int cuda_status(cudaError_t e, const char* what)
+{
+  return set_last_error(DGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void free_adjoint(dgb_handle* h);
+
+}  // namespace dgb

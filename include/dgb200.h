@@ -102,6 +102,9 @@ int dgb_destroy(dgb_handle* h);
  * NULL = legacy default stream, the reference's only stream). */
 int dgb_set_stream(dgb_handle* h, void* stream);
 
+/* Waits for the work the handle has queued on its stream. */
+int dgb_synchronize(dgb_handle* h);
+
 /* Number of doubles in one state array: nx*ny*nz * 5 * (p+1)^3. */
 long long dgb_state_size(const dgb_handle* h);
 
@@ -110,6 +113,10 @@ long long dgb_state_size(const dgb_handle* h);
  * (cudg.cu:117-122). */
 int dgb_set_state(dgb_handle* h, const double* U_host);
 int dgb_get_state(dgb_handle* h, double* U_host);
+
+/* Device -> device variants (caller-owned device arrays); synchronise. */
+int dgb_set_state_device(dgb_handle* h, const double* U_dev);
+int dgb_get_state_device(dgb_handle* h, double* U_dev);
 
 /* Device pointer of the handle's resident state (for callers that keep data
  * on the GPU). */
@@ -162,6 +169,56 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
  * This entry point has no counterpart in the reference. */
 int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params* params, const double* U_dev,
                          double* f_dev, void* stream);
+
+/* ------------------------------------------------------------------ adjoint
+ * Discrete adjoint of the FP64 residual and of the RK steps, hand-written
+ * (reverse mode of every kernel).  The reference has no adjoint: these entry
+ * points have no counterpart there.  Boundaries: periodic, freestream,
+ * inviscid and no-slip walls (DGB_ERR_UNSUPPORTED for subsonic inflow or
+ * outflow sides).  A mixed-precision handle recomputes states in its own
+ * precision and applies the FP64 adjoint at them. */
+
+/* Ubar = (df/dU)^T lam at U, f = -Minv R(U) as dgb_residual computes it.
+ * Host arrays in the state layout; synchronises. */
+int dgb_residual_vjp(dgb_handle* h, const double* U_host, const double* lam_host, double* Ubar_host);
+
+/* Same on device arrays (Ubar must not alias U or lam), on the handle's
+ * stream, no host synchronisation. */
+int dgb_residual_vjp_device(dgb_handle* h, const double* U_dev, const double* lam_dev, double* Ubar_dev);
+
+/* Reverse of one RK step U -> U' of `scheme`: lam_dev holds the adjoint of U'
+ * on entry and the adjoint of U on return (in place).  U_dev is unchanged.
+ * Synchronises. */
+int dgb_step_vjp_device(dgb_handle* h, int scheme, double dt, const double* U_dev, double* lam_dev);
+
+/* Recorded forward run: advances the resident state by nsteps like dgb_step
+ * (norms_host as there, may be NULL) and keeps up to `slots` device copies of
+ * intermediate states (one of them the initial state) for dgb_backward,
+ * placed by binomial checkpointing so that the backward sweep recomputes the
+ * fewest steps: slots >= nsteps stores every state, slots = 1 recomputes
+ * every step from the initial state.  Holds slots * dgb_state_size doubles
+ * of device memory until the handle is destroyed. */
+int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, int slots,
+                       double* norms_host);
+
+/* Backward sweep through the last recorded run: given dJ/dU_N (the adjoint
+ * of the final state) returns dJ/dU_0.  The resident state is left at U_N.
+ * May be called repeatedly for different dJ/dU_N. */
+int dgb_backward(dgb_handle* h, const double* dJdUN_host, double* dJdU0_host);
+int dgb_backward_device(dgb_handle* h, const double* dJdUN_dev, double* dJdU0_dev);
+
+/* Steps recomputed and reversed by the last backward sweep, and the forward
+ * steps of the whole checkpoint plan (recorded run included). */
+int dgb_adjoint_stats(const dgb_handle* h, long long* forward_steps, long long* reverse_steps,
+                      long long* planned_forward_steps);
+
+/* The binomial checkpoint plan itself (host only): 2 * *nops entries
+ * (kind, argument) into ops_out (capacity cap), kind 0 = advance `argument`
+ * steps, 1 = store the work state in buffer `argument`, 2 = restore it from
+ * buffer `argument`, 3 = reverse step `argument`.  ops_out may be NULL to
+ * query the size. */
+int dgb_checkpoint_plan(long long nsteps, int slots, long long* ops_out, long long cap, long long* nops,
+                        long long* forward_steps, int* peak_slots);
 
 /* ---------------------------------------------------------------- host side
  * Host-only helpers (no GPU needed) that mirror the reference's setup
