@@ -195,6 +195,98 @@ def _stage_kernel_ms(dg, s, U0, dt, reps):
     return float(np.mean([kms[1], kms[3], kms[4], kms[5]])), float(kms[0])
 
 
+def _reverse_step_ms(dg, torch, s, stream, U0, dt, reps):
+    """Device time (ms, CUDA events on the handle's stream) of one reverse RK4
+    step (3 stage recomputations + 4 residual VJPs) at state U0."""
+    Ud = torch.tensor(U0, device="cuda")
+    lam = torch.ones_like(Ud)
+    torch.cuda.synchronize()
+    s.step_vjp_device(dg.RK4, dt, Ud.data_ptr(), lam.data_ptr())  # warm-up, allocates the adjoint buffers
+    launches = s.last_launch_count
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    tot = 0.0
+    for _ in range(reps):
+        lam.fill_(1.0)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        s.step_vjp_device(dg.RK4, dt, Ud.data_ptr(), lam.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        tot += ev0.elapsed_time(ev1)
+    return tot / reps, launches
+
+
+def _adjoint_config(dg, torch, nsteps, budgets):
+    """Gradient of the final enstrophy w.r.t. the 8 x 3 amplitudes of seeded
+    Fourier velocity modes on a uniform flow: periodic [0, 2 pi]^3, 16^3 hexes,
+    p = 3, Re 500, Ma 0.3, RK4, FP64.  Times the recorded forward run and the
+    backward sweep for each checkpoint budget, and checks the gradient along
+    one random direction against central differences of two plain runs."""
+    from dgpr_b200 import autograd as dga
+    from dgpr_b200 import functionals as F
+    from tests import cases as C
+    n, p, Re, Ma = 16, 3, 500.0, 0.3
+    c = 1.0 / Ma
+    prm = C.params(mu=1.0 / Re, c=c, u=1.0, v=0.0, w=0.0)
+    nodes = C.box_nodes(n, n, n, 1, L_BOX, L_BOX, L_BOX)
+    xyz = F.box_node_coords(n, n, n, p, L_BOX, L_BOX, L_BOX)
+    modes = F.FourierModes(xyz, 1.4, 1.0, prm[5], (1.0, 0.0, 0.0), nmodes=8, kmax=4, amp=0.05, seed=0,
+                           device="cuda")
+    quad = F.BoxQuadrature(n, n, n, p, L_BOX, L_BOX, L_BOX, device="cuda")
+    dt = 0.2 * (L_BOX / n) / ((2 * p + 1) * (c + 1.5))
+    mesh = dg.Mesh(n, n, n, p, 1, nodes, [dg.PERIODIC] * 6)
+    out = {"workload": f"Fourier modes on uniform flow, periodic [0,2pi]^3, {n}^3 hexes, p={p}, Re={Re:g}, "
+                       f"Ma={Ma:g}, RK4 dt={dt:.3e}, {nsteps} steps, J = final enstrophy, 24 amplitudes",
+           "budgets": []}
+    with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
+        a0 = modes.amplitudes("cuda")
+        U0 = modes.state(a0).detach()
+        s.set_state(U0.cpu().numpy())
+        s.step(dg.RK4, dt, 5, norms=False)  # warm-up
+        grad = None
+        for slots in budgets:
+            a = a0.clone().requires_grad_(True)
+            Ua = modes.state(a)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            UN = dga.integrate(Ua, s, dg.RK4, dt, nsteps, slots=slots)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            J = F.enstrophy(UN, quad)
+            J.backward()
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            fwd, rev, planned = s.adjoint_stats()
+            g = a.grad.cpu().numpy()
+            if grad is None:
+                grad = g
+            out["budgets"].append({"slots": slots, "forward_s": t1 - t0, "backward_s": t2 - t1,
+                                   "backward_over_forward": (t2 - t1) / (t1 - t0),
+                                   "recomputed_steps": fwd, "reversed_steps": rev,
+                                   "gradient_equal_to_first_budget": bool(np.array_equal(g, grad))})
+        # plain forward time of the same run (no recording)
+        s.set_state(U0.cpu().numpy())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.step(dg.RK4, dt, nsteps, norms=False)
+        out["plain_forward_s"] = time.perf_counter() - t0
+        rng = np.random.default_rng(1)
+        d = torch.tensor(rng.standard_normal((8, 3)), device="cuda")
+
+        def Jof(av):
+            s.set_state(modes.state(av).detach().cpu().numpy())
+            s.step(dg.RK4, dt, nsteps, norms=False)
+            return float(F.enstrophy(torch.tensor(s.get_state(), device="cuda"), quad))
+
+        h = 1e-5
+        fd = (Jof(a0 + h * d) - Jof(a0 - h * d)) / (2 * h)
+        an = float((torch.tensor(grad, device="cuda") * d).sum())
+        out["fd_check"] = {"directional_adjoint": an, "directional_fd": fd, "rel_err": abs(an - fd) / abs(fd),
+                           "h": h}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import dgpr_b200 as dg
@@ -281,6 +373,17 @@ def run_ours(args, rank, world, local_rank):
         err = float(np.linalg.norm(out[dg.MIXED_FP32] - out[dg.FP64]) / np.linalg.norm(out[dg.FP64]))
         acc = {"steps": args.accuracy_steps, "rel_l2_mixed_vs_fp64": err}
 
+    # ---- adjoint: one reverse RK4 step against one forward step at this
+    # workload, and the adjoint configuration's full gradient
+    adj = None
+    if rank == 0 and args.adjoint_steps > 0:
+        with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as sa:
+            sa.set_stream(stream.cuda_stream)
+            rev_ms, rev_launches = _reverse_step_ms(dg, torch, sa, stream, U0, dt, reps)
+        adj = {"reverse_step_ms": rev_ms, "forward_step_ms": ms / args.steps,
+               "reverse_over_forward": rev_ms / (ms / args.steps), "reverse_step_launches": rev_launches,
+               "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20))}
+
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
     try:
@@ -323,6 +426,7 @@ def run_ours(args, rank, world, local_rank):
                       "trace_kernel_ms": trace_ms_mixed,
                       "dtype": "f32 contractions/fluxes, f64 geometry/inverse mass/RK state",
                       "accuracy": acc},
+            "adjoint": adj,
             "clocks": clocks,
         }
         if cpu:
@@ -338,6 +442,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
+    ap.add_argument("--adjoint-steps", type=int, default=400,
+                    help="RK4 steps of the adjoint configuration (0 skips the adjoint block)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (0 skips it)")
     args = ap.parse_args()

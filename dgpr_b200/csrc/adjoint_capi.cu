@@ -303,6 +303,7 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
   CK(cudaStreamSynchronize(h->stream));
   h->plan_pos = h->plan.first_reverse;
   h->recorded = true;
+  h->slots_dirty = false;
   h->rec_scheme = scheme;
   h->rec_dt = dt;
   h->rec_steps = nsteps;
@@ -319,10 +320,26 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
   const double dt = h->rec_dt;
   double* lam = h->d_adj[dgb_handle::ADJ_LAM];
   int rc;
+  long long nl = 0, fwd = 0, rev = 0;
+  if (h->slots_dirty) {
+    // an earlier sweep overwrote checkpoints: rebuild them from U_0 (buffer 0
+    // is never overwritten) by replaying the recorded run's part of the plan
+    if ((rc = copy_state(h, h->d_U, h->d_slots[0]))) return rc;
+    for (size_t k = 1; k < h->plan_pos; ++k) {
+      const CkOp& op = h->plan.ops[k];
+      if (op.kind == CK_STORE) {
+        if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+      } else {
+        if ((rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, nullptr))) return rc;
+        nl += h->last_launches;
+        fwd += op.arg;
+      }
+    }
+  } else {
+    if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
+  }
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   if ((rc = copy_state(h, lam, lamN_dev))) return rc;
-  if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
-  long long nl = 0, fwd = 0, rev = 0;
   for (size_t k = h->plan_pos; k < h->plan.ops.size(); ++k) {
     const CkOp& op = h->plan.ops[k];
     switch (op.kind) {
@@ -335,6 +352,7 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
         break;
       case CK_STORE:
         if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+        h->slots_dirty = true;
         break;
       case CK_FORWARD:
         // dgb_step clears the status word: keep what the reverse steps raised

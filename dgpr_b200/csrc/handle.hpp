@@ -61,6 +61,7 @@ struct dgb_handle {
   dgb::CheckpointPlan plan;    // the recorded forward's plan
   size_t plan_pos = 0;         // first op of the backward part
   bool recorded = false;
+  bool slots_dirty = false;    // a backward sweep overwrote checkpoints of the recorded run
   int rec_scheme = DGB_RK4;
   double rec_dt = 0.;
   unsigned long long rec_steps = 0;

@@ -203,7 +203,8 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
 
 /* Backward sweep through the last recorded run: given dJ/dU_N (the adjoint
  * of the final state) returns dJ/dU_0.  The resident state is left at U_N.
- * May be called repeatedly for different dJ/dU_N. */
+ * May be called repeatedly for different dJ/dU_N; when a sweep has
+ * overwritten checkpoints the next one first recomputes them from U_0. */
 int dgb_backward(dgb_handle* h, const double* dJdUN_host, double* dJdU0_host);
 int dgb_backward_device(dgb_handle* h, const double* dJdUN_dev, double* dJdU0_dev);
 
