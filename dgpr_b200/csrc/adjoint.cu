@@ -613,13 +613,17 @@ static cudaError_t prepare_p()
 template <int P>
 static cudaError_t vjp_p(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st)
 {
-  KLaunch L64 = L;
-  L64.precision = DGB_FP64;
-  L64.ops = L.opsd;
-  cudaError_t e = launch_trace(L64, v.U, s.trace, st);
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
+  const double* Tr = v.Tr;
+  if (!Tr) {
+    KLaunch L64 = L;
+    L64.precision = DGB_FP64;
+    L64.ops = L.opsd;
+    if ((e = launch_trace(L64, v.U, s.trace, st)) != cudaSuccess) return e;
+    Tr = s.trace;
+  }
   adjA_kernel<P><<<(unsigned)L.E, Cfg<P>::NT, AdjASmem<P>::TOTAL * sizeof(double), st>>>(
-      L.E, v.U, s.trace, v, L.opsd, L.geo, L.nbr, L.prm, s.part, s.ta, s.flag);
+      L.E, v.U, Tr, v, L.opsd, L.geo, L.nbr, L.prm, s.part, s.ta, s.flag);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   adjB_kernel<P><<<(unsigned)L.E, Cfg<P>::NT, AdjBSmem<P>::TOTAL * sizeof(double), st>>>(

@@ -15,6 +15,7 @@ namespace dgb {
 // alias X, Y or Z likewise.
 struct VjpArgs {
   const double* U;
+  const double* Tr;  // FP64 face traces of U [E][6][10][P*P], or null: computed into the scratch
   const double* X;
   const double* Y;
   const double* Z;
@@ -33,7 +34,7 @@ struct VjpScratch {
 };
 
 cudaError_t prepare_adjoint(int P);
-// trace_kernel (FP64) + adjA + adjB on stream st; L.opsd is the operator table
+// [trace_kernel (FP64)] + adjA + adjB on stream st; L.opsd is the operator table
 cudaError_t launch_residual_vjp(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
 
 }  // namespace dgb

@@ -82,80 +82,108 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
 //         a2 = J2^T (2/3 dt lam)      a1 = J1^T (dt/6 lam + dt/4 a2)
 //         a0 = J0^T (dt/6 lam + dt/4 a2 + dt a1)
 //   and in both  lam_i = lam + a0 + a1 + a2 (+ a3).
-// 3 (RK4) or 2 (TVD) stage launches + 1 trace launch, then 3 launches per VJP.
+// Face traces: an FP64 handle keeps the traces of U_i and of every
+// recomputed stage state (the stage epilogues write them) and hands them to
+// the VJPs; a mixed-precision handle recomputes the stages in FP32 with
+// rotating trace buffers and each VJP takes its own FP64 traces.
 int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl)
 {
   const KLaunch L = klaunch(h);
-  double* S0 = h->d_adj[dgb_handle::ADJ_S0];
-  double* S1 = h->d_adj[dgb_handle::ADJ_S1];
-  double* S2 = h->d_adj[dgb_handle::ADJ_S2];
+  double* S[3] = {h->d_adj[dgb_handle::ADJ_S0], h->d_adj[dgb_handle::ADJ_S1], h->d_adj[dgb_handle::ADJ_S2]};
   double* A0 = h->d_adj[dgb_handle::ADJ_A0];
   double* A1 = h->d_adj[dgb_handle::ADJ_A1];
   double* ACC = h->d_adj[dgb_handle::ADJ_ACC];
   const VjpScratch sc = scratch(h);
-  CK(launch_trace(L, Ui, h->d_trace[0], h->stream));
+  const bool f64 = h->precision == DGB_FP64;
+  void* const* T = h->d_trace;
+  void* TU = f64 ? (void*)h->d_adj_tr : T[0];
+  CK(launch_trace(L, Ui, TU, h->stream));
+  const int nst = scheme == DGB_RK4 ? 3 : 2;  // recomputed stage states
+  const int rk4[3] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2}, tvd[2] = {MODE_TVD_0, MODE_TVD_1};
+  // trace buffers read / written by the recomputed stages
+  const void* tin_f64[3] = {TU, T[0], T[1]};
+  void* tout_f64[3] = {T[0], T[1], T[2]};
+  const void* tin_mix[3] = {T[0], T[1], T[0]};
+  void* tout_mix[3] = {T[1], T[0], nullptr};
+  if (scheme != DGB_RK4) tout_mix[1] = nullptr;
+  for (int s = 0; s < nst; ++s) {
+    StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[s] : tvd[s], dt);
+    a.Ubase = Ui;
+    a.acc = h->d_acc;
+    a.Uout = S[s];
+    a.flag = h->d_flag;
+    a.Tnext = f64 ? tout_f64[s] : tout_mix[s];
+    CK(launch_stage(L, s == 0 ? Ui : S[s - 1], f64 ? tin_f64[s] : tin_mix[s], a, h->stream));
+  }
+  auto tr = [&](int s) -> const double* {  // FP64 traces of stage state s (-1: U_i)
+    if (!f64) return nullptr;
+    return (const double*)(s < 0 ? TU : tout_f64[s]);
+  };
+  VjpArgs v;
   if (scheme == DGB_RK4) {
-    const int modes[3] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2};
-    const double* in[3] = {Ui, S0, S1};
-    double* out[3] = {S0, S1, S2};
-    const int tin[3] = {0, 1, 0}, tout[3] = {1, 0, -1};
-    for (int s = 0; s < 3; ++s) {
-      StageArgs a = stage_args(modes[s], dt);
-      a.Ubase = Ui;
-      a.acc = h->d_acc;
-      a.Uout = out[s];
-      a.flag = h->d_flag;
-      a.Tnext = tout[s] >= 0 ? h->d_trace[tout[s]] : nullptr;
-      CK(launch_stage(L, in[s], h->d_trace[tin[s]], a, h->stream));
-    }
-    VjpArgs v = vjp(S2, dt / 6., lam);
+    v = vjp(S[2], dt / 6., lam);
+    v.Tr = tr(2);
     v.a_out = A0;
     v.acc_in = lam;
     v.acc_out = ACC;
     CK(launch_residual_vjp(L, v, sc, h->stream));
-    v = vjp(S1, dt / 3., lam, dt, A0);
+    v = vjp(S[1], dt / 3., lam, dt, A0);
+    v.Tr = tr(1);
     v.a_out = A0;
     v.acc_in = ACC;
     v.acc_out = ACC;
     CK(launch_residual_vjp(L, v, sc, h->stream));
-    v = vjp(S0, dt / 3., lam, dt / 2., A0);
+    v = vjp(S[0], dt / 3., lam, dt / 2., A0);
+    v.Tr = tr(0);
     v.a_out = A0;
     v.acc_in = ACC;
     v.acc_out = ACC;
     CK(launch_residual_vjp(L, v, sc, h->stream));
     v = vjp(Ui, dt / 6., lam, dt / 2., A0);
-    v.acc_in = ACC;
-    v.acc_out = lam;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
-    if (nl) *nl += 4 + 4 * 3;
   } else {
-    const int modes[2] = {MODE_TVD_0, MODE_TVD_1};
-    const double* in[2] = {Ui, S0};
-    double* out[2] = {S0, S1};
-    for (int s = 0; s < 2; ++s) {
-      StageArgs a = stage_args(modes[s], dt);
-      a.Ubase = Ui;
-      a.Uout = out[s];
-      a.flag = h->d_flag;
-      a.Tnext = s == 0 ? h->d_trace[1] : nullptr;
-      CK(launch_stage(L, in[s], h->d_trace[s], a, h->stream));
-    }
-    VjpArgs v = vjp(S1, 2. * dt / 3., lam);
+    v = vjp(S[1], 2. * dt / 3., lam);
+    v.Tr = tr(1);
     v.a_out = A0;
     v.acc_in = lam;
     v.acc_out = ACC;
     CK(launch_residual_vjp(L, v, sc, h->stream));
-    v = vjp(S0, dt / 6., lam, dt / 4., A0);
+    v = vjp(S[0], dt / 6., lam, dt / 4., A0);
+    v.Tr = tr(0);
     v.a_out = A1;
     v.acc_in = ACC;
     v.acc_out = ACC;
     CK(launch_residual_vjp(L, v, sc, h->stream));
     v = vjp(Ui, dt / 6., lam, dt / 4., A0, dt, A1);
-    v.acc_in = ACC;
-    v.acc_out = lam;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
-    if (nl) *nl += 3 + 3 * 3;
   }
+  v.Tr = tr(-1);
+  v.acc_in = ACC;
+  v.acc_out = lam;
+  CK(launch_residual_vjp(L, v, sc, h->stream));
+  if (nl) *nl += 1 + nst + (nst + 1) * (f64 ? 2 : 3);
+  return DGB_OK;
+}
+
+// The captured graph of one reverse step of the work state d_U with the
+// adjoint in ADJ_LAM (the backward sweep's REVERSE operation).
+int ensure_rev_graph(dgb_handle* h, int scheme, double dt)
+{
+  if (h->rev_graph && h->rev_scheme == scheme && h->rev_dt == dt) return DGB_OK;
+  if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
+  h->rev_graph = nullptr;
+  h->rev_scheme = -1;
+  cudaGraph_t g;
+  long long nl = 0;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_reverse_step(h, scheme, dt, h->d_U, h->d_adj[dgb_handle::ADJ_LAM], &nl);
+  cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+  if (rc) return rc;
+  if (ce != cudaSuccess) return cuda_status(ce, "cudaStreamEndCapture");
+  ce = cudaGraphInstantiate(&h->rev_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return cuda_status(ce, "cudaGraphInstantiate");
+  h->rev_scheme = scheme;
+  h->rev_dt = dt;
+  h->rev_launches = nl;
   return DGB_OK;
 }
 
@@ -187,6 +215,9 @@ int check_scheme(int scheme, double dt)
 
 void dgb::free_adjoint(dgb_handle* h)
 {
+  if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
+  h->rev_graph = nullptr;
+  h->rev_scheme = -1;
   for (double*& p : h->d_adj) {
     if (p) cudaFree(p);
     p = nullptr;
@@ -279,28 +310,38 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
     CK(cudaMalloc(&p, sizeof(double) * (size_t)h->n));
     h->d_slots.push_back(p);
   }
-  unsigned long long done = 0;
+  if ((rc = ensure_step_graph(h, scheme, dt, nsteps))) return rc;
+  CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  // Between graph replays the face traces of the resident state stay valid
+  // (each step's last stage writes them), and storing a checkpoint does not
+  // change the state: only the first replay needs the trace kernel.
+  bool need_trace = true;
   long long launches = 0;
   for (size_t k = 0; k < h->plan.first_reverse; ++k) {
     const CkOp& op = h->plan.ops[k];
     if (op.kind == CK_STORE) {
       if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
     } else if (op.kind == CK_FORWARD) {
-      rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, norms_host ? norms_host + done : nullptr);
-      if (rc) return rc;
-      launches += h->last_launches;
-      done += (unsigned long long)op.arg;
+      if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace))) return rc;
+      launches += (need_trace ? 1 : 0) + op.arg * h->launches_per_step;
+      need_trace = false;
     } else {
       return fail(DGB_ERR_ARG, "checkpoint plan restores during the forward run");
     }
   }
   // work state is U_{N-1}: keep it, take the last step on the resident state
   if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_WORK], h->d_U))) return rc;
-  rc = dgb_step(h, scheme, dt, 1, norms_host ? norms_host + done : nullptr);
-  if (rc) return rc;
-  launches += h->last_launches;
+  if ((rc = enqueue_steps(h, 1, need_trace))) return rc;
+  launches += (need_trace ? 1 : 0) + h->launches_per_step;
   if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], h->d_U))) return rc;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (norms_host)
+    CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   h->plan_pos = h->plan.first_reverse;
   h->recorded = true;
   h->slots_dirty = false;
@@ -320,31 +361,38 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
   const double dt = h->rec_dt;
   double* lam = h->d_adj[dgb_handle::ADJ_LAM];
   int rc;
+  // dgb_step calls since the record may have replaced the step graph
+  if ((rc = ensure_step_graph(h, scheme, dt, h->rec_steps))) return rc;
+  if ((rc = ensure_rev_graph(h, scheme, dt))) return rc;
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   long long nl = 0, fwd = 0, rev = 0;
   if (h->slots_dirty) {
     // an earlier sweep overwrote checkpoints: rebuild them from U_0 (buffer 0
     // is never overwritten) by replaying the recorded run's part of the plan
     if ((rc = copy_state(h, h->d_U, h->d_slots[0]))) return rc;
+    bool need_trace = true;
     for (size_t k = 1; k < h->plan_pos; ++k) {
       const CkOp& op = h->plan.ops[k];
       if (op.kind == CK_STORE) {
         if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
       } else {
-        if ((rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, nullptr))) return rc;
-        nl += h->last_launches;
+        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace))) return rc;
+        nl += (need_trace ? 1 : 0) + op.arg * h->launches_per_step;
+        need_trace = false;
         fwd += op.arg;
       }
     }
   } else {
     if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
   }
-  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   if ((rc = copy_state(h, lam, lamN_dev))) return rc;
   for (size_t k = h->plan_pos; k < h->plan.ops.size(); ++k) {
     const CkOp& op = h->plan.ops[k];
     switch (op.kind) {
       case CK_REVERSE:
-        if ((rc = enqueue_reverse_step(h, scheme, dt, h->d_U, lam, &nl))) return rc;
+        CK(cudaGraphLaunch(h->rev_graph, h->stream));
+        nl += h->rev_launches;
         ++rev;
         break;
       case CK_RESTORE:
@@ -355,10 +403,10 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
         h->slots_dirty = true;
         break;
       case CK_FORWARD:
-        // dgb_step clears the status word: keep what the reverse steps raised
-        if ((rc = read_flag(h))) return rc;
-        if ((rc = dgb_step(h, scheme, dt, (unsigned long long)op.arg, nullptr))) return rc;
-        nl += h->last_launches;
+        // the reverse steps reuse the trace buffers: recompute the traces
+        CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, true))) return rc;
+        nl += 1 + op.arg * h->launches_per_step;
         fwd += op.arg;
         break;
     }

@@ -89,8 +89,8 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     CK(launch_stage(L, in, tin, a, h->stream));
     if (s == 0) {
       if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-      CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, h->d_counter, h->d_flag,
-                     h->stream));
+      CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
+                     h->d_flag, h->stream));
     }
   }
   if (ev) CK(cudaEventRecord(ev[k++], h->stream));
@@ -114,6 +114,52 @@ void free_all(dgb_handle* h)
 }  // namespace
 
 int dgb::set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+
+// The captured graph of one step for (scheme, dt), with room for `cap` norms.
+int dgb::ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap)
+{
+  if (cap > h->norms_cap) {
+    if (h->d_norms) CK(cudaFree(h->d_norms));
+    h->d_norms = nullptr;
+    CK(cudaMalloc(&h->d_norms, sizeof(double) * cap));
+    h->norms_cap = cap;
+    if (h->graph) {  // the captured graph holds the old norms pointer and capacity
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      h->graph_scheme = -1;
+    }
+  }
+  if (h->graph && h->graph_scheme == scheme && h->graph_dt == dt) return DGB_OK;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_scheme = -1;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(h, scheme, dt);
+  cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+  if (rc) return rc;
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+  ce = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+  h->graph_scheme = scheme;
+  h->graph_dt = dt;
+  h->launches_per_step = launches_per_step(h, scheme);
+  return DGB_OK;
+}
+
+// k replays of the step graph; with initial_trace the face traces of the
+// resident state are computed first (otherwise the last step's epilogue left
+// them in trace buffer 0).  Norms go to d_norms[*d_counter ...].
+int dgb::enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace)
+{
+  if (initial_trace) {
+    int rc = enqueue_initial_traces(h);
+    if (rc) return rc;
+  }
+  for (unsigned long long s = 0; s < k; ++s) CK(cudaGraphLaunch(h->graph, h->stream));
+  return DGB_OK;
+}
 
 extern "C" {
 
@@ -351,38 +397,11 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
   if (!(dt == dt)) return fail(DGB_ERR_ARG, "dt is NaN");
   CK(cudaSetDevice(h->device));
   if (nsteps == 0) return DGB_OK;
-  if (nsteps > h->norms_cap) {
-    if (h->d_norms) CK(cudaFree(h->d_norms));
-    h->d_norms = nullptr;
-    CK(cudaMalloc(&h->d_norms, sizeof(double) * nsteps));
-    h->norms_cap = nsteps;
-    if (h->graph) {  // the captured graph holds the old norms pointer
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-      h->graph_scheme = -1;
-    }
-  }
-  if (!h->graph || h->graph_scheme != scheme || h->graph_dt != dt) {
-    if (h->graph) cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_step(h, scheme, dt);
-    cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-    if (rc) return rc;
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-    ce = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-    h->graph_scheme = scheme;
-    h->graph_dt = dt;
-    h->launches_per_step = launches_per_step(h, scheme);
-  }
+  int rc = ensure_step_graph(h, scheme, dt, nsteps);
+  if (rc) return rc;
   CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  int rc = enqueue_initial_traces(h);
-  if (rc) return rc;
-  for (unsigned long long s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->graph, h->stream));
+  if ((rc = enqueue_steps(h, nsteps, true))) return rc;
   h->last_launches = 1 + (long long)nsteps * h->launches_per_step;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));

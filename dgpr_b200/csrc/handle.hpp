@@ -65,6 +65,10 @@ struct dgb_handle {
   int rec_scheme = DGB_RK4;
   double rec_dt = 0.;
   unsigned long long rec_steps = 0;
+  cudaGraphExec_t rev_graph = nullptr;  // one reverse step of d_U with the adjoint in ADJ_LAM
+  int rev_scheme = -1;
+  double rev_dt = 0.;
+  long long rev_launches = 0;
   long long adj_forward_steps = 0;  // steps recomputed by the last dgb_backward
   long long adj_reverse_steps = 0;
 };
@@ -100,5 +104,7 @@ inline int cuda_status(cudaError_t e, const char* what)
 }
 
 void free_adjoint(dgb_handle* h);
+int ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap);
+int enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace);
 
 }  // namespace dgb

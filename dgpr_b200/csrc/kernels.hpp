@@ -55,7 +55,8 @@ cudaError_t launch_trace(const KLaunch& L, const double* U, void* Tout, cudaStre
 // one stage: residual of Us with traces Tin, then sa.mode's update
 cudaError_t launch_stage(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                          cudaStream_t st);
-cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, int* counter,
+// norms[*counter] = sqrt(sum(part) * inv_size) when *counter < cap; ++*counter
+cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, long cap, int* counter,
                         int* flag, cudaStream_t st);
 
 // per compute type (kernels_fp64.cu / kernels_fp32.cu)

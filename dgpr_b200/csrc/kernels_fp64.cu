@@ -34,8 +34,8 @@ void pack_ops(const Ops1D& o, double* t)
 size_t trace_elem_bytes(int precision) { return precision == DGB_MIXED_FP32 ? sizeof(float) : sizeof(double); }
 
 // sqrt(sum(part) / size) into norms[*counter], deterministic fixed-order sum
-__global__ void norm_kernel(long E, const double* __restrict__ part, double inv_size, double* norms, int* counter,
-                            int* flag)
+__global__ void norm_kernel(long E, const double* __restrict__ part, double inv_size, double* norms, long cap,
+                            int* counter, int* flag)
 {
   __shared__ double red[1024];
   const int tid = threadIdx.x;
@@ -50,16 +50,16 @@ __global__ void norm_kernel(long E, const double* __restrict__ part, double inv_
   if (tid == 0) {
     const int c = *counter;
     const double v = sqrt(red[0] * inv_size);
-    norms[c] = v;
+    if (c >= 0 && c < cap) norms[c] = v;
     if (!isfinite(v)) *flag |= 1;
     *counter = c + 1;
   }
 }
 
-cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, int* counter, int* flag,
-                        cudaStream_t st)
+cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, long cap, int* counter,
+                        int* flag, cudaStream_t st)
 {
-  norm_kernel<<<1, 1024, 0, st>>>(E, part, inv_size, norms, counter, flag);
+  norm_kernel<<<1, 1024, 0, st>>>(E, part, inv_size, norms, cap, counter, flag);
   return cudaGetLastError();
 }
 
