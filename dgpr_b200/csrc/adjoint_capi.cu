@@ -55,7 +55,7 @@ VjpScratch scratch(dgb_handle* h) { return {h->d_adj_tr, h->d_adj_ta, h->d_adj[d
 VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const double* Y = nullptr,
             double cz = 0., const double* Z = nullptr)
 {
-  VjpArgs v;
+  VjpArgs v{};  // every pointer not set below (Tr, a_out, acc_in, acc_out) stays null
   v.U = U;
   v.X = X;
   v.Y = Y;
@@ -63,9 +63,6 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
   v.cx = cx;
   v.cy = cy;
   v.cz = cz;
-  v.a_out = nullptr;
-  v.acc_in = nullptr;
-  v.acc_out = nullptr;
   return v;
 }
 
@@ -119,7 +116,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     if (!f64) return nullptr;
     return (const double*)(s < 0 ? TU : tout_f64[s]);
   };
-  VjpArgs v;
+  VjpArgs v{};
   if (scheme == DGB_RK4) {
     v = vjp(S[2], dt / 6., lam);
     v.Tr = tr(2);
