@@ -20,7 +20,24 @@
 #include "kernels.cuh"
 #include "physics_vjp.cuh"
 
+// 8 resident CTAs per SM (128 registers a thread at P <= 4): the spills this
+// costs are cheaper than the latency exposed at 4 CTAs per SM (measured on
+// the reverse RK4 step at 32^3 and 16^3, p = 3)
+#ifndef DGB_ADJA_MINB
+#define DGB_ADJA_MINB 8
+#endif
+#ifndef DGB_ADJB_MINB
+#define DGB_ADJB_MINB 8
+#endif
+
 namespace dgb {
+
+// resident CTAs per SM the adjoint kernels are compiled for (register cap);
+// applied to the small element sizes, where one CTA has few threads
+template <int P, int M>
+struct AdjMinB {
+  static constexpr int value = Cfg<P>::NT <= 64 ? M : 1;
+};
 
 // Face value S and reference gradient g of a nodal field sUx[5][NB] at the face
 // points of faces lf = 3*half + j (threads tid < 3*NQF), returned in
@@ -195,7 +212,7 @@ struct AdjASmem {
 };
 
 template <int P>
-__global__ void __launch_bounds__(Cfg<P>::NT)
+__global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJA_MINB>::value))
 adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr, VjpArgs v,
             const double* __restrict__ opsg, const double* __restrict__ geo, const int* __restrict__ nbr,
             DevParams prm, double* __restrict__ Ubar_part, double* __restrict__ TA, int* flag)
@@ -501,7 +518,7 @@ struct AdjBSmem {
 };
 
 template <int P>
-__global__ void __launch_bounds__(Cfg<P>::NT)
+__global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJB_MINB>::value))
 adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA, const double* __restrict__ opsg,
             const double* __restrict__ geo, const int* __restrict__ nbr, DevParams prm,
             const double* __restrict__ Ubar_part, VjpArgs v)
