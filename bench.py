@@ -291,6 +291,23 @@ def _adjoint_config(dg, torch, nsteps, budgets):
     return out
 
 
+def run_reverse_steps(args):
+    """Warm-up plus `steps` reverse RK4 steps of the FP64 adjoint at the
+    workload's state (a short, profilable run of the adjoint kernels)."""
+    import torch
+    import dgpr_b200 as dg
+    nodes, prm, U0, dt = tgv_case(N_EL, P_ORD)
+    mesh = dg.Mesh(N_EL, N_EL, N_EL, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
+    stream = torch.cuda.Stream()
+    with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
+        s.set_stream(stream.cuda_stream)
+        s.set_state(U0)
+        fwd = _timed_steps(dg, torch, s, stream, dt, args.steps) / args.steps
+        rev, launches = _reverse_step_ms(dg, torch, s, stream, U0, dt, args.steps)
+    print(json.dumps({"workload": config()["workload"].replace("32^3", f"{N_EL}^3"), "forward_step_ms": fwd,
+                      "reverse_step_ms": rev, "reverse_over_forward": rev / fwd, "launches": launches}))
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import dgpr_b200 as dg
@@ -446,6 +463,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
+    ap.add_argument("--reverse-steps-only", action="store_true",
+                    help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")
     ap.add_argument("--adjoint-steps", type=int, default=400,
                     help="RK4 steps of the adjoint configuration (0 skips the adjoint block)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
@@ -458,6 +477,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.reverse_steps_only:
+        run_reverse_steps(args)
         return
     if world > 1:
         import datetime

@@ -205,8 +205,7 @@ struct AdjASmem {
   static constexpr int oX = oMu + 5 * NB;          // scratch
   // volume: V0 V1 Sq [5NB each], G [15NB], N [15NB]
   static constexpr int VOL = 45 * NB;
-  // faces: sN[3][10] sY[3][15] (x NQF); the lifting adjoints db[3][5] and
-  // db2[3][5] reuse sN once the face values of mu are in registers
+  // faces: sN[3][10] sY[3][15] (x NQF)
   static constexpr int FACE = 75 * NQF;
   static constexpr int TOTAL = oX + (VOL > FACE ? VOL : FACE);
 };
@@ -340,50 +339,25 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   if (node) contract_reg<P, 2, true>(B, V0, tid, Ub);
   __syncthreads();
 
-  // ---- faces
+  // ---- faces.  The lifting's transpose is pointwise like the lifting
+  // (K = diag(1/w), see the stage kernel): zb = (K x K)^T (ef fw mu) = ef fJ mu.
   double* sN = sX;
   double* sY = sN + 30 * NQF;
-  double* db = sN;  // [3][5][NQF]  adjoint of the lifting source, after K^T K^T
-  double* db2 = sN + 15 * NQF;
-  const double* K = so + C::oK;
   const double* w1 = so + C::oW;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     double Sm[5], gm[3][5];
     face_value_grad<P>(half, Mu, sN, sY, so, Sm, gm);
     const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
-    int nb = 0;
-    double fw = 0., ef = 0.;
     if (tid < NH) {
-      nb = nbr[e * 6 + lf];
-      fw = sg[kGeoFJ + lf] * w1[q1] * w1[q2];
-      ef = prm.eta * (nb >= 0 ? 0.5 : 1.0);
-#pragma unroll
-      for (int r = 0; r < 5; ++r) db[(j * 5 + r) * NQF + fq] = ef * fw * Sm[r];
-    }
-    __syncthreads();
-    if (tid < NH) {  // lifting transpose, first direction: z2[k1,q2] = sum_q1 K[q1][k1] db[q1,q2]
-      const int k1 = q1;
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        double s = 0.;
-#pragma unroll
-        for (int q = 0; q < P; ++q) s = fma(K[q * P + k1], db[(j * 5 + r) * NQF + q + P * q2], s);
-        db2[(j * 5 + r) * NQF + fq] = s;
-      }
-    }
-    __syncthreads();
-    if (tid < NH) {
-      const int k1 = q1, k2 = q2;
+      const int nb = nbr[e * 6 + lf];
+      const double fJ = sg[kGeoFJ + lf];
+      const double fw = fJ * w1[q1] * w1[q2];
+      const double ef = prm.eta * (nb >= 0 ? 0.5 : 1.0);
       double zb[5];
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        double s = 0.;
-#pragma unroll
-        for (int q = 0; q < P; ++q) s = fma(K[q * P + k2], db2[(j * 5 + r) * NQF + k1 + P * q], s);
-        zb[r] = s;
-      }
       zb[0] = 0.;  // the lifting has no mass component
+#pragma unroll
+      for (int r = 1; r < 5; ++r) zb[r] = ef * fJ * Sm[r];
       const double* n = sg + kGeoN + 3 * lf;
       double ab[5];
 #pragma unroll

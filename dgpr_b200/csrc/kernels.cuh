@@ -299,10 +299,8 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
 // geometry (T) | misc] followed by one scratch region reused by the phases:
 //   volume  V0[5NB] V1[5NB] G[3][5][NB]                               (T)
 //   faces   (three faces at a time)                                    (T)
-//           Fa[3][5][NQF]   face flux coefficient of phi (then times fJ w)
+//           Fa[3][5][NQF]   face flux coefficient of phi, times fJ w
 //           Fb[3][12][NQF]  reference-space coefficient of grad phi, vars 1..4
-//           Fz[3][4][NQF]   BR2 lifting source, vars 1..4 (var 0 has no viscous flux)
-//           Fz2[3][4][NQF]  after the first lifting direction
 //           Su[3][13][NQF]  test functions after the first tangential direction
 //           Sc[3][9][NQF]   after the second (aliases Fb)
 //   minv    M0[5NB] M1[5NB]                                            (FP64)
@@ -320,7 +318,7 @@ struct StageSmem {
   static constexpr int oMisc = oGeo + align16(kGeoStride * ST);
   static constexpr int oX = oMisc + align16(8 * ST);
   static constexpr int VOL = 25 * NB * ST;
-  static constexpr int FACE = 3 * (5 + 12 + 4 + 4 + 13) * NQF * ST;
+  static constexpr int FACE = 3 * (5 + 12 + 13) * NQF * ST;
   static constexpr int MINV = 10 * NB * SD;
   static constexpr int RED = C::NT * SD;
   // byte offset of the new state inside the scratch: after the trace buffers
@@ -348,7 +346,6 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   T* so = reinterpret_cast<T*>(smraw + L::oOps);
   double* sMi = reinterpret_cast<double*>(smraw + L::oMi);
   T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
-  T* sMisc = reinterpret_cast<T*>(smraw + L::oMisc);
   unsigned char* sXb = smraw + L::oX;
   T* sX = reinterpret_cast<T*>(sXb);
   const long e = blockIdx.x;
@@ -442,20 +439,23 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   __syncthreads();
 
   // ---------------- faces (solve.cpp:393-794), three at a time
+  // BR2 lifting: the face-restricted lifting operator E_f Minv E_f^T of an
+  // affine element is (cend / detJ) (K x K) with K = B M1^-1 B^T; since
+  // M1 = B^T diag(w) B with B square, K = diag(1/w) and the lifted jump at a
+  // face point is (cend / detJ) fJ times the pointwise source (solve.cpp:402-480)
   T* Fa = sX;
   T* Fb = Fa + 15 * NQF;
-  T* Fz = Fb + 36 * NQF;
-  T* Fz2 = Fz + 12 * NQF;
-  T* Su = Fz2 + 12 * NQF;
+  T* Su = Fb + 36 * NQF;
   T* Sc = Fb;
-  const T* K = so + C::oK;
   const T* w1 = so + C::oW;
+  const T eta = T(prm.eta);
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     if (tid < NH) {
       const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
       const T* n = sg + kGeoN + 3 * lf;
-      const T fw = sg[kGeoFJ + lf] * w1[q1] * w1[q2];
+      const T fJ = sg[kGeoFJ + lf];
+      const T fw = fJ * w1[q1] * w1[q2];
       const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
       T Uo[5], Qo[5];
 #pragma unroll
@@ -466,7 +466,6 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
       const int nb = nbr[e * 6 + lf];
       T* fa = Fa + j * 5 * NQF + fq;
       T* fb = Fb + j * 12 * NQF + fq;
-      T* fz = Fz + j * 4 * NQF + fq;
       if (nb >= 0) {
         const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
         T Un[5];
@@ -497,12 +496,11 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
           T ro[5], rn[5];
           visc_jump_n(Uo, d, n, mu, ro);  // BR2 lifting sources of both sides
           visc_jump_n(Un, d, n, mu, rn);
-          const T co = T(0.5) * fw * so[C::oC + end] / detJ;
-          const T cn = T(0.5) * fw * so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+          const T lo = T(0.5) * eta * T(0.5) * fJ * so[C::oC + end] / detJ;
+          const T ln = T(0.5) * eta * T(0.5) * fJ * so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
 #pragma unroll
-          for (int r = 1; r < 5; ++r) fz[(r - 1) * NQF] = co * ro[r] + cn * rn[r];
+          for (int r = 1; r < 5; ++r) fa[r * NQF] += lo * ro[r] + ln * rn[r];
         }
-        if (fq == 0) sMisc[j] = T(0.5);
       } else {
         T Ub[5];
         const int bad = boundary_state(nb, Uo, n, prm, Ub);
@@ -519,46 +517,17 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ub[r];
           dual_consistency_ref(Uo, d, n, mu, Ji, fw, fb, NQF);
           visc_jump_n(Ub, d, n, mu, rb);
-          const T co = fw * so[C::oC + end] / detJ;
+          const T lb = eta * fJ * so[C::oC + end] / detJ;
 #pragma unroll
-          for (int r = 1; r < 5; ++r) fz[(r - 1) * NQF] = co * rb[r];
+          for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
         }
-        if (fq == 0) sMisc[j] = T(1);
       }
       if (mu == T(0)) {
 #pragma unroll
         for (int i = 0; i < 12; ++i) fb[i * NQF] = T(0);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) fz[r * NQF] = T(0);
       }
-    }
-    __syncthreads();
-    if (tid < NH) {  // lifting operator, first face direction
-      const int j = tid / NQF, fq = tid % NQF, q1 = fq % P, q2 = fq / P;
-      const T* fz = Fz + j * 4 * NQF;
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        T s = T(0);
-#pragma unroll
-        for (int k = 0; k < P; ++k) s = fma(K[q1 * P + k], fz[v * NQF + k + P * q2], s);
-        Fz2[(j * 4 + v) * NQF + fq] = s;
-      }
-    }
-    __syncthreads();
-    if (tid < NH) {  // second direction; a = (F - Qhat.n) fJ w
-      const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P;
-      const T fw = sg[kGeoFJ + lf] * w1[q1] * w1[q2];
-      const T ef = T(prm.eta) * sMisc[j];
-      T* fa = Fa + j * 5 * NQF;
-      const T* fz2 = Fz2 + j * 4 * NQF;
-      fa[fq] *= fw;
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        T s = T(0);
-#pragma unroll
-        for (int k = 0; k < P; ++k) s = fma(K[q2 * P + k], fz2[v * NQF + q1 + P * k], s);
-        fa[(v + 1) * NQF + fq] = (fa[(v + 1) * NQF + fq] + ef * s) * fw;
-      }
+      for (int r = 0; r < 5; ++r) fa[r * NQF] *= fw;
     }
     __syncthreads();
     if (tid < NH) {  // test functions, first tangential direction: items (j, t1, q2)
