@@ -102,7 +102,7 @@ long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == D
 void free_all(dgb_handle* h)
 {
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
+  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
                   h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
                   h->d_counter, h->d_flag};
   for (void* p : ptrs)
@@ -204,10 +204,10 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   h->NQF = h->P * h->P;
   h->E = (long)mesh->nx * mesh->ny * mesh->nz;
   h->n = (long long)h->E * 5 * h->NB;
-  std::vector<double> geo;
+  std::vector<double> geo, gv, gf;
   std::vector<int32_t> nbr;
   std::string why;
-  rc = build_geometry(*mesh, h->ops, geo, nbr, why);
+  rc = build_geometry(*mesh, h->ops, geo, nbr, why, h->curved, gv, gf);
   if (rc) {
     delete h;
     return fail(rc, why);
@@ -257,6 +257,12 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMemcpy(h->d_ops, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
   CKF(cudaMemcpy(h->d_geo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice));
   CKF(cudaMemcpy(h->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
+  if (h->curved) {
+    CKF(cudaMalloc(&h->d_gv, sizeof(double) * gv.size()));
+    CKF(cudaMalloc(&h->d_gf, sizeof(double) * gf.size()));
+    CKF(cudaMemcpy(h->d_gv, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice));
+    CKF(cudaMemcpy(h->d_gf, gf.data(), sizeof(double) * gf.size(), cudaMemcpyHostToDevice));
+  }
   CKF(cudaMemset(h->d_U, 0, sb));
   CKF(cudaMemset(h->d_counter, 0, sizeof(int)));
   CKF(cudaMemset(h->d_flag, 0, sizeof(int)));

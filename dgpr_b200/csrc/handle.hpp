@@ -28,6 +28,9 @@ struct dgb_handle {
   double* d_ops = nullptr;
   float* d_opsf = nullptr;    // operator table for the mixed form
   double* d_geo = nullptr;
+  bool curved = false;         // per-point geometry (non-affine elements)
+  double* d_gv = nullptr;      // [E][kVolC][P^3]
+  double* d_gf = nullptr;      // [E][6][kFaceC][P^2]
   int* d_nbr = nullptr;
   double* d_U = nullptr;      // resident state
   double* d_Us = nullptr;     // stage state
@@ -77,13 +80,15 @@ namespace dgb {
 
 inline KLaunch klaunch(const dgb_handle* h)
 {
-  KLaunch L;
+  KLaunch L{};
   L.P = h->P;
   L.precision = h->precision;
   L.E = h->E;
   L.ops = h->precision == DGB_MIXED_FP32 ? (const void*)h->d_opsf : (const void*)h->d_ops;
   L.opsd = h->d_ops;
   L.geo = h->d_geo;
+  L.gv = h->d_gv;
+  L.gf = h->d_gf;
   L.nbr = h->d_nbr;
   L.prm = h->dprm;
   return L;

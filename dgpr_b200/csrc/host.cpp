@@ -144,14 +144,8 @@ int build_ops(int p, Ops1D& o)
     }
   o.M1i = o.M1;
   if (invert_dense(P, o.M1i.data())) return DGB_ERR_GEOMETRY;
-  o.K.assign(P * P, 0.);
-  for (int a = 0; a < P; ++a)
-    for (int b = 0; b < P; ++b) {
-      double s = 0.;
-      for (int i = 0; i < P; ++i)
-        for (int j = 0; j < P; ++j) s += o.B[P * a + i] * o.M1i[P * i + j] * o.B[P * b + j];
-      o.K[P * a + b] = s;
-    }
+  o.Bi = o.B;  // B[q][i] -> Bi[i][q]
+  if (invert_dense(P, o.Bi.data())) return DGB_ERR_GEOMETRY;
   for (int e = 0; e < 2; ++e) {
     o.E[e].assign(P, 0.);
     o.D[e].assign(P, 0.);
@@ -163,6 +157,12 @@ int build_ops(int p, Ops1D& o)
     for (int i = 0; i < P; ++i)
       for (int j = 0; j < P; ++j) s += o.E[e][i] * o.M1i[P * i + j] * o.E[e][j];
     o.cend[e] = s;
+    o.EL[e].assign(P, 0.);
+    for (int q = 0; q < P; ++q) {
+      double v = 0.;
+      for (int i = 0; i < P; ++i) v += o.E[e][i] * o.Bi[P * i + q];
+      o.EL[e][q] = v;
+    }
   }
   o.Wb.assign(P, 0.);
   for (int i = 0; i < P; ++i) {
@@ -227,9 +227,93 @@ void jacobian(const double* X, int q, const double* r3, double* J)
 
 }  // namespace
 
-int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>& geo,
-                   std::vector<int32_t>& nbr, std::string& why)
+namespace {
+
+// face lf, tangential Gauss points (t1, t2) -> reference coordinates
+// (tangential axes in axis order: x faces (y,z), y faces (x,z), z faces (x,y))
+void face_point(const Ops1D& ops, int lf, int t1, int t2, double* r3)
 {
+  const int a = lf >> 1;
+  const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+  r3[a] = (double)(lf & 1);
+  r3[ax1] = ops.x[t1];
+  r3[ax2] = ops.x[t2];
+}
+
+// outward unit normal and surface Jacobian of face lf from the Jacobian at a
+// point of it: the face tangents are Jacobian columns, oriented as surf2vol
+// (basis.cpp:180-192) and compute_surface_geometry (geometry_common.cpp:416-454):
+// x faces (s,t) -> (y,z), y faces -> (z,x), z faces -> (x,y); low faces flipped
+void face_normal(const double* J, int lf, double* n, double* fj)
+{
+  const int a = lf >> 1;
+  const int c1 = a == 0 ? 1 : a == 1 ? 2 : 0;
+  const int c2 = a == 0 ? 2 : a == 1 ? 0 : 1;
+  const double ts[3] = {J[c1], J[3 + c1], J[6 + c1]};
+  const double tt[3] = {J[c2], J[3 + c2], J[6 + c2]};
+  double c[3];
+  cross(ts, tt, c);
+  *fj = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+  const double sg = (lf & 1) ? 1. : -1.;
+  for (int r = 0; r < 3; ++r) n[r] = sg * c[r] / *fj;
+}
+
+// per-point geometry of one element (layout in host.hpp)
+int curved_element(const double* X, int q, const Ops1D& ops, double* gv, double* gf, long e, std::string& why)
+{
+  const int P = ops.P, NB = P * P * P, NQF = P * P;
+  double J[9], Ji[9];
+  for (int k = 0; k < P; ++k)
+    for (int j = 0; j < P; ++j)
+      for (int i = 0; i < P; ++i) {
+        const int b = i + P * (j + P * k);
+        const double r3[3] = {ops.x[i], ops.x[j], ops.x[k]};
+        jacobian(X, q, r3, J);
+        const double dJ = det3(J);
+        if (!(dJ > 0.) || !std::isfinite(dJ)) {
+          char buf[120];
+          snprintf(buf, sizeof buf, "element %ld has a non-positive Jacobian determinant", e);
+          why = buf;
+          return DGB_ERR_GEOMETRY;
+        }
+        inv3(J, Ji);
+        for (int c = 0; c < 9; ++c) gv[c * NB + b] = Ji[c];
+        gv[kVolDetJ * NB + b] = dJ;
+      }
+  for (int lf = 0; lf < 6; ++lf) {
+    const int a = lf >> 1, end = lf & 1;
+    for (int t2 = 0; t2 < P; ++t2)
+      for (int t1 = 0; t1 < P; ++t1) {
+        const int fq = t1 + P * t2;
+        double r3[3], n[3], fj;
+        face_point(ops, lf, t1, t2, r3);
+        jacobian(X, q, r3, J);
+        inv3(J, Ji);
+        face_normal(J, lf, n, &fj);
+        double* g = gf + (size_t)lf * kFaceC * NQF;
+        for (int c = 0; c < 9; ++c) g[c * NQF + fq] = Ji[c];
+        for (int c = 0; c < 3; ++c) g[(kFaceN + c) * NQF + fq] = n[c];
+        g[kFaceFJ * NQF + fq] = fj;
+        double lift = 0.;
+        for (int ia = 0; ia < P; ++ia) {
+          const int b = a == 0 ? ia + P * (t1 + P * t2) : a == 1 ? t1 + P * (ia + P * t2) : t1 + P * (t2 + P * ia);
+          lift += ops.EL[end][ia] * ops.EL[end][ia] / (ops.w[ia] * gv[kVolDetJ * NB + b]);
+        }
+        g[kFaceLift * NQF + fq] = lift;
+      }
+  }
+  return DGB_OK;
+}
+
+}  // namespace
+
+int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>& geo,
+                   std::vector<int32_t>& nbr, std::string& why, bool& curved, std::vector<double>& gv,
+                   std::vector<double>& gf)
+{
+  curved = false;
+  gv.clear();
+  gf.clear();
   const int nx = m.nx, ny = m.ny, nz = m.nz, q = m.q, P = ops.P;
   if (nx <= 0 || ny <= 0 || nz <= 0 || q < 1 || q > 7 || !m.nodes) {
     why = "mesh sizes must be positive and 1 <= q <= 7";
@@ -277,15 +361,10 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     jacobian(X, q, centre, J0);
     double scale = 0.;
     for (int i = 0; i < 9; ++i) scale = std::fmax(scale, std::fabs(J0[i]));
-    for (int s = 0; s < npts; ++s) {
+    for (int s = 0; s < npts && !curved; ++s) {
       jacobian(X, q, &pts[3 * s], J);
       for (int i = 0; i < 9; ++i)
-        if (std::fabs(J[i] - J0[i]) > 1e-11 * scale) {
-          char buf[160];
-          snprintf(buf, sizeof buf, "element %ld has a non-constant Jacobian (curved geometry)", e);
-          why = buf;
-          return DGB_ERR_UNSUPPORTED;
-        }
+        if (std::fabs(J[i] - J0[i]) > 1e-11 * scale) curved = true;
     }
     double* g = &geo[(size_t)e * kGeoStride];
     const double dJ = det3(J0);
@@ -297,21 +376,16 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     }
     inv3(J0, g + kGeoJinv);
     g[kGeoDetJ] = dJ;
-    // face tangents are Jacobian columns; orientation as surf2vol
-    // (basis.cpp:180-192) and compute_surface_geometry (geometry_common.cpp:416-454):
-    // x faces (s,t) -> (y,z), y faces -> (z,x), z faces -> (x,y); low faces flipped
-    for (int lf = 0; lf < 6; ++lf) {
-      const int a = lf >> 1;
-      const int c1 = a == 0 ? 1 : a == 1 ? 2 : 0;
-      const int c2 = a == 0 ? 2 : a == 1 ? 0 : 1;
-      const double ts[3] = {J0[c1], J0[3 + c1], J0[6 + c1]};
-      const double tt[3] = {J0[c2], J0[3 + c2], J0[6 + c2]};
-      double n[3];
-      cross(ts, tt, n);
-      const double fj = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-      const double sg = (lf & 1) ? 1. : -1.;
-      for (int r = 0; r < 3; ++r) g[kGeoN + 3 * lf + r] = sg * n[r] / fj;
-      g[kGeoFJ + lf] = fj;
+    for (int lf = 0; lf < 6; ++lf) face_normal(J0, lf, g + kGeoN + 3 * lf, g + kGeoFJ + lf);
+  }
+  if (curved) {
+    const int NB = P * P * P, NQF = P * P;
+    gv.assign((size_t)E * kVolC * NB, 0.);
+    gf.assign((size_t)E * 6 * kFaceC * NQF, 0.);
+    for (long e = 0; e < E; ++e) {
+      const int rc = curved_element(m.nodes + (size_t)e * nq * 3, q, ops, &gv[(size_t)e * kVolC * NB],
+                                    &gf[(size_t)e * 6 * kFaceC * NQF], e, why);
+      if (rc) return rc;
     }
   }
 
@@ -339,6 +413,24 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     for (int lf = 0; lf < 6; ++lf) {
       const int en = nbr[6 * e + lf];
       if (en < 0) continue;
+      if (curved) {  // point by point
+        const int NQF = P * P;
+        const double* g = &gf[((size_t)e * 6 + lf) * kFaceC * NQF];
+        const double* h = &gf[((size_t)en * 6 + (lf ^ 1)) * kFaceC * NQF];
+        for (int fq = 0; fq < NQF; ++fq) {
+          double dn = 0.;
+          for (int r = 0; r < 3; ++r)
+            dn = std::fmax(dn, std::fabs(g[(kFaceN + r) * NQF + fq] + h[(kFaceN + r) * NQF + fq]));
+          const double df = std::fabs(g[kFaceFJ * NQF + fq] - h[kFaceFJ * NQF + fq]) / g[kFaceFJ * NQF + fq];
+          if (dn > 1e-10 || df > 1e-10) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "face %d of element %ld does not match its neighbour %d", lf, e, en);
+            why = buf;
+            return DGB_ERR_GEOMETRY;
+          }
+        }
+        continue;
+      }
       const double* g = &geo[(size_t)e * kGeoStride];
       const double* h = &geo[(size_t)en * kGeoStride];
       const int lo = lf ^ 1;

@@ -32,12 +32,24 @@ struct Ops1D {
   std::vector<double> Dq;     // Dq[q][k] = L_k'(x_q), L_k the Lagrange basis on the GL nodes
   std::vector<double> M1;     // M1[i][j] = sum_q w_q l_i(x_q) l_j(x_q)
   std::vector<double> M1i;    // inverse of M1
-  std::vector<double> K;      // K = B M1i B^T  (face lifting factor)
+  std::vector<double> Bi;     // Bi[i][q] = (B^-1)[i][q]: nodal coefficients from values at the GL nodes
   std::vector<double> E[2];   // E[end][i] = l_i(end), end 0 -> xi=0, 1 -> xi=1
   std::vector<double> D[2];   // D[end][i] = l_i'(end)
   std::vector<double> Wb;     // Wb[i] = sum_q w_q l_i(x_q)
   double cend[2] = {0, 0};    // E[end]^T M1i E[end]
+  std::vector<double> EL[2];  // EL[end][q] = (E[end] B^-1)[q]: value at xi = end of the
+                              // Lagrange polynomial through the GL nodes that is 1 at node q
 };
+
+// Curved (non-affine) elements carry their geometry per point:
+//   volume   gv[e][c][P^3]      c < kVolC:  Jinv[9] (row-major d xi_i / d x_c), detJ
+//   faces    gf[e][lf][c][P^2]  c < kFaceC: Jinv[9], outward unit normal[3],
+//                               surface Jacobian, BR2 lifting scale
+// The lifting scale of a face point is the diagonal of the face-restricted
+// lifting operator E_f Minv E_f^T times w_t1 w_t2:
+//   sum_a EL[end][a]^2 / (w_a detJ(a, t1, t2))   (= cend / detJ when affine).
+constexpr int kVolC = 10, kVolDetJ = 9;
+constexpr int kFaceC = 14, kFaceN = 9, kFaceFJ = 12, kFaceLift = 13;
 
 int build_ops(int p, Ops1D& ops);
 
@@ -48,14 +60,17 @@ double lagrange1d(int i, int p, double x);
 double lagrange1d_deriv(int i, int p, double x);
 void gauss_legendre(int n, double a, double b, double* x, double* w);
 
-// Affine element geometry + neighbour table for a structured nx*ny*nz mesh.
-//   geo[e*kGeoStride + ...]  as documented above
+// Element geometry + neighbour table for a structured nx*ny*nz mesh.
+//   geo[e*kGeoStride + ...]  affine record as documented above (Jacobian at the
+//                            element centre)
 //   nbr[e*6 + lf]            neighbour element (>= 0) or btype code (< 0)
-// Returns DGB_ERR_UNSUPPORTED for elements whose Jacobian is not constant
-// (curved geometry), DGB_ERR_GEOMETRY for singular Jacobians or mismatched
-// periodic sides.
+// When some element's Jacobian is not constant (curved geometry) `curved` is
+// set and gv / gf receive the per-point geometry of every element (layout
+// above); otherwise they are left empty.  Returns DGB_ERR_GEOMETRY for
+// singular Jacobians or faces that do not match their neighbour's.
 int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>& geo,
-                   std::vector<int32_t>& nbr, std::string& why);
+                   std::vector<int32_t>& nbr, std::string& why, bool& curved, std::vector<double>& gv,
+                   std::vector<double>& gf);
 
 // Total conditions used by the subsonic inflow state (solve.cpp:167-175).
 void total_conditions(const dgb_params& prm, double* Tt, double* Pt);

@@ -47,8 +47,8 @@ struct Cfg {
   static constexpr int NQF = P * P;     // face quadrature points
   static constexpr int NH = 3 * NQF;    // face points of half an element (3 faces)
   static constexpr int NT = (((NB > NH ? NB : NH) + 31) / 32) * 32;
-  // operator table: B Bd Dq M1i K (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2]
-  static constexpr int oB = 0, oBd = P * P, oDq = 2 * P * P, oMi = 3 * P * P, oK = 4 * P * P;
+  // operator table: B Bd Dq M1i Bi (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2]
+  static constexpr int oB = 0, oBd = P * P, oDq = 2 * P * P, oMi = 3 * P * P, oBi = 4 * P * P;
   static constexpr int oE = 5 * P * P, oD = oE + 2 * P, oWb = oD + 2 * P, oW = oWb + P;
   static constexpr int oC = oW + P;
   static constexpr int OPS = oC + 2;
@@ -163,9 +163,11 @@ __device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, con
 // sY[3][15][NQF].  Both the trace kernel and the stage kernel's epilogue call
 // this, so a trace is bit-identical whichever of them produced it.
 // sg: element geometry record in T (Jinv, detJ, normals, surface Jacobians).
-template <int P, class T>
+// CV (curved elements): the inverse Jacobian and normal of each face point
+// come from gfe, this element's per-point face geometry [6][kFaceC][P*P].
+template <int P, class T, bool CV>
 __device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY, const T* so, const T* sg,
-                                           T mu, T* __restrict__ Te)
+                                           T mu, T* __restrict__ Te, const double* __restrict__ gfe)
 {
   using C = Cfg<P>;
   constexpr int NB = C::NB, NQF = C::NQF, NH = C::NH;
@@ -235,14 +237,25 @@ __device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY,
     }
     T Qn[5] = {T(0), T(0), T(0), T(0), T(0)};
     if (mu != T(0)) {
-      const T* Ji = sg + kGeoJinv;
+      T Ji[9], n[3];
+      if constexpr (CV) {
+        const double* gp = gfe + lf * kFaceC * NQF + fq;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) Ji[c] = T(gp[c * NQF]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) n[c] = T(gp[(kFaceN + c) * NQF]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) Ji[c] = sg[kGeoJinv + c];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) n[c] = sg[kGeoN + 3 * lf + c];
+      }
       T G[3][5], Q[3][5];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int r = 0; r < 5; ++r) G[c][r] = Ji[c] * g[0][r] + Ji[3 + c] * g[1][r] + Ji[6 + c] * g[2][r];
       visc_flux(S, G, mu, Q);
-      const T* n = sg + kGeoN + 3 * lf;
 #pragma unroll
       for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
     }
@@ -267,10 +280,10 @@ struct TraceSmem {
 };
 
 // Face traces of U (FP64 in HBM) into Tr[e][lf][10][P*P] (type T).
-template <int P, class T>
+template <int P, class T, bool CV>
 __global__ void __launch_bounds__(Cfg<P>::NT)
 trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, const double* __restrict__ geo,
-             T* __restrict__ Tr, DevParams prm)
+             const double* __restrict__ gf, T* __restrict__ Tr, DevParams prm)
 {
   using C = Cfg<P>;
   using L = TraceSmem<P, T>;
@@ -290,7 +303,8 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
   __syncthreads();
   T* Te = Tr + e * 60 * NQF;
 #pragma unroll 1
-  for (int half = 0; half < 2; ++half) trace_half<P, T>(half, sU, sN, sY, so, sg, T(prm.mu), Te);
+  for (int half = 0; half < 2; ++half)
+    trace_half<P, T, CV>(half, sU, sN, sY, so, sg, T(prm.mu), Te, CV ? gf + e * 6 * kFaceC * NQF : nullptr);
 }
 
 // ------------------------------------------------------------- stage kernel
@@ -333,11 +347,15 @@ struct StageSmem {
   static_assert(oTrU >= MINV, "epilogue state must not overlap the inverse-mass buffers");
 };
 
-template <int P, class T>
+// CV (curved elements): geometry per point from gv [E][kVolC][P^3] and
+// gf [E][6][kFaceC][P^2]; the inverse mass matrix of such an element is
+// B3^-1 diag(1/(w detJ)) B3^-T (its mass matrix is B3^T diag(w detJ) B3 with
+// B3 = B x B x B square), applied as six 1D contractions and a scaling.
+template <int P, class T, bool CV>
 __global__ void __launch_bounds__(Cfg<P>::NT, (MinBlocks<P, T>::value))
 stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __restrict__ opsg,
-             const double* __restrict__ opsd, const double* __restrict__ geo, const int* __restrict__ nbr,
-             DevParams prm, StageArgs sa)
+             const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
+             const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm, StageArgs sa)
 {
   using C = Cfg<P>;
   using L = StageSmem<P, T>;
@@ -356,7 +374,7 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   T* V1 = sX + 5 * NB;
   T* G = sX + 10 * NB;
   for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < P * P; i += blockDim.x) sMi[i] = opsd[C::oMi + i];
+  for (int i = tid; i < P * P; i += blockDim.x) sMi[i] = opsd[(CV ? C::oBi : C::oMi) + i];
   for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
   const double* Ue = Us + e * 5 * NB;
   for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = T(Ue[i]);
@@ -370,6 +388,9 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   const T* Ji = sg + kGeoJinv;
   const T gamma = T(prm.gamma), mu = T(prm.mu);
   T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // residual of node tid
+  const double* gve = CV ? gv + e * kVolC * NB : nullptr;
+  const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
+  T wJq = T(0);  // w detJ at quadrature point tid (curved elements: for the source)
 
   // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
   if (node) contract<P, 0, false, false>(B, V0, V1, tid);
@@ -387,14 +408,24 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   if (node) {  // pointwise flux at quadrature point tid
     const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
     const T* w = so + C::oW;
-    const T wJ = w[qx] * w[qy] * w[qz] * detJ;
+    T Jbuf[9];
+    T wJ;
+    if constexpr (CV) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Jbuf[c] = T(gve[c * NB + tid]);
+      wJ = w[qx] * w[qy] * w[qz] * T(gve[kVolDetJ * NB + tid]);
+      wJq = wJ;
+    } else {
+      wJ = w[qx] * w[qy] * w[qz] * detJ;
+    }
+    const T* Jq = CV ? Jbuf : Ji;  // inverse Jacobian at this point
     T S[5], Gp[3][5], H[3][5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       S[r] = V1[r * NB + tid];
       const T g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Gp[c][r] = Ji[c] * g0 + Ji[3 + c] * g1 + Ji[6 + c] * g2;
+      for (int c = 0; c < 3; ++c) Gp[c][r] = Jq[c] * g0 + Jq[3 + c] * g1 + Jq[6 + c] * g2;
     }
     euler_flux(S, gamma, H);
     if (mu != T(0)) {
@@ -415,13 +446,17 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int r = 0; r < 5; ++r)
-        G[i * 5 * NB + r * NB + tid] = wJ * (Ji[3 * i] * H[0][r] + Ji[3 * i + 1] * H[1][r] + Ji[3 * i + 2] * H[2][r]);
+        G[i * 5 * NB + r * NB + tid] = wJ * (Jq[3 * i] * H[0][r] + Jq[3 * i + 1] * H[1][r] + Jq[3 * i + 2] * H[2][r]);
   }
   __syncthreads();
   if (node) {  // sum_i Dq_i^T Ghat_i
     contract<P, 0, true, false>(Dq, G, V0, tid);
     contract<P, 1, true, true>(Dq, G + 5 * NB, V0, tid);
     contract<P, 2, true, true>(Dq, G + 10 * NB, V0, tid);
+    if constexpr (CV) {  // source, tested at the quadrature points with w detJ
+#pragma unroll
+      for (int r = 0; r < 5; ++r) V0[r * NB + tid] -= T(prm.src[r]) * wJq;
+    }
   }
   __syncthreads();
   if (node) contract<P, 0, true, false>(B, V0, V1, tid);
@@ -430,11 +465,13 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   __syncthreads();
   if (node) {
     contract_reg<P, 2, true>(B, V0, tid, Rv);
-    const T* Wb = so + C::oWb;
-    const int ix = tid % P, iy = (tid / P) % P, iz = tid / (P * P);
-    const T ws = Wb[ix] * Wb[iy] * Wb[iz] * detJ;
+    if constexpr (!CV) {
+      const T* Wb = so + C::oWb;
+      const int ix = tid % P, iy = (tid / P) % P, iz = tid / (P * P);
+      const T ws = Wb[ix] * Wb[iy] * Wb[iz] * detJ;
 #pragma unroll
-    for (int r = 0; r < 5; ++r) Rv[r] -= T(prm.src[r]) * ws;
+      for (int r = 0; r < 5; ++r) Rv[r] -= T(prm.src[r]) * ws;
+    }
   }
   __syncthreads();
 
@@ -453,8 +490,16 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   for (int half = 0; half < 2; ++half) {
     if (tid < NH) {
       const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
-      const T* n = sg + kGeoN + 3 * lf;
-      const T fJ = sg[kGeoFJ + lf];
+      // geometry of this face point (affine elements: the element's, in shared
+      // memory; curved ones: per point, each value loaded where it is used)
+      const double* gp = CV ? gfe + lf * kFaceC * NQF + fq : nullptr;
+      T nbuf[3];
+      if constexpr (CV) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nbuf[c] = T(gp[(kFaceN + c) * NQF]);
+      }
+      const T* n = CV ? nbuf : sg + kGeoN + 3 * lf;
+      const T fJ = CV ? T(gp[kFaceFJ * NQF]) : sg[kGeoFJ + lf];
       const T fw = fJ * w1[q1] * w1[q2];
       const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
       T Uo[5], Qo[5];
@@ -490,14 +535,27 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
           T d[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - T(0.5) * (Uo[r] + Un[r]);  // Uo - Uhat
-          dual_consistency_ref(Uo, d, n, mu, Ji, fw, fb, NQF);
+          {
+            T Jbuf[9];
+            if constexpr (CV) {
+#pragma unroll
+              for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
+            }
+            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF);
+          }
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
           T ro[5], rn[5];
           visc_jump_n(Uo, d, n, mu, ro);  // BR2 lifting sources of both sides
           visc_jump_n(Un, d, n, mu, rn);
-          const T lo = T(0.5) * eta * T(0.5) * fJ * so[C::oC + end] / detJ;
-          const T ln = T(0.5) * eta * T(0.5) * fJ * so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+          T lift_n;  // the neighbour's lifting scale at this face point
+          if constexpr (CV)
+            lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
+          else
+            lift_n = so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+          const T lift = CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ;
+          const T lo = T(0.5) * eta * T(0.5) * fJ * lift;
+          const T ln = T(0.5) * eta * T(0.5) * fJ * lift_n;
 #pragma unroll
           for (int r = 1; r < 5; ++r) fa[r * NQF] += lo * ro[r] + ln * rn[r];
         }
@@ -515,9 +573,16 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
           T d[5], rb[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ub[r];
-          dual_consistency_ref(Uo, d, n, mu, Ji, fw, fb, NQF);
+          {
+            T Jbuf[9];
+            if constexpr (CV) {
+#pragma unroll
+              for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
+            }
+            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF);
+          }
           visc_jump_n(Ub, d, n, mu, rb);
-          const T lb = eta * fJ * so[C::oC + end] / detJ;
+          const T lb = eta * fJ * (CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ);
 #pragma unroll
           for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
         }
@@ -633,15 +698,37 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     for (int r = 0; r < 5; ++r) M0[r * NB + tid] = double(Rv[r]);
   }
   __syncthreads();
-  if (node) contract<P, 0, false, false>(sMi, M0, M1, tid);
+  if constexpr (CV) {  // B3^-T, 1/(w detJ), then B3^-1 (the last direction below)
+    if (node) contract<P, 0, true, false>(sMi, M0, M1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, true, false>(sMi, M1, M0, tid);
+    __syncthreads();
+    if (node) {
+      contract<P, 2, true, false>(sMi, M0, M1, tid);
+      const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+      const double iw = 1.0 / (opsd[C::oW + qx] * opsd[C::oW + qy] * opsd[C::oW + qz] * gve[kVolDetJ * NB + tid]);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) M1[r * NB + tid] *= iw;
+    }
+    __syncthreads();
+    if (node) contract<P, 0, false, false>(sMi, M1, M0, tid);
+    __syncthreads();
+  }
+  if (node) contract<P, CV ? 1 : 0, false, false>(sMi, M0, M1, tid);
   __syncthreads();
-  if (node) contract<P, 1, false, false>(sMi, M1, M0, tid);
+  if (node) contract<P, CV ? 2 : 1, false, false>(sMi, M1, M0, tid);
   __syncthreads();
   T* sUn = reinterpret_cast<T*>(sXb + L::oTrU);  // new state for the epilogue traces
   if (node) {
     double f[5];
-    contract_reg<P, 2, false>(sMi, M0, tid, f);
-    const double sc = -1.0 / detJd;
+    if constexpr (CV) {
+      // all three directions of B3^-1 are done; copy out
+#pragma unroll
+      for (int r = 0; r < 5; ++r) f[r] = M0[r * NB + tid];
+    } else {
+      contract_reg<P, 2, false>(sMi, M0, tid, f);
+    }
+    const double sc = CV ? -1.0 : -1.0 / detJd;
     const long base = e * 5 * NB;
     const double dt = sa.dt;
 #pragma unroll
@@ -690,7 +777,7 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     __syncthreads();
     T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
 #pragma unroll 1
-    for (int half = 0; half < 2; ++half) trace_half<P, T>(half, sUn, sX, sX + 30 * NQF, so, sg, mu, Te);
+    for (int half = 0; half < 2; ++half) trace_half<P, T, CV>(half, sUn, sX, sX + 30 * NQF, so, sg, mu, Te, gfe);
   }
 }
 
@@ -699,18 +786,29 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
 template <int P, class T>
 cudaError_t prepare_p()
 {
-  cudaError_t e = cudaFuncSetAttribute(trace_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(trace_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TraceSmem<P, T>::TOTAL);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              StageSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(trace_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TraceSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(stage_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             StageSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(stage_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             StageSmem<P, T>::TOTAL);
+  return e;
 }
 
 template <int P, class T>
 cudaError_t launch_trace_p(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
 {
-  trace_kernel<P, T><<<(unsigned)L.E, Cfg<P>::NT, TraceSmem<P, T>::TOTAL, st>>>(
-      L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, reinterpret_cast<T*>(Tout), L.prm);
+  if (L.gf)
+    trace_kernel<P, T, true><<<(unsigned)L.E, Cfg<P>::NT, TraceSmem<P, T>::TOTAL, st>>>(
+        L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, L.gf, reinterpret_cast<T*>(Tout), L.prm);
+  else
+    trace_kernel<P, T, false><<<(unsigned)L.E, Cfg<P>::NT, TraceSmem<P, T>::TOTAL, st>>>(
+        L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, nullptr, reinterpret_cast<T*>(Tout), L.prm);
   return cudaGetLastError();
 }
 
@@ -718,9 +816,14 @@ template <int P, class T>
 cudaError_t launch_stage_p(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                            cudaStream_t st)
 {
-  stage_kernel<P, T><<<(unsigned)L.E, Cfg<P>::NT, StageSmem<P, T>::TOTAL, st>>>(
-      L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.nbr, L.prm,
-      sa);
+  if (L.gv)
+    stage_kernel<P, T, true><<<(unsigned)L.E, Cfg<P>::NT, StageSmem<P, T>::TOTAL, st>>>(
+        L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
+        L.nbr, L.prm, sa);
+  else
+    stage_kernel<P, T, false><<<(unsigned)L.E, Cfg<P>::NT, StageSmem<P, T>::TOTAL, st>>>(
+        L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
+        nullptr, L.nbr, L.prm, sa);
   return cudaGetLastError();
 }
 

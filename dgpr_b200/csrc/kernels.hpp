@@ -41,6 +41,8 @@ struct KLaunch {
   const void* ops;     // packed 1D operator table in the compute type (pack_ops)
   const double* opsd;  // the same table in FP64 (inverse mass matrix)
   const double* geo;   // [E][kGeoStride]
+  const double* gv;    // curved meshes: per-point volume geometry [E][kVolC][P^3], else null
+  const double* gf;    // curved meshes: per-point face geometry [E][6][kFaceC][P^2], else null
   const int* nbr;      // [E][6]
   DevParams prm;
 };

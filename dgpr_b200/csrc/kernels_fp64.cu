@@ -16,7 +16,7 @@ void pack_ops(const Ops1D& o, double* t)
     t[PP + i] = o.Bd[i];
     t[2 * PP + i] = o.Dq[i];
     t[3 * PP + i] = o.M1i[i];
-    t[4 * PP + i] = o.K[i];
+    t[4 * PP + i] = o.Bi[i];
   }
   const int oE = 5 * PP, oD = oE + 2 * P, oWb = oD + 2 * P, oW = oWb + P, oC = oW + P;
   for (int i = 0; i < P; ++i) {

@@ -54,11 +54,14 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   Ops1D ops;
   int rc = build_ops(mesh->p, ops);
   if (rc) return set_last_error(rc, "solution order outside 0..6");
-  std::vector<double> geo;
+  std::vector<double> geo, gv, gf;
   std::vector<int32_t> nbr;
   std::string why;
-  rc = build_geometry(*mesh, ops, geo, nbr, why);
+  bool curved = false;
+  rc = build_geometry(*mesh, ops, geo, nbr, why, curved, gv, gf);
   if (rc) return set_last_error(rc, why);
+  if (curved)
+    return set_last_error(DGB_ERR_UNSUPPORTED, "curved elements need per-point geometry: use dgb_create");
   const int P = ops.P, NQF = P * P;
   const long E = (long)mesh->nx * mesh->ny * mesh->nz;
   std::vector<double> table(ops_table_size(P));
@@ -110,7 +113,7 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   NA_CK(cudaMemcpyAsync(base + oNbr, nbr.data(), sizeof(int32_t) * nbr.size(), cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));  // status word must start at zero
 
-  KLaunch L;
+  KLaunch L{};
   L.P = P;
   L.precision = DGB_FP64;
   L.E = E;

@@ -42,6 +42,42 @@ def box_nodes(nx, ny, nz, q, lx, ly, lz, shear=0.0):
     return X.ravel()
 
 
+def sine_nodes(nx, ny, nz, q, lx, ly, lz, amp, walls=False):
+    """Curved order-q elements: equispaced box nodes with y displaced by
+    amp sin(2 pi x / lx) sin(2 pi z / lz), times (1 - (2y/ly - 1)^2) when the
+    y sides are walls (they stay flat).  Periodic in x and z, and in y too
+    without the wall factor.  The reference has no generator for this mesh;
+    its nodes reach it as a .dg node array (io.cpp:131-136)."""
+    X = box_nodes(nx, ny, nz, q, lx, ly, lz).reshape(-1, 3)
+    d = amp * np.sin(2 * math.pi * X[:, 0] / lx) * np.sin(2 * math.pi * X[:, 2] / lz)
+    if walls:
+        d *= 1.0 - (2.0 * X[:, 1] / ly - 1.0) ** 2
+    X[:, 1] += d
+    return X.ravel()
+
+
+def bump_nodes(nx, ny, nz, q, lx, ly, lz, height=0.1, center=1.0, variance=0.05):
+    """The reference's bump channel (generate_bump_nodes,
+    geometry_common.cpp:494-576, no stretching), restated here so the cases
+    need no library."""
+    Q = q + 1
+    X = np.zeros((nz, ny, nx, Q, Q, Q, 3))
+    elx, ely, elz = lx / nx, ly / ny, lz / nz
+    nsx, nsy, nsz = elx / q, ely / q, elz / q
+    for ez in range(nz):
+        for ey in range(ny):
+            for ex in range(nx):
+                for k in range(Q):
+                    for j in range(Q):
+                        for i in range(Q):
+                            x = ex * elx + nsx * i
+                            y = ey * ely + nsy * j
+                            z = ez * elz + nsz * k
+                            f = height * math.exp(-((x - center) * (x - center)) / (2.0 * variance))
+                            X[ez, ey, ex, k, j, i] = (x, (y / ly) * (ly - f) + f, z)
+    return X.ravel()
+
+
 def node_coords(nx, ny, nz, p, q, nodes):
     """Physical coordinates of the solution nodes (equispaced reference nodes
     i/p mapped through the order-q geometry), shape [E][nb][3]."""
@@ -135,6 +171,20 @@ def residual_cases():
     add("p6", 1, 1, 2, 6, 1, (0.5, 0.5, 1.0), [P_] * 6, visc)
     add("euler_p2", 2, 2, 2, 2, 1, (1.0, 1.0, 1.0), [P_] * 6, params(mu=0.0, u=0.3, v=0.2))
     add("source_p2", 2, 2, 2, 2, 1, (1.0, 1.0, 1.0), [P_] * 6, params(mu=1e-2, source=(0.0, 0.3, 0.0, 0.0, 0.0)))
+
+    # curved (non-affine) elements: per-point geometry
+    def add_curved(name, nx, ny, nz, p, q, nodes, bounds, prm, amp=0.05):
+        U = random_state(prm, nx * ny * nz, (p + 1) ** 3, rng, amp)
+        out.append(Case(name, nx, ny, nz, p, q, nodes, bounds, prm, U))
+
+    add_curved("bump_p2_q2", 3, 2, 2, 2, 2, bump_nodes(3, 2, 2, 2, 2.0, 1.0, 0.5),
+               [F_, F_, NS_, W_, P_, P_], params(mu=1e-2, u=0.3))
+    add_curved("bump_p3_q3", 3, 2, 1, 3, 3, bump_nodes(3, 2, 1, 3, 2.0, 1.0, 0.5),
+               [F_, F_, W_, F_, P_, P_], params(mu=5e-3, u=0.3, source=(0.0, 0.2, 0.0, 0.0, 0.0)))
+    add_curved("sine_periodic_p2_q2", 2, 2, 2, 2, 2, sine_nodes(2, 2, 2, 2, 1.0, 1.0, 1.0, 0.04),
+               [P_] * 6, visc)
+    add_curved("sine_euler_p3_q2", 2, 2, 2, 3, 2, sine_nodes(2, 2, 2, 2, 1.0, 1.0, 1.0, 0.04),
+               [P_] * 6, params(mu=0.0, u=0.3, v=0.2))
     return out
 
 
@@ -164,5 +214,11 @@ def run_cases():
     prm = params(mu=1e-2, u=0.3)
     U = random_state(prm, 12, 27, rng, 0.02)
     out.append(Case("channel_tvdrk3", 3, 2, 2, 2, 1, nodes, [IN_, OUT_, NS_, W_, P_, P_], prm, U,
+                    scheme=1, dt=2e-3, nsteps=5))
+    # sinusoidally mapped channel (curved q = 3 elements), no-slip walls, body force
+    nodes = sine_nodes(3, 2, 2, 3, 2.0, 1.0, 1.0, 0.05, walls=True)
+    prm = params(mu=1e-2, u=0.3, source=(0.0, 0.05, 0.0, 0.0, 0.0))
+    U = random_state(prm, 12, 27, rng, 0.02)
+    out.append(Case("sine_channel_tvdrk3", 3, 2, 2, 2, 3, nodes, [P_, P_, NS_, NS_, P_, P_], prm, U,
                     scheme=1, dt=2e-3, nsteps=5))
     return out

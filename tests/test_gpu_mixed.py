@@ -29,7 +29,8 @@ def solver(c, precision):
 
 @pytest.mark.parametrize("case", [c for c in C.residual_cases() if c.name in
                                   ("periodic_p2", "periodic_p3_q2", "sheared_p2", "walls_inout_p2",
-                                   "freestream_p2", "noslip_p3", "p4", "euler_p2", "source_p2")],
+                                   "freestream_p2", "noslip_p3", "p4", "euler_p2", "source_p2",
+                                   "bump_p2_q2", "sine_periodic_p2_q2")],
                          ids=lambda c: c.name)
 def test_mixed_residual_close_to_oracle(case):
     with solver(case, dg.MIXED_FP32) as s:
