@@ -57,7 +57,7 @@ def build(verbose=False, jobs=None):
     if os.path.exists(main_src):
         exe = os.path.join(LIB, "dgb")
         subprocess.check_call([_nvcc()] + ARCH + FLAGS + ["-x", "cu", main_src, "-o", exe, "-L" + LIB,
-                               "-ldgb200", "-Xlinker", "-rpath='$ORIGIN'"])
+                               "-ldgb200", "-Xlinker", "-rpath=$ORIGIN"])
     return so
 
 

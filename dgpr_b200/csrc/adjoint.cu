@@ -208,6 +208,9 @@ struct AdjASmem {
   // faces: sN[3][10] sY[3][15] (x NQF)
   static constexpr int FACE = 75 * NQF;
   static constexpr int TOTAL = oX + (VOL > FACE ? VOL : FACE);
+  // contractions read lines of even P with 16-byte loads: tiles must start on
+  // even double offsets
+  static_assert(P % 2 == 1 || (oMu % 2 == 0 && oX % 2 == 0 && NB % 2 == 0), "16-byte aligned tiles");
 };
 
 template <int P>

@@ -76,9 +76,38 @@ __device__ __forceinline__ int face_node(int a, int ia, int t1, int t2)
   return a == 0 ? ia + P * (t1 + P * t2) : a == 1 ? t1 + P * (ia + P * t2) : t1 + P * (t2 + P * ia);
 }
 
+// P consecutive values from shared memory p[0..P-1] (p aligned to P values):
+// 16-byte vector loads where the line length allows (P = 4 in FP32, P even
+// in FP64), so a line costs one or two load instructions instead of P.
+template <int P, class T>
+__device__ __forceinline__ void load_line(const T* p, T* v)
+{
+  if constexpr (sizeof(T) == 4 && P % 4 == 0) {
+#pragma unroll
+    for (int k = 0; k < P; k += 4) {
+      const float4 q = *reinterpret_cast<const float4*>(p + k);
+      v[k] = q.x;
+      v[k + 1] = q.y;
+      v[k + 2] = q.z;
+      v[k + 3] = q.w;
+    }
+  } else if constexpr (sizeof(T) == 8 && P % 2 == 0) {
+#pragma unroll
+    for (int k = 0; k < P; k += 2) {
+      const double2 q = *reinterpret_cast<const double2*>(p + k);
+      v[k] = q.x;
+      v[k + 1] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < P; ++k) v[k] = p[k];
+  }
+}
+
 // one output point o of a 1D contraction along axis AX for all 5 variables:
 //   out[r][o] (+)= scale * sum_k M(a, k) in[r][o with coordinate AX replaced by k]
-// M(a,k) = Mat[a*P+k], or Mat[k*P+a] when TR.
+// M(a,k) = Mat[a*P+k], or Mat[k*P+a] when TR.  Along x (AX = 0) the P inputs
+// of a line are contiguous and aligned, as is an operator row when !TR.
 template <int P, int AX, bool TR, bool ACC, class T>
 __device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in, T* out, int o,
                                          T scale = T(1))
@@ -88,13 +117,24 @@ __device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in,
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
+  if constexpr (TR) {
 #pragma unroll
-  for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
+    for (int k = 0; k < P; ++k) m[k] = Mat[k * P + a];
+  } else {
+    load_line<P>(Mat + a * P, m);
+  }
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
+    T x[P];
+    if constexpr (AX == 0) {
+      load_line<P>(in + r * NB + base, x);
+    } else {
+#pragma unroll
+      for (int k = 0; k < P; ++k) x[k] = in[r * NB + base + k * S];
+    }
     T s = T(0);
 #pragma unroll
-    for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
+    for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     s *= scale;
     out[r * NB + o] = ACC ? out[r * NB + o] + s : s;
   }
@@ -109,13 +149,24 @@ __device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T*
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
+  if constexpr (TR) {
 #pragma unroll
-  for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
+    for (int k = 0; k < P; ++k) m[k] = Mat[k * P + a];
+  } else {
+    load_line<P>(Mat + a * P, m);
+  }
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
+    T x[P];
+    if constexpr (AX == 0) {
+      load_line<P>(in + r * NB + base, x);
+    } else {
+#pragma unroll
+      for (int k = 0; k < P; ++k) x[k] = in[r * NB + base + k * S];
+    }
     T s = T(0);
 #pragma unroll
-    for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
+    for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     res[r] = s;
   }
 }
@@ -345,6 +396,8 @@ struct StageSmem {
   static constexpr int X = X2 > TRACE ? X2 : TRACE;
   static constexpr int TOTAL = oX + align16(X);
   static_assert(oTrU >= MINV, "epilogue state must not overlap the inverse-mass buffers");
+  static_assert(oX % 16 == 0 && oMi % 16 == 0 && (5 * NB * ST) % 16 == 0 || P % 2 == 1,
+                "contraction tiles start on 16-byte boundaries");
 };
 
 // CV (curved elements): geometry per point from gv [E][kVolC][P^3] and
