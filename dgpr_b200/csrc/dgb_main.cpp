@@ -331,7 +331,7 @@ int main(int argc, char** argv)
     if (rc) die("dgb_step", rc);
     tstep += n;
   }
-  write(in.ofile + ".dg", tstep);
+  write(in.ofile + ".dg", tstep - 1);  // the index of the last step taken, as cudg.cu:140-141 writes
   dgb_destroy(h);
   return 0;
 }
