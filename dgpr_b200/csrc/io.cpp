@@ -114,9 +114,10 @@ extern "C" int dgb_read_state(const char* fname, unsigned long long* tstep, int*
     char name[1024];
     if (kl && fread(name, 1, kl, fp.f) != kl) return DGB_ERR_IO;
     name[kl] = '\0';
-    if (key && data && strcmp(name, key) == 0) {
+    const bool match = key && strcmp(name, key) == 0;
+    if (match) found = true;
+    if (match && data) {
       if (fread(data, sizeof(double), E * 5 * nb, fp.f) != E * 5 * nb) return DGB_ERR_IO;
-      found = true;
     } else {
       // skip, but verify the payload is present
       buf.resize(E * 5 * nb);

@@ -252,7 +252,8 @@ int dgb_write_state(const char* fname, unsigned long long tstep, const dgb_mesh_
 
 /* Reads a .dg header (io.cpp:92-124): sizes and bounds; nodes and the state
  * named `key` are copied when their pointers are non-NULL.  Returns
- * DGB_ERR_IO on a short or malformed file. */
+ * DGB_ERR_IO on a short or malformed file, or when `key` is given and the
+ * file holds no output of that name (whether or not data is NULL). */
 int dgb_read_state(const char* fname, unsigned long long* tstep, int* nx, int* ny, int* nz,
                    int* p, int* q, long long* bounds, double* nodes, const char* key,
                    double* data);

@@ -135,3 +135,15 @@ def test_noalloc_residual_rejects_curved_meshes_before_device_work():
     # device pointers are never touched: the mesh is refused first
     assert fn(ctypes.byref(desc), ctypes.byref(prm), ctypes.c_void_p(16), ctypes.c_void_p(16), None) == \
         dg.ERR_UNSUPPORTED
+
+
+def test_read_state_finds_a_key_without_copying(tmp_path):
+    import ctypes
+    mesh = dg.Mesh(1, 1, 1, 1, 1, C.box_nodes(1, 1, 1, 1, 1.0, 1.0, 1.0), [dg.PERIODIC] * 6)
+    f = str(tmp_path / "k.dg")
+    dg.write_state(f, 3, mesh, {"state": np.ones(40)})
+    t = ctypes.c_ulonglong()
+    rc = dg.lib().dgb_read_state(f.encode(), ctypes.byref(t), None, None, None, None, None, None, None, b"state", None)
+    assert rc == dg.OK and t.value == 3
+    rc = dg.lib().dgb_read_state(f.encode(), None, None, None, None, None, None, None, None, b"other", None)
+    assert rc == dg.ERR_IO
