@@ -77,21 +77,13 @@ __device__ __forceinline__ int face_node(int a, int ia, int t1, int t2)
 }
 
 // P consecutive values from shared memory p[0..P-1] (p aligned to P values):
-// 16-byte vector loads where the line length allows (P = 4 in FP32, P even
-// in FP64), so a line costs one or two load instructions instead of P.
+// 16-byte vector loads for FP64 lines of even length, so a line costs P/2
+// load instructions instead of P.  (FP32 lines stay scalar: float4 loads
+// measured 1.7% slower in the mixed stage kernel, which then spills.)
 template <int P, class T>
 __device__ __forceinline__ void load_line(const T* p, T* v)
 {
-  if constexpr (sizeof(T) == 4 && P % 4 == 0) {
-#pragma unroll
-    for (int k = 0; k < P; k += 4) {
-      const float4 q = *reinterpret_cast<const float4*>(p + k);
-      v[k] = q.x;
-      v[k + 1] = q.y;
-      v[k + 2] = q.z;
-      v[k + 3] = q.w;
-    }
-  } else if constexpr (sizeof(T) == 8 && P % 2 == 0) {
+  if constexpr (sizeof(T) == 8 && P % 2 == 0) {
 #pragma unroll
     for (int k = 0; k < P; k += 2) {
       const double2 q = *reinterpret_cast<const double2*>(p + k);
