@@ -109,24 +109,24 @@ __device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in,
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
-  if constexpr (TR) {
-#pragma unroll
-    for (int k = 0; k < P; ++k) m[k] = Mat[k * P + a];
-  } else {
+  if constexpr (!TR && sizeof(T) == 8 && P % 2 == 0) {
     load_line<P>(Mat + a * P, m);
+  } else {
+#pragma unroll
+    for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
   }
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
-    T x[P];
-    if constexpr (AX == 0) {
+    T s = T(0);
+    if constexpr (AX == 0 && sizeof(T) == 8 && P % 2 == 0) {
+      T x[P];
       load_line<P>(in + r * NB + base, x);
+#pragma unroll
+      for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     } else {
 #pragma unroll
-      for (int k = 0; k < P; ++k) x[k] = in[r * NB + base + k * S];
+      for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
     }
-    T s = T(0);
-#pragma unroll
-    for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     s *= scale;
     out[r * NB + o] = ACC ? out[r * NB + o] + s : s;
   }
@@ -141,24 +141,24 @@ __device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T*
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
-  if constexpr (TR) {
-#pragma unroll
-    for (int k = 0; k < P; ++k) m[k] = Mat[k * P + a];
-  } else {
+  if constexpr (!TR && sizeof(T) == 8 && P % 2 == 0) {
     load_line<P>(Mat + a * P, m);
+  } else {
+#pragma unroll
+    for (int k = 0; k < P; ++k) m[k] = TR ? Mat[k * P + a] : Mat[a * P + k];
   }
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
-    T x[P];
-    if constexpr (AX == 0) {
+    T s = T(0);
+    if constexpr (AX == 0 && sizeof(T) == 8 && P % 2 == 0) {
+      T x[P];
       load_line<P>(in + r * NB + base, x);
+#pragma unroll
+      for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     } else {
 #pragma unroll
-      for (int k = 0; k < P; ++k) x[k] = in[r * NB + base + k * S];
+      for (int k = 0; k < P; ++k) s = fma(m[k], in[r * NB + base + k * S], s);
     }
-    T s = T(0);
-#pragma unroll
-    for (int k = 0; k < P; ++k) s = fma(m[k], x[k], s);
     res[r] = s;
   }
 }
