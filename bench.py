@@ -164,6 +164,25 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, device="cuda"):
+    """The maximum of a per-rank number over all ranks of the default process
+    group (the rank itself when there is none): the multi-GPU time of a step
+    is the slowest replica's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, dof_stage, stages_per_step, steps, ms):
+    """Whole-job DOF-updates/s of `world` independent replicas, each doing
+    `steps` steps in `ms` (the max over ranks)."""
+    return world * dof_stage * stages_per_step * steps / (ms * 1e-3)
+
+
 def _timed_steps(dg, torch, s, stream, dt, steps):
     """Device time (ms) of `steps` graph-launched RK4 steps on the handle's stream."""
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -326,13 +345,6 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---- FP64 form: warm-up (>= W steps and >= 0.5 s, clocks sampled from
     # here), then K graph-launched steps with the state resident in HBM
     s = dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64)
@@ -347,7 +359,7 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     clocks = clk.stop()
     launches = s.last_launch_count
-    value = world * dof_stage * 4 * args.steps / (ms * 1e-3)
+    value = replica_rate(world, dof_stage, 4, args.steps, ms)
 
     # ---- end to end through the C ABI with host buffers: every step copies the
     # state in from pinned host memory and the state and norm back out
@@ -364,7 +376,7 @@ def run_ours(args, rank, world, local_rank):
         dg._check(dg.lib().dgb_get_state(s.h, dg._p(Uhost)))
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = world * dof_stage * 4 * args.steps / e2e_s
+    e2e = replica_rate(world, dof_stage, 4, args.steps, e2e_s * 1e3)
 
     reps = max(3, min(args.steps, 10))
     stage_ms, trace_ms = _stage_kernel_ms(dg, s, U0, dt, reps)
@@ -378,7 +390,7 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     torch.cuda.synchronize()
     ms_mixed = max_over_ranks(_timed_steps(dg, torch, sm, stream, dt, args.steps))
-    value_mixed = world * dof_stage * 4 * args.steps / (ms_mixed * 1e-3)
+    value_mixed = replica_rate(world, dof_stage, 4, args.steps, ms_mixed)
     stage_ms_mixed, trace_ms_mixed = _stage_kernel_ms(dg, sm, U0, dt, reps)
     sm.close()
 
