@@ -240,7 +240,8 @@ def _adjoint_config(dg, torch, nsteps, budgets):
     """Gradient of the final enstrophy w.r.t. the 8 x 3 amplitudes of seeded
     Fourier velocity modes on a uniform flow: periodic [0, 2 pi]^3, 16^3 hexes,
     p = 3, Re 500, Ma 0.3, RK4, FP64.  Times the recorded forward run and the
-    backward sweep for each checkpoint budget, and checks the gradient along
+    backward sweep for each checkpoint budget (a number of state buffers, or
+    -1: every state and stage state kept), and checks the gradient along
     one random direction against central differences of two plain runs."""
     from dgpr_b200 import autograd as dga
     from dgpr_b200 import functionals as F
@@ -267,7 +268,10 @@ def _adjoint_config(dg, torch, nsteps, budgets):
         for slots in budgets:
             # untimed recorded run first: allocates (or frees) the checkpoint buffers
             s.set_state(U0.cpu().numpy())
-            s.forward_record(dg.RK4, dt, nsteps, slots, norms=False)
+            if slots == dga.STAGES:
+                s.forward_record_stages(dg.RK4, dt, nsteps, norms=False)
+            else:
+                s.forward_record(dg.RK4, dt, nsteps, slots, norms=False)
             a = a0.clone().requires_grad_(True)
             Ua = modes.state(a)
             torch.cuda.synchronize()
@@ -283,7 +287,8 @@ def _adjoint_config(dg, torch, nsteps, budgets):
             g = a.grad.cpu().numpy()
             if grad is None:
                 grad = g
-            out["budgets"].append({"slots": slots, "recorded_forward_s": t1 - t0, "backward_s": t2 - t1,
+            out["budgets"].append({"slots": "every state and stage state" if slots == dga.STAGES else slots,
+                                   "recorded_forward_s": t1 - t0, "backward_s": t2 - t1,
                                    "recomputed_steps": fwd, "reversed_steps": rev,
                                    "gradient_equal_to_first_budget": bool(np.array_equal(g, grad))})
         # plain forward time of the same run (no recording)
@@ -415,7 +420,7 @@ def run_ours(args, rank, world, local_rank):
             rev_ms, rev_launches = _reverse_step_ms(dg, torch, sa, stream, U0, dt, reps)
         adj = {"reverse_step_ms": rev_ms, "forward_step_ms": ms / args.steps,
                "reverse_over_forward": rev_ms / (ms / args.steps), "reverse_step_launches": rev_launches,
-               "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20))}
+               "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}

@@ -99,6 +99,8 @@ def lib():
             "dgb_step_vjp_device": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, vp, vp]),
             "dgb_forward_record": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong,
                                                   ctypes.c_int, _dp]),
+            "dgb_forward_record_stages": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong,
+                                                         _dp]),
             "dgb_backward": (ctypes.c_int, [vp, _dp, _dp]),
             "dgb_backward_device": (ctypes.c_int, [vp, vp, vp]),
             "dgb_adjoint_stats": (ctypes.c_int, [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3),
@@ -366,6 +368,15 @@ class Solver:
         out = np.zeros(max(int(nsteps), 1))
         _check(lib().dgb_forward_record(self.h, int(scheme), float(dt), int(nsteps), int(slots),
                                         _p(out) if norms else None))
+        return out[:nsteps]
+
+    def forward_record_stages(self, scheme, dt, nsteps, norms=True):
+        """Recorded run keeping every state and stage state: the backward
+        sweep then recomputes nothing."""
+        self.record_id = getattr(self, "record_id", 0) + 1
+        out = np.zeros(max(int(nsteps), 1))
+        _check(lib().dgb_forward_record_stages(self.h, int(scheme), float(dt), int(nsteps),
+                                               _p(out) if norms else None))
         return out[:nsteps]
 
     def backward(self, lamN):

@@ -14,7 +14,11 @@ import torch
 
 from . import DgbError, ERR_ARG
 
-__all__ = ["integrate", "residual"]
+__all__ = ["integrate", "residual", "STAGES"]
+
+# `slots` value for integrate(): keep every state and every RK stage state,
+# so the backward sweep recomputes nothing (dgb_forward_record_stages)
+STAGES = -1
 
 
 def _dev_f64(t, n, what):
@@ -31,7 +35,10 @@ class _Integrate(torch.autograd.Function):
         U0 = _dev_f64(U0, solver.n, "U0")
         torch.cuda.current_stream().synchronize()
         solver.set_state_device(U0.data_ptr())
-        solver.forward_record(scheme, dt, nsteps, slots, norms=False)
+        if slots == STAGES:
+            solver.forward_record_stages(scheme, dt, nsteps, norms=False)
+        else:
+            solver.forward_record(scheme, dt, nsteps, slots, norms=False)
         UN = torch.empty_like(U0)
         solver.get_state_device(UN.data_ptr())
         ctx.solver = solver
@@ -76,7 +83,8 @@ class _Residual(torch.autograd.Function):
 
 def integrate(U0, solver, scheme, dt, nsteps, slots=None):
     """U_N after nsteps RK steps from U0, differentiable in U0.  slots: number
-    of state checkpoints held on the device (default: every state)."""
+    of state checkpoints held on the device (default: every state), or STAGES
+    to keep every stage state as well."""
     return _Integrate.apply(U0, solver, int(scheme), float(dt), int(nsteps),
                             int(slots if slots is not None else nsteps))
 

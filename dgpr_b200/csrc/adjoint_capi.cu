@@ -84,10 +84,15 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
 // recomputed stage state (the stage epilogues write them) and hands them to
 // the VJPs; a mixed-precision handle recomputes the stages in FP32 with
 // rotating trace buffers and each VJP takes its own FP64 traces.
-int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl)
+// With `stored` (the recorded stage states of this step) nothing is
+// recomputed: an FP64 handle takes the traces of the stored states.
+int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl,
+                         double* const* stored = nullptr)
 {
   const KLaunch L = klaunch(h);
   double* S[3] = {h->d_adj[dgb_handle::ADJ_S0], h->d_adj[dgb_handle::ADJ_S1], h->d_adj[dgb_handle::ADJ_S2]};
+  if (stored)
+    for (int s = 0; s < 3; ++s) S[s] = stored[s];
   double* A0 = h->d_adj[dgb_handle::ADJ_A0];
   double* A1 = h->d_adj[dgb_handle::ADJ_A1];
   double* ACC = h->d_adj[dgb_handle::ADJ_ACC];
@@ -95,7 +100,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   const bool f64 = h->precision == DGB_FP64;
   void* const* T = h->d_trace;
   void* TU = f64 ? (void*)h->d_adj_tr : T[0];
-  CK(launch_trace(L, Ui, TU, h->stream));
+  if (f64 || !stored) CK(launch_trace(L, Ui, TU, h->stream));
   const int nst = scheme == DGB_RK4 ? 3 : 2;  // recomputed stage states
   const int rk4[3] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2}, tvd[2] = {MODE_TVD_0, MODE_TVD_1};
   // trace buffers read / written by the recomputed stages
@@ -105,6 +110,10 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   void* tout_mix[3] = {T[1], T[0], nullptr};
   if (scheme != DGB_RK4) tout_mix[1] = nullptr;
   for (int s = 0; s < nst; ++s) {
+    if (stored) {  // the stage state is at hand; an FP64 handle still needs its traces
+      if (f64) CK(launch_trace(L, S[s], tout_f64[s], h->stream));
+      continue;
+    }
     StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[s] : tvd[s], dt);
     a.Ubase = Ui;
     a.acc = h->d_acc;
@@ -157,7 +166,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   v.acc_in = ACC;
   v.acc_out = lam;
   CK(launch_residual_vjp(L, v, sc, h->stream));
-  if (nl) *nl += 1 + nst + (nst + 1) * (f64 ? 2 : 3);
+  if (nl) *nl += (stored && !f64 ? 0 : 1 + nst) + (nst + 1) * (f64 ? 2 : 3);
   return DGB_OK;
 }
 
@@ -226,6 +235,9 @@ void dgb::free_adjoint(dgb_handle* h)
   for (double* p : h->d_slots)
     if (p) cudaFree(p);
   h->d_slots.clear();
+  if (h->d_stage_store) cudaFree(h->d_stage_store);
+  h->d_stage_store = nullptr;
+  h->stage_store_cap = 0;
   h->recorded = false;
 }
 
@@ -342,10 +354,95 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   h->plan_pos = h->plan.first_reverse;
   h->recorded = true;
+  h->rec_stages = false;
   h->slots_dirty = false;
   h->rec_scheme = scheme;
   h->rec_dt = dt;
   h->rec_steps = nsteps;
+  h->last_launches = launches;
+  return DGB_OK;
+}
+
+int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, double* norms_host)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  int rc = check_scheme(scheme, dt);
+  if (rc) return rc;
+  if (nsteps < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1");
+  if ((rc = check_bounds(h))) return rc;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_adjoint(h))) return rc;
+  h->recorded = false;
+  const int nst = scheme == DGB_RK4 ? 4 : 3;
+  // every state U_0 .. U_{N-1} in the slots, every intermediate stage state
+  // in one store
+  while (h->d_slots.size() > nsteps) {
+    cudaFree(h->d_slots.back());
+    h->d_slots.pop_back();
+  }
+  while (h->d_slots.size() < nsteps) {
+    double* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(double) * (size_t)h->n));
+    h->d_slots.push_back(p);
+  }
+  const size_t need = (size_t)nsteps * (nst - 1) * (size_t)h->n;
+  if (need > h->stage_store_cap) {
+    if (h->d_stage_store) CK(cudaFree(h->d_stage_store));
+    h->d_stage_store = nullptr;
+    h->stage_store_cap = 0;
+    CK(cudaMalloc(&h->d_stage_store, sizeof(double) * need));
+    h->stage_store_cap = need;
+  }
+  if (nsteps > h->norms_cap) {  // room for every step's norm (ensure_step_graph grows it)
+    if ((rc = ensure_step_graph(h, scheme, dt, nsteps))) return rc;
+  }
+  CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  // the step of enqueue_step (capi.cu) launch by launch, with every stage
+  // state written to its own buffer: the same kernels on the same inputs,
+  // so the states are those dgb_step computes, bit for bit
+  const KLaunch L = klaunch(h);
+  const int rk4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
+  const int tvd[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
+  const int tin4[4] = {0, 1, 0, 1}, tout4[4] = {1, 0, 1, 0};
+  const int tin3[3] = {0, 1, 2}, tout3[3] = {1, 2, 0};
+  CK(launch_trace(L, h->d_U, h->d_trace[0], h->stream));
+  long long launches = 1;
+  for (unsigned long long i = 0; i < nsteps; ++i) {
+    if ((rc = copy_state(h, h->d_slots[i], h->d_U))) return rc;
+    double* Si = h->d_stage_store + (size_t)i * (nst - 1) * (size_t)h->n;
+    for (int st = 0; st < nst; ++st) {
+      StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[st] : tvd[st], dt);
+      a.Ubase = h->d_U;
+      a.acc = h->d_acc;
+      a.Uout = st == nst - 1 ? h->d_U : Si + (size_t)st * h->n;
+      a.part = st == 0 ? h->d_part : nullptr;
+      a.flag = h->d_flag;
+      a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[st] : tout3[st]];
+      const double* in = st == 0 ? h->d_U : Si + (size_t)(st - 1) * h->n;
+      CK(launch_stage(L, in, h->d_trace[scheme == DGB_RK4 ? tin4[st] : tin3[st]], a, h->stream));
+      ++launches;
+      if (st == 0) {
+        CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
+                       h->d_flag, h->stream));
+        ++launches;
+      }
+    }
+  }
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], h->d_U))) return rc;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (norms_host)
+    CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
+  h->recorded = true;
+  h->rec_stages = true;
+  h->rec_scheme = scheme;
+  h->rec_dt = dt;
+  h->rec_steps = nsteps;
+  h->slots_dirty = false;
   h->last_launches = launches;
   return DGB_OK;
 }
@@ -355,6 +452,24 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
   if (!h || !lamN_dev || !lam0_dev) return fail(DGB_ERR_ARG, "null argument");
   if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
   CK(cudaSetDevice(h->device));
+  if (h->rec_stages) {  // every state and stage state was kept: reverse only
+    const int nst = h->rec_scheme == DGB_RK4 ? 4 : 3;
+    double* lam = h->d_adj[dgb_handle::ADJ_LAM];
+    int rc;
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    if ((rc = copy_state(h, lam, lamN_dev))) return rc;
+    long long nl = 0;
+    for (unsigned long long k = h->rec_steps; k-- > 0;) {
+      double* Si = h->d_stage_store + (size_t)k * (nst - 1) * (size_t)h->n;
+      double* stored[3] = {Si, Si + (size_t)h->n, nst > 3 ? Si + 2 * (size_t)h->n : nullptr};
+      if ((rc = enqueue_reverse_step(h, h->rec_scheme, h->rec_dt, h->d_slots[k], lam, &nl, stored))) return rc;
+    }
+    if ((rc = copy_state(h, lam0_dev, lam))) return rc;
+    h->last_launches = nl;
+    h->adj_forward_steps = 0;
+    h->adj_reverse_steps = (long long)h->rec_steps;
+    return read_flag(h);
+  }
   const int scheme = h->rec_scheme;
   const double dt = h->rec_dt;
   double* lam = h->d_adj[dgb_handle::ADJ_LAM];

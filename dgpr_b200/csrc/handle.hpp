@@ -61,6 +61,9 @@ struct dgb_handle {
   double* d_adj_tr = nullptr;  // FP64 face traces [E][6][10][NQF]
   double* d_adj_ta = nullptr;  // face-trace adjoints [E][6][20][NQF]
   std::vector<double*> d_slots;  // checkpoints
+  double* d_stage_store = nullptr;  // recorded stage states [nsteps][stages - 1][n] (dgb_forward_record_stages)
+  size_t stage_store_cap = 0;       // doubles
+  bool rec_stages = false;          // the recorded run kept its stage states
   dgb::CheckpointPlan plan;    // the recorded forward's plan
   size_t plan_pos = 0;         // first op of the backward part
   bool recorded = false;

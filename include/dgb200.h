@@ -201,6 +201,13 @@ int dgb_step_vjp_device(dgb_handle* h, int scheme, double dt, const double* U_de
 int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, int slots,
                        double* norms_host);
 
+/* Recorded forward run that keeps every state and every intermediate RK
+ * stage state (nsteps * 4 states for RK4, * 3 for TVD-RK3, on the device), so
+ * that dgb_backward recomputes nothing: each reverse step is the residual
+ * VJPs of its stages only.  Same states and norms as dgb_step. */
+int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned long long nsteps,
+                              double* norms_host);
+
 /* Backward sweep through the last recorded run: given dJ/dU_N (the adjoint
  * of the final state) returns dJ/dU_0.  The resident state is left at U_N.
  * May be called repeatedly for different dJ/dU_N; when a sweep has

@@ -179,6 +179,12 @@ def test_n_step_adjoint_fd_and_checkpoint_invariance(scheme):
             rec = sum(a for kind, a in ops[:first] if kind == "forward")
             assert rev == N and planned == pfwd and fwd == pfwd - rec
             assert np.array_equal(s.get_state(), UN), "backward leaves the final state resident"
+        s.set_state(U0)
+        s.forward_record_stages(scheme, dt, N)
+        assert np.array_equal(s.get_state(), UN), "the stage-keeping record computes the same states"
+        grads["stages"] = s.backward(w)
+        fwd, rev, _ = s.adjoint_stats()
+        assert fwd == 0 and rev == N
         ref = _step(s, U0, scheme, dt, N)
         assert np.array_equal(UN, ref), "recorded run equals dgb_step"
         for slots, g in grads.items():
