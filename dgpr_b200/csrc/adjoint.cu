@@ -213,11 +213,15 @@ struct AdjASmem {
   static_assert(P % 2 == 1 || (oMu % 2 == 0 && oX % 2 == 0 && NB % 2 == 0), "16-byte aligned tiles");
 };
 
-template <int P>
+// CV (curved elements): per-point geometry from gv / gf as in the stage
+// kernel; the inverse mass matrix B3^-1 diag(1/(w detJ)) B3^-T is symmetric,
+// so mu takes the same operator.
+template <int P, bool CV>
 __global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJA_MINB>::value))
 adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr, VjpArgs v,
-            const double* __restrict__ opsg, const double* __restrict__ geo, const int* __restrict__ nbr,
-            DevParams prm, double* __restrict__ Ubar_part, double* __restrict__ TA, int* flag)
+            const double* __restrict__ opsg, const double* __restrict__ geo, const double* __restrict__ gv,
+            const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm,
+            double* __restrict__ Ubar_part, double* __restrict__ TA, int* flag)
 {
   using C = Cfg<P>;
   using L = AdjASmem<P>;
@@ -247,17 +251,40 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   __syncthreads();
   const double* B = so + C::oB;
   const double* Dq = so + C::oDq;
-  const double* Mi = so + C::oMi;
+  const double* Mi = so + (CV ? C::oBi : C::oMi);
   const double detJ = sg[kGeoDetJ];
   const double* Ji = sg + kGeoJinv;
   const double gamma = prm.gamma, mu = prm.mu;
+  const double* gve = CV ? gv + e * kVolC * NB : nullptr;
+  const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
 
   // mu = -Minv^T lam  (f = -Minv R)
-  if (node) contract<P, 0, true, false>(Mi, V0, V1, tid);
-  __syncthreads();
-  if (node) contract<P, 1, true, false>(Mi, V1, V0, tid);
-  __syncthreads();
-  if (node) contract<P, 2, true, false>(Mi, V0, Mu, tid, -1.0 / detJ);
+  if constexpr (CV) {  // B3^-T, 1/(w detJ), B3^-1
+    if (node) contract<P, 0, true, false>(Mi, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, true, false>(Mi, V1, V0, tid);
+    __syncthreads();
+    if (node) {
+      contract<P, 2, true, false>(Mi, V0, V1, tid);
+      const double* w = so + C::oW;
+      const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+      const double iw = -1.0 / (w[qx] * w[qy] * w[qz] * gve[kVolDetJ * NB + tid]);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) V1[r * NB + tid] *= iw;
+    }
+    __syncthreads();
+    if (node) contract<P, 0, false, false>(Mi, V1, V0, tid);
+    __syncthreads();
+    if (node) contract<P, 1, false, false>(Mi, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 2, false, false>(Mi, V1, Mu, tid);
+  } else {
+    if (node) contract<P, 0, true, false>(Mi, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, true, false>(Mi, V1, V0, tid);
+    __syncthreads();
+    if (node) contract<P, 2, true, false>(Mi, V0, Mu, tid, -1.0 / detJ);
+  }
   __syncthreads();
   for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = U[e * 5 * NB + i];
   __syncthreads();
@@ -290,7 +317,13 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   if (node) {  // pointwise reverse at quadrature point tid
     const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
     const double* w = so + C::oW;
-    const double wJ = w[qx] * w[qy] * w[qz] * detJ;
+    double Jbuf[9];
+    if constexpr (CV) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Jbuf[c] = gve[c * NB + tid];
+    }
+    const double* Ji = CV ? Jbuf : sg + kGeoJinv;  // inverse Jacobian at this point
+    const double wJ = w[qx] * w[qy] * w[qz] * (CV ? gve[kVolDetJ * NB + tid] : detJ);
     double S[5], Gp[3][5], Hb[3][5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
@@ -354,14 +387,24 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
     if (tid < NH) {
       const int nb = nbr[e * 6 + lf];
-      const double fJ = sg[kGeoFJ + lf];
+      const double* gp = CV ? gfe + lf * kFaceC * NQF + fq : nullptr;  // this face point's geometry
+      const double fJ = CV ? gp[kFaceFJ * NQF] : sg[kGeoFJ + lf];
       const double fw = fJ * w1[q1] * w1[q2];
       const double ef = prm.eta * (nb >= 0 ? 0.5 : 1.0);
+      const double lift = CV ? gp[kFaceLift * NQF] : so[C::oC + end] / detJ;  // own lifting scale
       double zb[5];
       zb[0] = 0.;  // the lifting has no mass component
 #pragma unroll
       for (int r = 1; r < 5; ++r) zb[r] = ef * fJ * Sm[r];
-      const double* n = sg + kGeoN + 3 * lf;
+      double nbuf[3], Jbuf[9];
+      if constexpr (CV) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nbuf[c] = gp[(kFaceN + c) * NQF];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) Jbuf[c] = gp[c * NQF];
+      }
+      const double* n = CV ? nbuf : sg + kGeoN + 3 * lf;
+      const double* Ji = CV ? Jbuf : sg + kGeoJinv;
       double ab[5];
 #pragma unroll
       for (int r = 0; r < 5; ++r) ab[r] = Sm[r];
@@ -414,8 +457,9 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             d[r] = Uo[r] - Un[r];
             dbar[r] = 0.;
           }
-          const double co = 0.5 * fw * so[C::oC + end] / detJ;
-          const double cn = 0.5 * fw * so[C::oC + (end ^ 1)] / geo[(long)nb * kGeoStride + kGeoDetJ];
+          const double co = 0.5 * fw * lift;
+          const double cn = 0.5 * fw * (CV ? gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]
+                                           : so[C::oC + (end ^ 1)] / geo[(long)nb * kGeoStride + kGeoDetJ]);
           double rob[5], rnb[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
@@ -453,7 +497,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ubd[r];
           visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar);
-          const double co = fw * so[C::oC + end] / detJ;
+          const double co = fw * lift;
           double rbb[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) rbb[r] = co * zb[r];
@@ -494,11 +538,11 @@ struct AdjBSmem {
   static constexpr int TOTAL = oX + 75 * NQF + 60 * NQF;
 };
 
-template <int P>
+template <int P, bool CV>
 __global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJB_MINB>::value))
 adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA, const double* __restrict__ opsg,
-            const double* __restrict__ geo, const int* __restrict__ nbr, DevParams prm,
-            const double* __restrict__ Ubar_part, VjpArgs v)
+            const double* __restrict__ geo, const double* __restrict__ gf, const int* __restrict__ nbr,
+            DevParams prm, const double* __restrict__ Ubar_part, VjpArgs v)
 {
   using C = Cfg<P>;
   using L = AdjBSmem<P>;
@@ -525,7 +569,6 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
     for (int r = 0; r < 5; ++r) Racc[r] = Ubar_part[e * 5 * NB + r * NB + tid];
   }
   __syncthreads();
-  const double* Ji = sg + kGeoJinv;
   const double mu = prm.mu;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
@@ -555,7 +598,16 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
 #pragma unroll
         for (int r = 0; r < 5; ++r) gb[c][r] = 0.;
       if (mu != 0.) {  // trace Qn = A(S, Gp) . n
-        const double* n = sg + kGeoN + 3 * lf;
+        double nbuf[3], Jbuf[9];
+        if constexpr (CV) {
+          const double* gp = gf + ((e * 6 + lf) * kFaceC) * NQF + fq;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) nbuf[c] = gp[(kFaceN + c) * NQF];
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Jbuf[c] = gp[c * NQF];
+        }
+        const double* n = CV ? nbuf : sg + kGeoN + 3 * lf;
+        const double* Ji = CV ? Jbuf : sg + kGeoJinv;
         double Gp[3][5], Qb[3][5], Gpb[3][5];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -593,15 +645,35 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
 
 // ------------------------------------------------------------ host launchers
 
+template <int P, bool CV>
+static cudaError_t prepare_pc()
+{
+  static_assert(AdjASmem<P>::TOTAL * 8 <= 227 * 1024, "adjoint shared memory");
+  cudaError_t e = cudaFuncSetAttribute(adjA_kernel<P, CV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(AdjASmem<P>::TOTAL * sizeof(double)));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(adjB_kernel<P, CV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(AdjBSmem<P>::TOTAL * sizeof(double)));
+}
+
 template <int P>
 static cudaError_t prepare_p()
 {
-  static_assert(AdjASmem<P>::TOTAL * 8 <= 227 * 1024, "adjoint shared memory");
-  cudaError_t e = cudaFuncSetAttribute(adjA_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(AdjASmem<P>::TOTAL * sizeof(double)));
+  cudaError_t e = prepare_pc<P, false>();
+  return e == cudaSuccess ? prepare_pc<P, true>() : e;
+}
+
+template <int P, bool CV>
+static cudaError_t vjp_pc(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, const double* Tr,
+                          cudaStream_t st)
+{
+  adjA_kernel<P, CV><<<(unsigned)L.E, Cfg<P>::NT, AdjASmem<P>::TOTAL * sizeof(double), st>>>(
+      L.E, v.U, Tr, v, L.opsd, L.geo, L.gv, L.gf, L.nbr, L.prm, s.part, s.ta, s.flag);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(adjB_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(AdjBSmem<P>::TOTAL * sizeof(double)));
+  adjB_kernel<P, CV><<<(unsigned)L.E, Cfg<P>::NT, AdjBSmem<P>::TOTAL * sizeof(double), st>>>(
+      L.E, v.U, s.ta, L.opsd, L.geo, L.gf, L.nbr, L.prm, s.part, v);
+  return cudaGetLastError();
 }
 
 template <int P>
@@ -616,13 +688,7 @@ static cudaError_t vjp_p(const KLaunch& L, const VjpArgs& v, const VjpScratch& s
     if ((e = launch_trace(L64, v.U, s.trace, st)) != cudaSuccess) return e;
     Tr = s.trace;
   }
-  adjA_kernel<P><<<(unsigned)L.E, Cfg<P>::NT, AdjASmem<P>::TOTAL * sizeof(double), st>>>(
-      L.E, v.U, Tr, v, L.opsd, L.geo, L.nbr, L.prm, s.part, s.ta, s.flag);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  adjB_kernel<P><<<(unsigned)L.E, Cfg<P>::NT, AdjBSmem<P>::TOTAL * sizeof(double), st>>>(
-      L.E, v.U, s.ta, L.opsd, L.geo, L.nbr, L.prm, s.part, v);
-  return cudaGetLastError();
+  return L.gv ? vjp_pc<P, true>(L, v, s, Tr, st) : vjp_pc<P, false>(L, v, s, Tr, st);
 }
 
 cudaError_t prepare_adjoint(int P)

@@ -27,7 +27,6 @@ int fail(int code, const char* msg) { return set_last_error(code, msg); }
 // have none
 int check_bounds(const dgb_handle* h)
 {
-  if (h->curved) return fail(DGB_ERR_UNSUPPORTED, "the adjoint covers affine elements only");
   for (int s = 0; s < 6; ++s)
     if (h->bounds[s] == DGB_BT_SUBSONIC_INFLOW || h->bounds[s] == DGB_BT_SUBSONIC_OUTFLOW)
       return fail(DGB_ERR_UNSUPPORTED, "the adjoint covers periodic, freestream and wall boundaries only");
