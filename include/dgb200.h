@@ -90,7 +90,9 @@ const char* dgb_last_error_message(void);
  * cuda_residual_workspace (solve_cuda.cu:303), plus the host precompute they
  * consume (core_geometry::precompute, geometry_common.cpp:292;
  * shared_geometry::precompute_face_geometry, geometry_shared.cpp:156).
- * Uses the current CUDA device. */
+ * Meshes of affine elements keep one Jacobian per element; a mesh with any
+ * curved (non-affine, q >= 2) element gets per-point geometry.  Uses the
+ * current CUDA device. */
 int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precision,
                dgb_handle** out);
 
@@ -152,6 +154,7 @@ long long dgb_last_launch_count(const dgb_handle* h);
 int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk);
 
 /* One FP64 residual f = -Minv R of a device-resident state U_dev into f_dev
+ * on a mesh of affine elements (curved meshes: DGB_ERR_UNSUPPORTED)
  * (both caller-owned device arrays, layout U[e][r][b]), for callers that may
  * not allocate GPU memory -- e.g. a host application that owns the device
  * memory pool, or a solver that has claimed all of HBM for its own state.
