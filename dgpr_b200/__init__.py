@@ -92,6 +92,9 @@ def lib():
             "dgb_profile_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
                                                 ctypes.POINTER(ctypes.c_int)]),
             "dgb_synchronize": (ctypes.c_int, [vp]),
+            "dgb_mean_update": (ctypes.c_int, [vp, ctypes.c_ulonglong, ctypes.c_ulonglong]),
+            "dgb_set_mean": (ctypes.c_int, [vp, _dp]),
+            "dgb_get_mean": (ctypes.c_int, [vp, _dp]),
             "dgb_set_state_device": (ctypes.c_int, [vp, vp]),
             "dgb_get_state_device": (ctypes.c_int, [vp, vp]),
             "dgb_residual_vjp": (ctypes.c_int, [vp, _dp, _dp, _dp]),
@@ -333,6 +336,15 @@ class Solver:
     @property
     def last_launch_count(self):
         return lib().dgb_last_launch_count(self.h)
+
+    def mean_update(self, tstep, mean_start):
+        """Running mean after step tstep (the reference's update_mean)."""
+        _check(lib().dgb_mean_update(self.h, int(tstep), int(mean_start)))
+
+    def get_mean(self):
+        M = np.zeros(self.n)
+        _check(lib().dgb_get_mean(self.h, _p(M)))
+        return M
 
     def synchronize(self):
         _check(lib().dgb_synchronize(self.h))

@@ -102,7 +102,7 @@ long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == D
 void free_all(dgb_handle* h)
 {
   if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
+  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_mean, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
                   h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
                   h->d_counter, h->d_flag};
   for (void* p : ptrs)
@@ -352,6 +352,40 @@ int dgb_get_state_device(dgb_handle* h, double* U_dev)
   if (!h || !U_dev) return fail(DGB_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(U_dev, h->d_U, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_mean_update(dgb_handle* h, unsigned long long tstep, unsigned long long mean_start)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (tstep < mean_start) return fail(DGB_ERR_ARG, "tstep before mean_start");
+  CK(cudaSetDevice(h->device));
+  if (!h->d_mean) {  // a mean that was never set starts from zero
+    CK(cudaMalloc(&h->d_mean, sizeof(double) * (size_t)h->n));
+    CK(cudaMemsetAsync(h->d_mean, 0, sizeof(double) * (size_t)h->n, h->stream));
+  }
+  const double old_w = (double)(tstep - mean_start), new_w = (double)(tstep + 1 - mean_start);
+  CK(launch_mean_update((long)h->n, h->d_mean, h->d_U, old_w, new_w, tstep == mean_start ? 1 : 0, h->stream));
+  return DGB_OK;
+}
+
+int dgb_set_mean(dgb_handle* h, const double* mean_host)
+{
+  if (!h || !mean_host) return fail(DGB_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  if (!h->d_mean) CK(cudaMalloc(&h->d_mean, sizeof(double) * (size_t)h->n));
+  CK(cudaMemcpyAsync(h->d_mean, mean_host, sizeof(double) * (size_t)h->n, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_get_mean(dgb_handle* h, double* mean_host)
+{
+  if (!h || !mean_host) return fail(DGB_ERR_ARG, "null argument");
+  if (!h->d_mean) return fail(DGB_ERR_ARG, "no running mean (dgb_mean_update / dgb_set_mean)");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(mean_host, h->d_mean, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return DGB_OK;
 }

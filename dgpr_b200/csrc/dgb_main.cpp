@@ -9,8 +9,9 @@
 // library's CUDA kernels.
 //
 // Differences: the arithmetic is FP64 (or -precision mixed), not the
-// reference GPU build's FP32; -npx/-npy/-npz must be 1 (one GPU); the
-// running mean (-mean_start) is not produced.
+// reference GPU build's FP32; -npx/-npy/-npz must be 1 (one GPU).  The
+// running mean (-mean_start) follows the reference's CPU driver dg.cpp, which
+// has it (cudg.cu does not).
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
@@ -84,7 +85,7 @@ int parse(int argc, char** argv, Inputs& in)
       {"scheme", "time stepping scheme (RK4, tvdRK3)", K_SCHEME, &in.scheme},
       {"eta", "BR2 stabilization parameter", K_DBL, &in.eta},
       {"turb", "initialize turbulent instead of uniform", K_BOOL, &in.turb},
-      {"mean_start", "iteration at which to start averaging (not produced)", K_U64, &in.mean_start},
+      {"mean_start", "iteration at which to start averaging", K_U64, &in.mean_start},
       {"gamma", "ratio of specific heats", K_DBL, &in.gamma},
       {"mu", "dynamic viscosity", K_DBL, &in.mu},
       {"c", "speed of sound", K_DBL, &in.c},
@@ -294,18 +295,32 @@ int main(int argc, char** argv)
   if ((rc = dgb_create(&mesh, &prm, in.precision, &h))) die("dgb_create", rc);
   if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
 
-  const char* keys[1] = {"state"};
-  const double* data[1] = {U.data()};
+  // running mean (dg.cpp:123-131): an input file may carry one to continue
+  std::vector<double> M(U.size());
+  bool have_mean = false;
+  if (!in.ifile.empty()) {
+    const std::string f = in.ifile + ".dg";
+    if (dgb_read_state(f.c_str(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, "mean",
+                       M.data()) == DGB_OK) {
+      if ((rc = dgb_set_mean(h, M.data()))) die("dgb_set_mean", rc);
+      have_mean = true;
+    }
+  }
+
+  const char* keys[2] = {"state", "mean"};
+  const double* data[2] = {U.data(), M.data()};
   auto write = [&](const std::string& f, unsigned long long ts) {
     int r = dgb_get_state(h, U.data());
     if (r) die("dgb_get_state", r);
-    r = dgb_write_state(f.c_str(), ts, &mesh, 1, keys, data);
+    if (have_mean && (r = dgb_get_mean(h, M.data()))) die("dgb_get_mean", r);
+    r = dgb_write_state(f.c_str(), ts, &mesh, have_mean ? 2 : 1, keys, data);
     if (r) die(f.c_str(), r);
   };
 
   // time stepping: the reference checkpoints before the step whose index
   // satisfies (tstep + 1) % chkint == 0 (cudg.cu:112-130); between checkpoints
-  // the steps run as one dgb_step call (one CUDA graph replay per step)
+  // the steps run as one dgb_step call (one CUDA graph replay per step), or
+  // one at a time once the running mean is being accumulated
   const unsigned long long tfinal = tstep + in.niter;
   std::vector<double> norms;
   while (tstep < tfinal) {
@@ -320,6 +335,10 @@ int main(int argc, char** argv)
       if (next > tstep && next - tstep < n) n = next - tstep;
       if (n == 0) n = 1;
     }
+    if (tstep >= in.mean_start)
+      n = 1;
+    else if (in.mean_start - tstep < n)
+      n = in.mean_start - tstep;
     norms.resize(n);
     rc = dgb_step(h, in.scheme, in.dt, n, norms.data());
     if (rc == DGB_OK || rc == DGB_ERR_NONFINITE) {  // the reference prints up to the NaN, then aborts
@@ -330,6 +349,10 @@ int main(int argc, char** argv)
     }
     if (rc) die("dgb_step", rc);
     tstep += n;
+    if (tstep - 1 >= in.mean_start) {  // after step tstep - 1 (n == 1 here)
+      if ((rc = dgb_mean_update(h, tstep - 1, in.mean_start))) die("dgb_mean_update", rc);
+      have_mean = true;
+    }
   }
   write(in.ofile + ".dg", tstep - 1);  // the index of the last step taken, as cudg.cu:140-141 writes
   dgb_destroy(h);

@@ -40,6 +40,7 @@ struct dgb_handle {
   double* d_f = nullptr;
   double* d_R = nullptr;
   double* d_part = nullptr;
+  double* d_mean = nullptr;   // running mean of the state (dgb_mean_update)
   double* d_norms = nullptr;
   int* d_counter = nullptr;
   int* d_flag = nullptr;

@@ -61,6 +61,10 @@ cudaError_t launch_stage(const KLaunch& L, const double* Us, const void* Tin, co
 cudaError_t launch_norm(long E, const double* part, double inv_size, double* norms, long cap, int* counter,
                         int* flag, cudaStream_t st);
 
+// mean = (mean*old_w + U) / new_w over n values (mean starts at 0 when reset)
+cudaError_t launch_mean_update(long n, double* mean, const double* U, double old_w, double new_w, int reset,
+                               cudaStream_t st);
+
 // per compute type (kernels_fp64.cu / kernels_fp32.cu)
 cudaError_t prepare_fp64(int P);
 cudaError_t launch_trace_fp64(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);

@@ -63,6 +63,24 @@ cudaError_t launch_norm(long E, const double* part, double inv_size, double* nor
   return cudaGetLastError();
 }
 
+// running mean of the state (output.cpp:39-49): mean = (mean*old + U) / new,
+// unfused like the reference's expression; `reset` starts from zero
+__global__ void mean_update_kernel(long n, double* __restrict__ mean, const double* __restrict__ U, double old_w,
+                                   double new_w, int reset)
+{
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double m = reset ? 0. : mean[i];
+    mean[i] = __ddiv_rn(__dadd_rn(__dmul_rn(m, old_w), U[i]), new_w);
+  }
+}
+
+cudaError_t launch_mean_update(long n, double* mean, const double* U, double old_w, double new_w, int reset,
+                               cudaStream_t st)
+{
+  mean_update_kernel<<<148 * 8, 256, 0, st>>>(n, mean, U, old_w, new_w, reset);
+  return cudaGetLastError();
+}
+
 cudaError_t prepare_fp64(int P)
 {
   switch (P) {

@@ -120,6 +120,17 @@ int dgb_get_state(dgb_handle* h, double* U_host);
 int dgb_set_state_device(dgb_handle* h, const double* U_dev);
 int dgb_get_state_device(dgb_handle* h, double* U_dev);
 
+/* Running mean of the resident state, the reference's "mean" output
+ * (update_mean, output.cpp:39-49, called after every step from -mean_start,
+ * dg.cpp:123-131): after step `tstep` >= mean_start,
+ *   mean = (mean * (tstep - mean_start) + U) / (tstep + 1 - mean_start),
+ * starting from zero at tstep == mean_start.  Queued on the handle's stream.
+ * dgb_set_mean / dgb_get_mean copy it from / to the host (e.g. to continue
+ * averaging after reading a .dg file that holds a "mean" output). */
+int dgb_mean_update(dgb_handle* h, unsigned long long tstep, unsigned long long mean_start);
+int dgb_set_mean(dgb_handle* h, const double* mean_host);
+int dgb_get_mean(dgb_handle* h, double* mean_host);
+
 /* Device pointer of the handle's resident state (for callers that keep data
  * on the GPU). */
 int dgb_state_device_ptr(dgb_handle* h, double** U_dev);

@@ -67,3 +67,20 @@ def test_dgb_restarts_from_its_own_checkpoint(tmp_path):
     a = dg.read_state(str(tmp_path / "restart_.dg"))[2]
     b = dg.read_state(str(tmp_path / "full_.dg"))[2]
     assert np.array_equal(a, b)
+
+
+def test_dgb_running_mean_matches_the_reference_driver(tmp_path):
+    """-mean_start: the running mean (dg.cpp:123-131, output.cpp:39-49) is
+    written beside the state in the checkpoint and final files."""
+    if not os.path.exists(REF):
+        pytest.skip("reference driver not built here")
+    extra = ["-mean_start", "2"]
+    ours = _run(DGB, "ours_", tmp_path, extra)
+    ref = _run(REF, "ref_", tmp_path, extra)
+    for k in ref:
+        assert abs(ours[k] - ref[k]) <= 1e-10 * ref[k]
+    for suffix in ("3.dg", ".dg"):
+        for key in ("state", "mean"):
+            _, _, a = dg.read_state(str(tmp_path / f"ours_{suffix}"), key)
+            _, _, b = dg.read_state(str(tmp_path / f"ref_{suffix}"), key)
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12, (suffix, key)

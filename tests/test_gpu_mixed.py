@@ -71,3 +71,31 @@ def test_mixed_time_steps_track_reference_fixture():
         s.step(c.scheme, c.dt, c.nsteps)
         U = s.get_state()
     assert rel(U, gold[f"{c.name}/UN"]) < 1e-7
+
+
+def test_mixed_at_the_48_cubed_p4_configuration():
+    """The mixed-precision configuration's size (TGV, 48^3 hexes, p = 4): after
+    200 RK4 steps the mixed state is within 1e-6 (relative L2) of the FP64
+    form's, and the kinetic-energy history (dissipation) agrees to 1e-7."""
+    import math
+
+    import torch
+
+    from dgpr_b200 import functionals as F
+    c, dt = _tgv(48, 4)
+    L = 2 * math.pi
+    quad = F.BoxQuadrature(48, 48, 48, 4, L, L, L, device="cuda")
+    out, ke = {}, {}
+    for prec in (dg.FP64, dg.MIXED_FP32):
+        with solver(c, prec) as s:
+            s.set_state(c.U)
+            hist = []
+            for _ in range(4):
+                s.step(dg.RK4, dt, 50, norms=False)
+                hist.append(float(F.kinetic_energy(torch.tensor(s.get_state(), device="cuda"), quad)))
+            out[prec] = s.get_state()
+            ke[prec] = np.array(hist)
+    err = rel(out[dg.MIXED_FP32], out[dg.FP64])
+    assert err < 1e-6, err
+    assert np.max(np.abs(ke[dg.MIXED_FP32] - ke[dg.FP64])) < 1e-7 * np.max(np.abs(ke[dg.FP64]))
+    assert np.all(np.diff(ke[dg.FP64]) < 0), "viscous TGV dissipates kinetic energy"
