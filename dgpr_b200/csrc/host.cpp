@@ -2,6 +2,9 @@
 // operators, affine element geometry and the structured neighbour table.
 #include "host.hpp"
 
+#include <algorithm>
+#include <thread>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -378,15 +381,26 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     g[kGeoDetJ] = dJ;
     for (int lf = 0; lf < 6; ++lf) face_normal(J0, lf, g + kGeoN + 3 * lf, g + kGeoFJ + lf);
   }
-  if (curved) {
+  if (curved) {  // per-point geometry, elements split over the host's threads
     const int NB = P * P * P, NQF = P * P;
     gv.assign((size_t)E * kVolC * NB, 0.);
     gf.assign((size_t)E * 6 * kFaceC * NQF, 0.);
-    for (long e = 0; e < E; ++e) {
-      const int rc = curved_element(m.nodes + (size_t)e * nq * 3, q, ops, &gv[(size_t)e * kVolC * NB],
-                                    &gf[(size_t)e * 6 * kFaceC * NQF], e, why);
-      if (rc) return rc;
-    }
+    const int nth = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<int> rcs(nth, DGB_OK);
+    std::vector<std::string> whys(nth);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; ++t)
+      pool.emplace_back([&, t]() {
+        for (long e = t; e < E && rcs[t] == DGB_OK; e += nth)
+          rcs[t] = curved_element(m.nodes + (size_t)e * nq * 3, q, ops, &gv[(size_t)e * kVolC * NB],
+                                  &gf[(size_t)e * 6 * kFaceC * NQF], e, whys[t]);
+      });
+    for (auto& th : pool) th.join();
+    for (int t = 0; t < nth; ++t)
+      if (rcs[t]) {
+        why = whys[t];
+        return rcs[t];
+      }
   }
 
   // neighbours (geometry_common.cpp:397-414 adjacency, periodic wrap as
