@@ -253,7 +253,6 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   const double* Dq = so + C::oDq;
   const double* Mi = so + (CV ? C::oBi : C::oMi);
   const double detJ = sg[kGeoDetJ];
-  const double* Ji = sg + kGeoJinv;
   const double gamma = prm.gamma, mu = prm.mu;
   const double* gve = CV ? gv + e * kVolC * NB : nullptr;
   const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
