@@ -507,7 +507,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             Ubb[r] -= dbar[r];
           }
         }
-        if (boundary_state_vjp(nb, Uo, n, Ubb, Uob) && flag) atomicOr(flag, 8);
+        if (boundary_state_vjp(nb, Uo, n, prm, Ubb, Uob) && flag) atomicOr(flag, 8);
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
           TAe[r * NQF + fq] = Uob[r];

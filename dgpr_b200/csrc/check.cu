@@ -88,7 +88,7 @@ extern "C" int dgb_check_pointwise(int which, const double* x, const double* yba
       if (boundary_state(bt, x, aux + 1, prm, y)) return DGB_ERR_BOUNDARY;
       if (xbar && ybar) {
         for (int i = 0; i < 5; ++i) xbar[i] = 0.;
-        if (boundary_state_vjp(bt, x, aux + 1, ybar, xbar)) return DGB_ERR_UNSUPPORTED;
+        if (boundary_state_vjp(bt, x, aux + 1, prm, ybar, xbar)) return DGB_ERR_UNSUPPORTED;
       }
       return DGB_OK;
     }

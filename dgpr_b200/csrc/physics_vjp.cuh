@@ -388,11 +388,14 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   Urbar[0] += rrb;
 }
 
-// Boundary ghost state (boundary_state): Ubbar -> ULbar.  Freestream, inviscid
-// wall and no-slip wall; returns 1 for the subsonic inflow / outflow states,
-// whose adjoint this build does not provide.
+// Boundary ghost state (boundary_state): Ubbar -> ULbar for every boundary
+// type.  Subsonic inflow depends on UL only through the outgoing Riemann
+// invariant Jp (the boundary Mach number is a root of a quadratic in Jp, the
+// same root as the forward picks; none -> no dependence); subsonic outflow
+// through Jp, the entropy pp / rho^gamma and the tangential velocity.
+// Returns 0 (1 is kept for a boundary type without an adjoint).
 template <class T>
-DGB_HD int boundary_state_vjp(int bt, const T* UL, const T* n, const T* Ubbar, T* ULbar)
+DGB_HD int boundary_state_vjp(int bt, const T* UL, const T* n, const DevParams& prm, const T* Ubbar, T* ULbar)
 {
   if (bt == -3) return 0;  // freestream: constant
   if (bt == -4) {
@@ -425,7 +428,122 @@ DGB_HD int boundary_state_vjp(int bt, const T* UL, const T* n, const T* Ubbar, T
     ULbar[4] += Ubbar[4];
     return 0;
   }
-  return 1;
+  if (bt != -5 && bt != -6) return 1;
+
+  // forward quantities shared by inflow and outflow
+  const T gamma = T(prm.gamma), gm1 = gamma - T(1);
+  const T r0 = UL[0], ir = T(1) / r0;
+  const T v[3] = {UL[1] * ir, UL[2] * ir, UL[3] * ir};
+  const T q2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const T pp = gm1 * (UL[4] - T(0.5) * r0 * q2);
+  const T unp = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+  const T cp = sqrt(gamma * pp / r0);
+  const T Jp = unp + T(2) * cp / gm1;
+  T Jpbar = T(0), unpbar = T(0), vbar[3] = {T(0), T(0), T(0)}, ppbar = T(0), r0bar = T(0);
+
+  if (bt == -5) {  // subsonic inflow
+    const T RTt = gamma * T(prm.R) * T(prm.Tt);
+    const T a = RTt - T(0.5) * gm1 * Jp * Jp;
+    const T b = -T(4) * RTt / gm1;
+    const T c = T(4) * RTt / (gm1 * gm1) - Jp * Jp;
+    const T disc = sqrt(b * b - T(4) * a * c);
+    const T s0 = (-b + disc) / (T(2) * a), s1 = (-b - disc) / (T(2) * a);
+    int pick = -1;  // 0: s0, 1: s1 (the forward's choice)
+    if (s0 >= T(0) && s1 >= T(0)) pick = s0 < s1 ? 0 : 1;
+    else if (s0 >= T(0)) pick = 0;
+    else if (s1 >= T(0)) pick = 1;
+    if (pick < 0) return 0;  // no root: the ghost state does not depend on UL
+    const T Mb = pick == 0 ? s0 : s1;
+    const T Tt = T(prm.Tt), Pt = T(prm.Pt), R = T(prm.R);
+    const T den = T(1) + T(0.5) * gm1 * Mb * Mb;
+    const T Tb = Tt / den;
+    const T Pb = Pt * pow(Tb / Tt, gamma / gm1);
+    const T rb = Pb / (R * Tb);
+    const T cb = sqrt(gamma * Pb / rb);
+    // Ub = (rb, rb ub, Pb/gm1 + rb |ub|^2 / 2), ub = -Mb cb n
+    T rbbar = Ubbar[0], Mbbar = T(0), cbbar = T(0), Pbbar = Ubbar[4] / gm1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T ubk = -Mb * cb * n[k];
+      rbbar += Ubbar[1 + k] * ubk;
+      const T ubbar = Ubbar[1 + k] * rb;
+      Mbbar += -ubbar * cb * n[k];
+      cbbar += -ubbar * Mb * n[k];
+    }
+    rbbar += T(0.5) * Ubbar[4] * Mb * Mb * cb * cb;
+    Mbbar += Ubbar[4] * rb * Mb * cb * cb;
+    cbbar += Ubbar[4] * rb * Mb * Mb * cb;
+    // cb = sqrt(gamma Pb / rb)
+    Pbbar += cbbar * cb / (T(2) * Pb);
+    rbbar += -cbbar * cb / (T(2) * rb);
+    // rb = Pb / (R Tb)
+    Pbbar += rbbar / (R * Tb);
+    T Tbbar = -rbbar * rb / Tb;
+    // Pb = Pt (Tb/Tt)^(gamma/gm1)
+    Tbbar += Pbbar * Pb * (gamma / gm1) / Tb;
+    // Tb = Tt / den, den = 1 + gm1 Mb^2 / 2
+    Mbbar += -Tbbar * Tb / den * gm1 * Mb;
+    // Mb = (-b +- disc) / (2 a)
+    const T sgn = pick == 0 ? T(1) : T(-1);
+    const T discbar = Mbbar * sgn / (T(2) * a);
+    T abar = -Mbbar * Mb / a;
+    // disc = sqrt(b^2 - 4 a c)
+    abar += -discbar * T(2) * c / disc;
+    const T cbar = -discbar * T(2) * a / disc;
+    // a = RTt - gm1 Jp^2 / 2, c = 4 RTt / gm1^2 - Jp^2
+    Jpbar = -abar * gm1 * Jp - cbar * T(2) * Jp;
+  } else {  // subsonic outflow
+    const T Pf = T(prm.P);
+    const T Sp = pp / pow(r0, gamma);
+    const T rb = pow(Pf / Sp, T(1) / gamma);
+    const T cb = sqrt(gamma * Pf / rb);
+    const T unb = Jp - T(2) * cb / gm1;
+    T ub[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ub[k] = v[k] - unp * n[k] + unb * n[k];
+    // Ub = (rb, rb ub, Pf/gm1 + rb |ub|^2 / 2)
+    T rbbar = Ubbar[0], unbbar = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      rbbar += Ubbar[1 + k] * ub[k] + T(0.5) * Ubbar[4] * ub[k] * ub[k];
+      const T ubbar = Ubbar[1 + k] * rb + Ubbar[4] * rb * ub[k];
+      vbar[k] += ubbar;
+      unpbar += -ubbar * n[k];
+      unbbar += ubbar * n[k];
+    }
+    // unb = Jp - 2 cb / gm1
+    Jpbar += unbbar;
+    const T cbbar = -T(2) * unbbar / gm1;
+    // cb = sqrt(gamma Pf / rb)
+    rbbar += -cbbar * cb / (T(2) * rb);
+    // rb = (Pf / Sp)^(1/gamma)
+    const T Spbar = -rbbar * rb / (gamma * Sp);
+    // Sp = pp rho^-gamma
+    ppbar += Spbar * Sp / pp;
+    r0bar += -Spbar * gamma * Sp / r0;
+  }
+  // Jp = unp + 2 cp / gm1, cp = sqrt(gamma pp / rho)
+  unpbar += Jpbar;
+  const T cpbar = T(2) * Jpbar / gm1;
+  ppbar += cpbar * cp / (T(2) * pp);
+  r0bar += -cpbar * cp / (T(2) * r0);
+  // unp = v . n
+#pragma unroll
+  for (int k = 0; k < 3; ++k) vbar[k] += unpbar * n[k];
+  // pp = gm1 (E - rho q2 / 2)
+  ULbar[4] += gm1 * ppbar;
+  r0bar += -T(0.5) * gm1 * q2 * ppbar;
+  const T q2bar = -T(0.5) * gm1 * r0 * ppbar;
+  // q2 = |v|^2, v = m / rho
+  T irbar = T(0);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const T vk = vbar[k] + T(2) * v[k] * q2bar;
+    ULbar[1 + k] += vk * ir;
+    irbar += vk * UL[1 + k];
+  }
+  ULbar[0] += r0bar - irbar * ir * ir;
+  return 0;
 }
 
 }  // namespace dgb

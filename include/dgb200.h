@@ -187,10 +187,9 @@ int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params* params, co
 /* ------------------------------------------------------------------ adjoint
  * Discrete adjoint of the FP64 residual and of the RK steps, hand-written
  * (reverse mode of every kernel).  The reference has no adjoint: these entry
- * points have no counterpart there.  Boundaries: periodic, freestream,
- * inviscid and no-slip walls (DGB_ERR_UNSUPPORTED for subsonic inflow or
- * outflow sides).  A mixed-precision handle recomputes states in its own
- * precision and applies the FP64 adjoint at them. */
+ * points have no counterpart there.  They cover every mesh and boundary
+ * type the forward path does.  A mixed-precision handle recomputes states in
+ * its own precision and applies the FP64 adjoint at them. */
 
 /* Ubar = (df/dU)^T lam at U, f = -Minv R(U) as dgb_residual computes it.
  * Host arrays in the state layout; synchronises. */

@@ -17,7 +17,7 @@ enum {
   DGB_CHECK_VISC_JUMP_N = 4,     /* x = S[5], d[5];    aux = {mu, n[3]};    y = A(S, d n^T).n[5] */
   DGB_CHECK_ROE = 5,             /* x = Ul[5], Ur[5];  aux = {gamma, n[3]}; y = Roe flux[5] (flux.cpp:56-154) */
   DGB_CHECK_BOUNDARY_STATE = 6   /* x = UL[5]; aux = {btype, n[3], gamma, R, P, Pt, Tt, Ufr[5]}; y = Ub[5]
-                                    (bound_states.cpp:24-130); reverse mode for btype -3, -4, -7 */
+                                    (bound_states.cpp:24-130); reverse mode for btype -3 .. -7 */
 };
 
 /* Evaluates function `which` at x into y; when ybar and xbar are non-NULL

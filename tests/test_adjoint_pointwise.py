@@ -112,6 +112,37 @@ def test_wall_and_freestream_state_vjp(bt):
         fd_check(6, state(rng), aux, rng)
 
 
+@pytest.mark.parametrize("bt,normal", [(-5, (-1.0, 0.0, 0.0)), (-6, (1.0, 0.0, 0.0))],
+                         ids=["subsonic_inflow", "subsonic_outflow"])
+def test_inflow_outflow_state_vjp(bt, normal):
+    """The characteristic inflow / outflow ghost states (bound_states.cpp:53-130):
+    total conditions of a Mach 0.3 freestream, interior states near it,
+    normals near the side's axis."""
+    rng = np.random.default_rng(40 + bt)
+    g, R, rho, u, c = 1.4, 287.0, 1.0, 0.3, 1.0
+    P = c * c * rho / g
+    T = P / (rho * R)
+    M = u / c
+    Tt = T * (1 + 0.5 * (g - 1) * M * M)
+    Pt = P * (Tt / T) ** (g / (g - 1))
+    Ufr = [rho, rho * u, 0.0, 0.0, P / (g - 1) + 0.5 * rho * u * u]
+    checked = 0
+    for _ in range(60):
+        n = np.array(normal) + 0.2 * rng.standard_normal(3)
+        n /= np.linalg.norm(n)
+        x = state(rng, rho=1.0, vel=0.3, p=P)
+        x[1] += 0.3 * x[0]
+        aux = [bt, *n, g, R, P, Pt, Tt, *Ufr]
+        y = np.zeros(5)
+        if _fn()(6, _p(x), None, _p(np.array(aux, np.float64)), _p(y), None) == dg.ERR_BOUNDARY:
+            continue  # the forward has no boundary Mach root for this state (it reports that)
+        fd_check(6, x, aux, rng)
+        checked += 1
+        if checked == 6:
+            break
+    assert checked == 6
+
+
 def test_forward_pointwise_matches_reference():
     ref = oracle.reference()
     if ref is None:

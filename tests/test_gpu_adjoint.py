@@ -3,7 +3,7 @@
   residual VJP   the full vector (df/dU)^T lam against central-difference
                  Jacobians of dgb_residual on tiny meshes (every entry), and
                  dot-product tests <lam, J v> = <J^T lam, v> on every residual
-                 case with an adjoint (periodic, freestream, walls; p = 0..6)
+                 case (all boundary types, affine and curved, p = 0..6)
   step VJP       one RK4 / TVD-RK3 step against central differences of dgb_step
   N steps        dgb_forward_record / dgb_backward against central differences,
                  bit-identical gradients for every checkpoint budget, and the
@@ -81,7 +81,7 @@ def test_residual_vjp_equals_transposed_fd_jacobian(case):
     assert rel(vjp, fd) < 1e-7, rel(vjp, fd)
 
 
-ADJ_CASES = [c for c in C.residual_cases() if c.name != "walls_inout_p2"]
+ADJ_CASES = C.residual_cases()
 
 
 @pytest.mark.parametrize("case", ADJ_CASES, ids=lambda c: c.name)
@@ -96,14 +96,6 @@ def test_residual_vjp_dot_product(case):
             fd = lam @ (s.residual(U + h * v)[1] - s.residual(U - h * v)[1]) / (2 * h)
             an = s.residual_vjp(U, lam) @ v
             assert abs(fd - an) <= 1e-7 * abs(an), (fd, an)
-
-
-def test_subsonic_inflow_outflow_adjoint_is_unsupported():
-    case = next(c for c in C.residual_cases() if c.name == "walls_inout_p2")
-    with solver(case) as s:
-        with pytest.raises(dg.DgbError) as e:
-            s.residual_vjp(case.U, np.ones(case.U.size))
-        assert e.value.code == dg.ERR_UNSUPPORTED
 
 
 def test_residual_vjp_is_linear_in_lam():
@@ -127,6 +119,7 @@ STEP_CASES = [
     ("walls_visc", "freestream_p2", 2e-3),
     ("noslip", "noslip_p3", 1e-3),
     ("euler", "euler_p2", 2e-3),
+    ("inflow_outflow", "walls_inout_p2", 2e-3),
 ]
 
 
