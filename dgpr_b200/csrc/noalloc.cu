@@ -60,8 +60,6 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   bool curved = false;
   rc = build_geometry(*mesh, ops, geo, nbr, why, curved, gv, gf);
   if (rc) return set_last_error(rc, why);
-  if (curved)
-    return set_last_error(DGB_ERR_UNSUPPORTED, "curved elements need per-point geometry: use dgb_create");
   const int P = ops.P, NQF = P * P;
   const long E = (long)mesh->nx * mesh->ny * mesh->nz;
   std::vector<double> table(ops_table_size(P));
@@ -72,7 +70,9 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   const size_t oGeo = oOps + round256(sizeof(double) * table.size());
   const size_t oNbr = oGeo + round256(sizeof(double) * geo.size());
   const size_t oTr = oNbr + round256(sizeof(int32_t) * nbr.size());
-  const size_t oFlag = oTr + round256(sizeof(double) * (size_t)E * 60 * NQF);
+  const size_t oGv = oTr + round256(sizeof(double) * (size_t)E * 60 * NQF);  // curved meshes: per-point geometry
+  const size_t oGf = oGv + round256(sizeof(double) * gv.size());
+  const size_t oFlag = oGf + round256(sizeof(double) * gf.size());
   const size_t need = oFlag + 256;
   if (need > kNoallocScratchBytes)
     return set_last_error(DGB_ERR_ARG, "mesh needs " + std::to_string(need) +
@@ -110,6 +110,10 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   } while (0)
   NA_CK(cudaMemcpyAsync(base + oOps, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(base + oGeo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice, st));
+  if (curved) {
+    NA_CK(cudaMemcpyAsync(base + oGv, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice, st));
+    NA_CK(cudaMemcpyAsync(base + oGf, gf.data(), sizeof(double) * gf.size(), cudaMemcpyHostToDevice, st));
+  }
   NA_CK(cudaMemcpyAsync(base + oNbr, nbr.data(), sizeof(int32_t) * nbr.size(), cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));  // status word must start at zero
 
@@ -121,6 +125,8 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   L.opsd = reinterpret_cast<const double*>(base + oOps);
   L.geo = reinterpret_cast<const double*>(base + oGeo);
   L.nbr = reinterpret_cast<const int*>(base + oNbr);
+  L.gv = curved ? reinterpret_cast<const double*>(base + oGv) : nullptr;
+  L.gf = curved ? reinterpret_cast<const double*>(base + oGf) : nullptr;
   L.prm.gamma = params->gamma;
   L.prm.R = params->R;
   L.prm.mu = params->mu;

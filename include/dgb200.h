@@ -165,7 +165,6 @@ long long dgb_last_launch_count(const dgb_handle* h);
 int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk);
 
 /* One FP64 residual f = -Minv R of a device-resident state U_dev into f_dev
- * on a mesh of affine elements (curved meshes: DGB_ERR_UNSUPPORTED)
  * (both caller-owned device arrays, layout U[e][r][b]), for callers that may
  * not allocate GPU memory -- e.g. a host application that owns the device
  * memory pool, or a solver that has claimed all of HBM for its own state.
@@ -173,7 +172,7 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
  * element geometry, neighbour table, face traces, status word) lives in one
  * file-scope device array of 32 MiB built into the library, which every GPU
  * that loads the library holds until the process exits.  Meshes needing more
- * scratch than that (about 4,000 elements at p = 3) are rejected with
+ * scratch than that (about 4,000 affine or 1,500 curved elements at p = 3) are rejected with
  * DGB_ERR_ARG and a message giving the size needed.
  * The first call on each device looks up the array's device address (set-up);
  * make that first call before any stream capture.  All calls share the array

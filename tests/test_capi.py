@@ -122,20 +122,22 @@ def test_invalid_meshes_are_rejected_before_device_work():
     assert _try_create(2, 2, 2, 2, 2, bump, [dg.PERIODIC, dg.PERIODIC] + [dg.FREESTREAM] * 4) == dg.ERR_GEOMETRY
 
 
-def test_noalloc_residual_rejects_curved_meshes_before_device_work():
+def test_noalloc_residual_rejects_oversized_meshes_before_device_work():
+    """The 32 MiB static scratch bounds the mesh; the size check comes before
+    any CUDA call (curved meshes need more per element than affine ones)."""
     import ctypes
-    bump = dg.bump_nodes(2, 2, 1, 2, 2.0, 1.0, 0.5, 0.0, 0.1, 1.0, 0.05)
-    mesh = dg.Mesh(2, 2, 1, 2, 2, bump, [dg.FREESTREAM] * 6)
     prm = dg.make_reference_state()
     fn = dg.lib().dgb_residual_noalloc
     fn.restype = ctypes.c_int
     fn.argtypes = [ctypes.POINTER(dg.MeshDesc), ctypes.POINTER(dg.Params), ctypes.c_void_p, ctypes.c_void_p,
                    ctypes.c_void_p]
-    desc = mesh.desc()
-    # device pointers are never touched: the mesh is refused first
-    assert fn(ctypes.byref(desc), ctypes.byref(prm), ctypes.c_void_p(16), ctypes.c_void_p(16), None) == \
-        dg.ERR_UNSUPPORTED
-
+    for n, q, nodes in [(20, 1, C.box_nodes(20, 20, 20, 1, 1.0, 1.0, 1.0)),
+                        (12, 2, C.sine_nodes(12, 12, 12, 2, 1.0, 1.0, 1.0, 0.02))]:
+        desc = dg.Mesh(n, n, n, 3, q, nodes, [dg.PERIODIC] * 6).desc()
+        # device pointers are never touched: the mesh is refused first
+        assert fn(ctypes.byref(desc), ctypes.byref(prm), ctypes.c_void_p(16), ctypes.c_void_p(16), None) == \
+            dg.ERR_ARG
+        assert "32 MiB" in dg.lib().dgb_last_error_message().decode()
 
 def test_read_state_finds_a_key_without_copying(tmp_path):
     import ctypes

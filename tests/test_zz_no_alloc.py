@@ -66,3 +66,12 @@ def test_noalloc_rejects_meshes_beyond_its_scratch():
     with pytest.raises(dg.DgbError) as e:
         _noalloc(c, c.U)
     assert e.value.code == dg.ERR_ARG and "32 MiB" in str(e.value)
+
+
+def test_noalloc_residual_on_curved_meshes():
+    """Curved elements: the per-point geometry shares the static array."""
+    cases = {c.name: c for c in C.residual_cases()}
+    for name in ("bump_p2_q2", "sine_periodic_p2_q2"):
+        c = cases[name]
+        f = _noalloc(c, c.U)
+        assert rel(f, _reference_entry(c, c.U)) < 1e-11, name
