@@ -322,6 +322,29 @@ def _adjoint_config(dg, torch, nsteps, budgets):
     return out
 
 
+def _curved_block(dg, torch, steps):
+    """The same TGV workload on curved elements: the 32^3 box sinusoidally
+    mapped (q = 2 nodes, y displaced by 0.1 sin x sin z), so every element
+    carries per-point geometry.  Device time per step of both forms."""
+    from tests import cases as C
+    n, p, q = N_EL, P_ORD, 2
+    nodes = C.sine_nodes(n, n, n, q, L_BOX, L_BOX, L_BOX, 0.1)
+    prm = C.params(mu=1.0 / 1600.0, c=10.0, u=0.0, v=0.0, w=0.0)
+    U0 = C.taylor_green(C.node_coords(n, n, n, p, q, nodes)).reshape(-1)
+    dt = 0.2 * (L_BOX / n) / ((2 * p + 1) * (10.0 + 1.0))
+    mesh = dg.Mesh(n, n, n, p, q, nodes, [dg.PERIODIC] * 6)
+    stream = torch.cuda.Stream()
+    out = {"workload": f"TGV on a sinusoidally mapped {n}^3 mesh, q = {q}, p = {p}, RK4 (per-point geometry)"}
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_stream(stream.cuda_stream)
+            s.set_state(U0)
+            _warm(dg, torch, s, dt, 3)
+            ms = _timed_steps(dg, torch, s, stream, dt, steps) / steps
+        out[name] = {"ms_per_step": ms, "value": 5 * (p + 1) ** 3 * n ** 3 * 4 / (ms * 1e-3), "unit": UNIT}
+    return out
+
+
 def run_reverse_steps(args):
     """Warm-up plus `steps` reverse RK4 steps of the FP64 adjoint at the
     workload's state (a short, profilable run of the adjoint kernels)."""
@@ -429,6 +452,8 @@ def run_ours(args, rank, world, local_rank):
                "reverse_over_forward": rev_ms / (ms / args.steps), "reverse_step_launches": rev_launches,
                "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
+    curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
+
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
     try:
@@ -472,6 +497,7 @@ def run_ours(args, rank, world, local_rank):
                       "dtype": "f32 contractions/fluxes, f64 geometry/inverse mass/RK state",
                       "accuracy": acc},
             "adjoint": adj,
+            "curved": curved,
             "clocks": clocks,
         }
         if cpu:
@@ -486,6 +512,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-curved", action="store_true", help="skip the curved-mesh block")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")
