@@ -222,3 +222,23 @@ def run_cases():
     out.append(Case("sine_channel_tvdrk3", 3, 2, 2, 2, 3, nodes, [P_, P_, NS_, NS_, P_, P_], prm, U,
                     scheme=1, dt=2e-3, nsteps=5))
     return out
+
+
+def long_run_cases():
+    """The benchmark configurations at their own step counts, sized for the
+    reference CPU solver: the isentropic vortex in full (8^3, p = 2, 100 RK4
+    steps of dt 0.01 on [0,10]^3) and the Taylor-Green vortex (Re 1600,
+    Ma 0.1) at 8^3 hexes, p = 3, for 1000 RK4 steps."""
+    out = []
+    n = 8
+    nodes = box_nodes(n, n, n, 1, 10.0, 10.0, 10.0)
+    prm = params(mu=0.0, c=math.sqrt(1.4), u=1.0, v=1.0)  # rho = p = 1
+    U = isentropic_vortex(node_coords(n, n, n, 2, 1, nodes)).reshape(-1)
+    out.append(Case("vortex_8_p2_100", n, n, n, 2, 1, nodes, [P_] * 6, prm, U, scheme=0, dt=0.01, nsteps=100))
+    L = 2 * math.pi
+    nodes = box_nodes(n, n, n, 1, L, L, L)
+    prm = params(mu=1.0 / 1600.0, c=10.0, u=0.0, v=0.0, w=0.0)
+    U = taylor_green(node_coords(n, n, n, 3, 1, nodes)).reshape(-1)
+    dt = 0.2 * (L / n) / ((2 * 3 + 1) * (10.0 + 1.0))
+    out.append(Case("tgv_8_p3_1000", n, n, n, 3, 1, nodes, [P_] * 6, prm, U, scheme=0, dt=dt, nsteps=1000))
+    return out

@@ -191,3 +191,27 @@ def test_curved_steps_match_oracle():
         U = s.get_state()
     Uo, _ = oracle.restatement().run(oracle.Mesh(3, 3, 3, 3, 3, c.nodes, c.bounds), c.prm, c.U, 0, dt, 3)
     assert rel(U, Uo) < 1e-12
+
+
+LONG = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden", "long_runs.npz")
+
+
+@pytest.mark.parametrize("case", C.long_run_cases(), ids=lambda c: c.name)
+def test_long_runs_match_the_reference(case):
+    """The isentropic vortex in full (100 steps) and the Taylor-Green vortex
+    for its 1000 steps (8^3, p = 3) against the reference FP64 solver: the
+    state after N steps within 1e-12 relative L2, every printed norm within
+    1e-10; the mixed form within 1e-6."""
+    gold = np.load(LONG)
+    UN, norms_ref = gold[f"{case.name}/UN"], gold[f"{case.name}/norms"]
+    with solver(case) as s:
+        s.set_state(case.U)
+        norms = s.step(case.scheme, case.dt, case.nsteps)
+        U = s.get_state()
+    assert rel(U, UN) < 1e-12, rel(U, UN)
+    assert rel(norms, norms_ref) < 1e-10
+    with solver(case, dg.MIXED_FP32) as s:
+        s.set_state(case.U)
+        s.step(case.scheme, case.dt, case.nsteps, norms=False)
+        Um = s.get_state()
+    assert rel(Um, UN) < 1e-6, rel(Um, UN)
