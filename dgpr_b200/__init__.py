@@ -81,6 +81,7 @@ def lib():
                                           ctypes.POINTER(vp)]),
             "dgb_destroy": (ctypes.c_int, [vp]),
             "dgb_set_stream": (ctypes.c_int, [vp, vp]),
+            "dgb_set_prandtl": (ctypes.c_int, [vp, ctypes.c_double]),
             "dgb_state_size": (ctypes.c_longlong, [vp]),
             "dgb_set_state": (ctypes.c_int, [vp, _dp]),
             "dgb_get_state": (ctypes.c_int, [vp, _dp]),
@@ -348,6 +349,12 @@ class Solver:
 
     def synchronize(self):
         _check(lib().dgb_synchronize(self.h))
+
+    def set_prandtl(self, prandtl):
+        """Heat conduction with Prandtl number `prandtl` (0 or inf: off, the
+        reference's physics); drops captured step graphs and any recorded
+        forward run."""
+        _check(lib().dgb_set_prandtl(self.h, float(prandtl)))
 
     def set_state_device(self, U_ptr):
         _check(lib().dgb_set_state_device(self.h, ctypes.c_void_p(U_ptr)))

@@ -36,5 +36,8 @@ struct VjpScratch {
 cudaError_t prepare_adjoint(int P);
 // [trace_kernel (FP64)] + adjA + adjB on stream st; L.opsd is the operator table
 cudaError_t launch_residual_vjp(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
+// the heat-conducting kernels (adjoint_heat.cu); launch_residual_vjp picks them when L.prm.kq != 0
+cudaError_t prepare_adjoint_heat(int P);
+cudaError_t launch_residual_vjp_heat(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
 
 }  // namespace dgb

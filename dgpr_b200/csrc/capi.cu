@@ -308,6 +308,26 @@ int dgb_set_stream(dgb_handle* h, void* stream)
   return DGB_OK;
 }
 
+int dgb_set_prandtl(dgb_handle* h, double prandtl)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (!(prandtl >= 0.)) return fail(DGB_ERR_ARG, "Prandtl number must be >= 0 (0: no heat flux)");
+  const double kq = (prandtl == 0. || std::isinf(prandtl)) ? 0. : h->dprm.mu * h->dprm.gamma / prandtl;
+  if (kq == h->dprm.kq) return DGB_OK;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->dprm.kq = kq;
+  // captured graphs hold the kernel parameters by value; a recorded forward
+  // run was made with the old physics
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_scheme = -1;
+  if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
+  h->rev_graph = nullptr;
+  h->recorded = false;
+  return DGB_OK;
+}
+
 int dgb_synchronize(dgb_handle* h)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");

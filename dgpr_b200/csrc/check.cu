@@ -34,37 +34,43 @@ extern "C" int dgb_check_pointwise(int which, const double* x, const double* yba
       }
       return DGB_OK;
     }
-    case DGB_CHECK_VISC_FLUX: {  // x = S[5] G[3][5], aux = {mu}
+    case DGB_CHECK_VISC_FLUX:       // x = S[5] G[3][5], aux = {mu}
+    case DGB_CHECK_VISC_FLUX_HEAT: {  // aux = {mu, kq}
+      const double kq = which == DGB_CHECK_VISC_FLUX_HEAT ? aux[1] : 0.;
       double G[3][5], Q[3][5];
       std::memcpy(G, x + 5, sizeof G);
-      visc_flux(x, G, aux[0], Q);
+      visc_flux(x, G, aux[0], Q, kq);
       std::memcpy(y, Q, sizeof Q);
       if (xbar && ybar) {
         double Qb[3][5], Gb[3][5] = {};
         std::memcpy(Qb, ybar, sizeof Qb);
         for (int i = 0; i < 5; ++i) xbar[i] = 0.;
-        visc_flux_vjp(x, G, aux[0], Qb, xbar, Gb);
+        visc_flux_vjp(x, G, aux[0], Qb, xbar, Gb, kq);
         std::memcpy(xbar + 5, Gb, sizeof Gb);
       }
       return DGB_OK;
     }
-    case DGB_CHECK_VISC_RANK1: {  // x = S[5] d[5], aux = {mu, n[3]}
+    case DGB_CHECK_VISC_RANK1:       // x = S[5] d[5], aux = {mu, n[3]}
+    case DGB_CHECK_VISC_RANK1_HEAT: {  // aux = {mu, n[3], kq}
+      const double kq = which == DGB_CHECK_VISC_RANK1_HEAT ? aux[4] : 0.;
       double Q[3][5];
-      visc_rank1(x, x + 5, aux + 1, aux[0], Q);
+      visc_rank1(x, x + 5, aux + 1, aux[0], Q, kq);
       std::memcpy(y, Q, sizeof Q);
       if (xbar && ybar) {
         double Qb[3][5];
         std::memcpy(Qb, ybar, sizeof Qb);
         for (int i = 0; i < 10; ++i) xbar[i] = 0.;
-        visc_rank1_vjp(x, x + 5, aux + 1, aux[0], Qb, xbar, xbar + 5);
+        visc_rank1_vjp(x, x + 5, aux + 1, aux[0], Qb, xbar, xbar + 5, kq);
       }
       return DGB_OK;
     }
-    case DGB_CHECK_VISC_JUMP_N: {  // x = S[5] d[5], aux = {mu, n[3]}
-      visc_jump_n(x, x + 5, aux + 1, aux[0], y);
+    case DGB_CHECK_VISC_JUMP_N:       // x = S[5] d[5], aux = {mu, n[3]}
+    case DGB_CHECK_VISC_JUMP_N_HEAT: {  // aux = {mu, n[3], kq}
+      const double kq = which == DGB_CHECK_VISC_JUMP_N_HEAT ? aux[4] : 0.;
+      visc_jump_n(x, x + 5, aux + 1, aux[0], y, kq);
       if (xbar && ybar) {
         for (int i = 0; i < 10; ++i) xbar[i] = 0.;
-        visc_jump_n_vjp(x, x + 5, aux + 1, aux[0], ybar, xbar, xbar + 5);
+        visc_jump_n_vjp(x, x + 5, aux + 1, aux[0], ybar, xbar, xbar + 5, kq);
       }
       return DGB_OK;
     }

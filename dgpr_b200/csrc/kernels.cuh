@@ -197,7 +197,7 @@ __device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T*
 // Written for variables 1..4 (dc has no mass component): fb[(i*4 + r-1)*stride].
 template <class T>
 __device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, const T* n, T mu, const T* Ji,
-                                                     T fw, T* fb, int stride)
+                                                     T fw, T* fb, int stride, T kq)
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -222,6 +222,12 @@ __device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, con
     }
     fb[(i * 4 + 3) * stride] = -fw * en;
   }
+  if (kq != T(0)) {  // the heat flux kq Y(d) n of the energy row
+    const T h = kq * heat_y(S, d);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      fb[(i * 4 + 3) * stride] -= fw * h * (Ji[3 * i] * n[0] + Ji[3 * i + 1] * n[1] + Ji[3 * i + 2] * n[2]);
+  }
 }
 
 // ------------------------------------------------------------- face traces
@@ -238,7 +244,7 @@ __device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, con
 // come from gfe, this element's per-point face geometry [6][kFaceC][P*P].
 template <int P, class T, bool CV>
 __device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY, const T* so, const T* sg,
-                                           T mu, T* __restrict__ Te, const double* __restrict__ gfe)
+                                           T mu, T kq, T* __restrict__ Te, const double* __restrict__ gfe)
 {
   using C = Cfg<P>;
   constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
@@ -326,7 +332,7 @@ __device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY,
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int r = 0; r < 5; ++r) G[c][r] = Ji[c] * g[0][r] + Ji[3 + c] * g[1][r] + Ji[6 + c] * g[2][r];
-      visc_flux(S, G, mu, Q);
+      visc_flux(S, G, mu, Q, kq);
 #pragma unroll
       for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
     }
@@ -351,7 +357,8 @@ struct TraceSmem {
 };
 
 // Face traces of U (FP64 in HBM) into Tr[e][lf][10][P*P] (type T).
-template <int P, class T, bool CV>
+// HT: with the heat flux (prm.kq); without it the heat terms compile away.
+template <int P, class T, bool CV, bool HT>
 __global__ void __launch_bounds__(Cfg<P>::NTS)
 trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, const double* __restrict__ geo,
              const double* __restrict__ gf, T* __restrict__ Tr, DevParams prm)
@@ -376,7 +383,7 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
 #pragma unroll 1
   for (int half = 0; half < 6 / C::FPP; ++half) {
     if (half) __syncthreads();  // the scratch of the previous pass is reused
-    trace_half<P, T, CV>(half, sU, sN, sY, so, sg, T(prm.mu), Te, CV ? gf + e * 6 * kFaceC * NQF : nullptr);
+    trace_half<P, T, CV>(half, sU, sN, sY, so, sg, T(prm.mu), HT ? T(prm.kq) : T(0), Te, CV ? gf + e * 6 * kFaceC * NQF : nullptr);
   }
 }
 
@@ -426,7 +433,9 @@ struct StageSmem {
 // gf [E][6][kFaceC][P^2]; the inverse mass matrix of such an element is
 // B3^-1 diag(1/(w detJ)) B3^-T (its mass matrix is B3^T diag(w detJ) B3 with
 // B3 = B x B x B square), applied as six 1D contractions and a scaling.
-template <int P, class T, bool CV>
+// HT: with the heat flux kq = mu gamma / Pr (prm.kq), an extension the
+// reference does not have; the HT = false kernels carry no trace of it.
+template <int P, class T, bool CV, bool HT>
 __global__ void __launch_bounds__(Cfg<P>::NTS, (MinBlocks<P, T>::value))
 stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __restrict__ opsg,
              const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
@@ -473,7 +482,7 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   const double detJd = geo[e * kGeoStride + kGeoDetJ];
   const T detJ = sg[kGeoDetJ];
   const T* Ji = sg + kGeoJinv;
-  const T gamma = T(prm.gamma), mu = T(prm.mu);
+  const T gamma = T(prm.gamma), mu = T(prm.mu), kq = HT ? T(prm.kq) : T(0);
   T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // residual of node tid
   const double* gve = CV ? gv + e * kVolC * NB : nullptr;
   const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
@@ -517,7 +526,7 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     euler_flux(S, gamma, H);
     if (mu != T(0)) {
       T Q[3][5];
-      visc_flux(S, Gp, mu, Q);
+      visc_flux(S, Gp, mu, Q, kq);
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -628,13 +637,13 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
 #pragma unroll
               for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
             }
-            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF);
+            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
           }
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
           T ro[5], rn[5];
-          visc_jump_n(Uo, d, n, mu, ro);  // BR2 lifting sources of both sides
-          visc_jump_n(Un, d, n, mu, rn);
+          visc_jump_n(Uo, d, n, mu, ro, kq);  // BR2 lifting sources of both sides
+          visc_jump_n(Un, d, n, mu, rn, kq);
           T lift_n;  // the neighbour's lifting scale at this face point
           if constexpr (CV)
             lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
@@ -666,9 +675,9 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
 #pragma unroll
               for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
             }
-            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF);
+            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
           }
-          visc_jump_n(Ub, d, n, mu, rb);
+          visc_jump_n(Ub, d, n, mu, rb, kq);
           const T lb = eta * fJ * (CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ);
 #pragma unroll
           for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
@@ -866,55 +875,104 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
 #pragma unroll 1
     for (int half = 0; half < 6 / FPP; ++half) {
       if (half) __syncthreads();
-      trace_half<P, T, CV>(half, sUn, sX, sX + 10 * FPP * NQF, so, sg, mu, Te, gfe);
+      trace_half<P, T, CV>(half, sUn, sX, sX + 10 * FPP * NQF, so, sg, mu, kq, Te, gfe);
     }
   }
 }
 
 // ------------------------------------------------------------ host launchers
+// Instantiated per compute type T and heat flag HT, one translation unit each
+// (kernels_fp64.cu, kernels_fp32.cu, kernels_heat_fp64.cu, kernels_heat_fp32.cu).
 
-template <int P, class T>
+template <int P, class T, bool HT>
 cudaError_t prepare_p()
 {
-  cudaError_t e = cudaFuncSetAttribute(trace_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(trace_kernel<P, T, false, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TraceSmem<P, T>::TOTAL);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(trace_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(trace_kernel<P, T, true, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TraceSmem<P, T>::TOTAL);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(stage_kernel<P, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(stage_kernel<P, T, false, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              StageSmem<P, T>::TOTAL);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(stage_kernel<P, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(stage_kernel<P, T, true, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              StageSmem<P, T>::TOTAL);
   return e;
 }
 
-template <int P, class T>
+template <int P, class T, bool HT>
 cudaError_t launch_trace_p(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
 {
   if (L.gf)
-    trace_kernel<P, T, true><<<(unsigned)L.E, Cfg<P>::NTS, TraceSmem<P, T>::TOTAL, st>>>(
+    trace_kernel<P, T, true, HT><<<(unsigned)L.E, Cfg<P>::NTS, TraceSmem<P, T>::TOTAL, st>>>(
         L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, L.gf, reinterpret_cast<T*>(Tout), L.prm);
   else
-    trace_kernel<P, T, false><<<(unsigned)L.E, Cfg<P>::NTS, TraceSmem<P, T>::TOTAL, st>>>(
+    trace_kernel<P, T, false, HT><<<(unsigned)L.E, Cfg<P>::NTS, TraceSmem<P, T>::TOTAL, st>>>(
         L.E, U, reinterpret_cast<const T*>(L.ops), L.geo, nullptr, reinterpret_cast<T*>(Tout), L.prm);
   return cudaGetLastError();
 }
 
-template <int P, class T>
+template <int P, class T, bool HT>
 cudaError_t launch_stage_p(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                            cudaStream_t st)
 {
   if (L.gv)
-    stage_kernel<P, T, true><<<(unsigned)L.E, Cfg<P>::NTS, StageSmem<P, T>::TOTAL, st>>>(
+    stage_kernel<P, T, true, HT><<<(unsigned)L.E, Cfg<P>::NTS, StageSmem<P, T>::TOTAL, st>>>(
         L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
         L.nbr, L.prm, sa);
   else
-    stage_kernel<P, T, false><<<(unsigned)L.E, Cfg<P>::NTS, StageSmem<P, T>::TOTAL, st>>>(
+    stage_kernel<P, T, false, HT><<<(unsigned)L.E, Cfg<P>::NTS, StageSmem<P, T>::TOTAL, st>>>(
         L.E, Us, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
         nullptr, L.nbr, L.prm, sa);
   return cudaGetLastError();
+}
+
+// the dispatch on the order, for one (T, HT)
+template <class T, bool HT>
+cudaError_t prepare_t(int P)
+{
+  switch (P) {
+    case 1: return prepare_p<1, T, HT>();
+    case 2: return prepare_p<2, T, HT>();
+    case 3: return prepare_p<3, T, HT>();
+    case 4: return prepare_p<4, T, HT>();
+    case 5: return prepare_p<5, T, HT>();
+    case 6: return prepare_p<6, T, HT>();
+    case 7: return prepare_p<7, T, HT>();
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class T, bool HT>
+cudaError_t launch_trace_t(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
+{
+  switch (L.P) {
+    case 1: return launch_trace_p<1, T, HT>(L, U, Tout, st);
+    case 2: return launch_trace_p<2, T, HT>(L, U, Tout, st);
+    case 3: return launch_trace_p<3, T, HT>(L, U, Tout, st);
+    case 4: return launch_trace_p<4, T, HT>(L, U, Tout, st);
+    case 5: return launch_trace_p<5, T, HT>(L, U, Tout, st);
+    case 6: return launch_trace_p<6, T, HT>(L, U, Tout, st);
+    case 7: return launch_trace_p<7, T, HT>(L, U, Tout, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class T, bool HT>
+cudaError_t launch_stage_t(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                           cudaStream_t st)
+{
+  switch (L.P) {
+    case 1: return launch_stage_p<1, T, HT>(L, Us, Tin, sa, st);
+    case 2: return launch_stage_p<2, T, HT>(L, Us, Tin, sa, st);
+    case 3: return launch_stage_p<3, T, HT>(L, Us, Tin, sa, st);
+    case 4: return launch_stage_p<4, T, HT>(L, Us, Tin, sa, st);
+    case 5: return launch_stage_p<5, T, HT>(L, Us, Tin, sa, st);
+    case 6: return launch_stage_p<6, T, HT>(L, Us, Tin, sa, st);
+    case 7: return launch_stage_p<7, T, HT>(L, Us, Tin, sa, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace dgb

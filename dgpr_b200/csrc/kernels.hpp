@@ -74,5 +74,14 @@ cudaError_t prepare_fp32(int P);
 cudaError_t launch_trace_fp32(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
 cudaError_t launch_stage_fp32(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                               cudaStream_t st);
+// the same with the heat flux (kernels_heat_fp64.cu / kernels_heat_fp32.cu)
+cudaError_t prepare_fp64_heat(int P);
+cudaError_t launch_trace_fp64_heat(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
+cudaError_t launch_stage_fp64_heat(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                                   cudaStream_t st);
+cudaError_t prepare_fp32_heat(int P);
+cudaError_t launch_trace_fp32_heat(const KLaunch& L, const double* U, void* Tout, cudaStream_t st);
+cudaError_t launch_stage_fp32_heat(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
+                                   cudaStream_t st);
 
 }  // namespace dgb

@@ -7,45 +7,20 @@ namespace dgb {
 
 cudaError_t prepare_fp32(int P)
 {
-  switch (P) {
-    case 1: return prepare_p<1, float>();
-    case 2: return prepare_p<2, float>();
-    case 3: return prepare_p<3, float>();
-    case 4: return prepare_p<4, float>();
-    case 5: return prepare_p<5, float>();
-    case 6: return prepare_p<6, float>();
-    case 7: return prepare_p<7, float>();
-  }
-  return cudaErrorInvalidValue;
+  cudaError_t e = prepare_t<float, false>(P);
+  return e == cudaSuccess ? prepare_fp32_heat(P) : e;
 }
 
 cudaError_t launch_trace_fp32(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
 {
-  switch (L.P) {
-    case 1: return launch_trace_p<1, float>(L, U, Tout, st);
-    case 2: return launch_trace_p<2, float>(L, U, Tout, st);
-    case 3: return launch_trace_p<3, float>(L, U, Tout, st);
-    case 4: return launch_trace_p<4, float>(L, U, Tout, st);
-    case 5: return launch_trace_p<5, float>(L, U, Tout, st);
-    case 6: return launch_trace_p<6, float>(L, U, Tout, st);
-    case 7: return launch_trace_p<7, float>(L, U, Tout, st);
-  }
-  return cudaErrorInvalidValue;
+  return L.prm.kq != 0. ? launch_trace_fp32_heat(L, U, Tout, st) : launch_trace_t<float, false>(L, U, Tout, st);
 }
 
 cudaError_t launch_stage_fp32(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                               cudaStream_t st)
 {
-  switch (L.P) {
-    case 1: return launch_stage_p<1, float>(L, Us, Tin, sa, st);
-    case 2: return launch_stage_p<2, float>(L, Us, Tin, sa, st);
-    case 3: return launch_stage_p<3, float>(L, Us, Tin, sa, st);
-    case 4: return launch_stage_p<4, float>(L, Us, Tin, sa, st);
-    case 5: return launch_stage_p<5, float>(L, Us, Tin, sa, st);
-    case 6: return launch_stage_p<6, float>(L, Us, Tin, sa, st);
-    case 7: return launch_stage_p<7, float>(L, Us, Tin, sa, st);
-  }
-  return cudaErrorInvalidValue;
+  return L.prm.kq != 0. ? launch_stage_fp32_heat(L, Us, Tin, sa, st)
+                        : launch_stage_t<float, false>(L, Us, Tin, sa, st);
 }
 
 }  // namespace dgb

@@ -81,47 +81,24 @@ cudaError_t launch_mean_update(long n, double* mean, const double* U, double old
   return cudaGetLastError();
 }
 
+// the heat-conducting kernels (kernels_heat_fp64.cu) are prepared with the
+// plain ones and launched when the handle has a heat flux
 cudaError_t prepare_fp64(int P)
 {
-  switch (P) {
-    case 1: return prepare_p<1, double>();
-    case 2: return prepare_p<2, double>();
-    case 3: return prepare_p<3, double>();
-    case 4: return prepare_p<4, double>();
-    case 5: return prepare_p<5, double>();
-    case 6: return prepare_p<6, double>();
-    case 7: return prepare_p<7, double>();
-  }
-  return cudaErrorInvalidValue;
+  cudaError_t e = prepare_t<double, false>(P);
+  return e == cudaSuccess ? prepare_fp64_heat(P) : e;
 }
 
 cudaError_t launch_trace_fp64(const KLaunch& L, const double* U, void* Tout, cudaStream_t st)
 {
-  switch (L.P) {
-    case 1: return launch_trace_p<1, double>(L, U, Tout, st);
-    case 2: return launch_trace_p<2, double>(L, U, Tout, st);
-    case 3: return launch_trace_p<3, double>(L, U, Tout, st);
-    case 4: return launch_trace_p<4, double>(L, U, Tout, st);
-    case 5: return launch_trace_p<5, double>(L, U, Tout, st);
-    case 6: return launch_trace_p<6, double>(L, U, Tout, st);
-    case 7: return launch_trace_p<7, double>(L, U, Tout, st);
-  }
-  return cudaErrorInvalidValue;
+  return L.prm.kq != 0. ? launch_trace_fp64_heat(L, U, Tout, st) : launch_trace_t<double, false>(L, U, Tout, st);
 }
 
 cudaError_t launch_stage_fp64(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                               cudaStream_t st)
 {
-  switch (L.P) {
-    case 1: return launch_stage_p<1, double>(L, Us, Tin, sa, st);
-    case 2: return launch_stage_p<2, double>(L, Us, Tin, sa, st);
-    case 3: return launch_stage_p<3, double>(L, Us, Tin, sa, st);
-    case 4: return launch_stage_p<4, double>(L, Us, Tin, sa, st);
-    case 5: return launch_stage_p<5, double>(L, Us, Tin, sa, st);
-    case 6: return launch_stage_p<6, double>(L, Us, Tin, sa, st);
-    case 7: return launch_stage_p<7, double>(L, Us, Tin, sa, st);
-  }
-  return cudaErrorInvalidValue;
+  return L.prm.kq != 0. ? launch_stage_fp64_heat(L, Us, Tin, sa, st)
+                        : launch_stage_t<double, false>(L, Us, Tin, sa, st);
 }
 
 cudaError_t prepare_kernels(int P, int precision)

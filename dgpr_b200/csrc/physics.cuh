@@ -16,6 +16,7 @@ namespace dgb {
 
 struct DevParams {
   double gamma, R, mu, P, Pt, Tt, eta;
+  double kq;  // heat-flux coefficient mu gamma / Pr (0: no heat conduction, the reference's physics)
   double Ufr[5];
   double src[5];
 };
@@ -55,10 +56,23 @@ DGB_HD void euler_flux(const T* U, T gamma, T F[3][5])
   }
 }
 
-// Viscous (Stokes, no heat conduction) flux Q[c][r] = A(S, grad S)
-// (flux.cpp:156-202).  G[c][r] = d S_r / d x_c.
+// Heat conduction, an extension the reference does not have (its A has no
+// heat flux, flux.cpp:185-201): the energy flux gains kappa dT/dx with
+// kappa = mu c_p / Pr, T = p / (rho R), which is kq Y with kq = mu gamma / Pr
+// and Y = d(E/rho) - u . du = (1/rho) [dE - e drho - u . dm + |u|^2 drho]
+// for a derivative g = dS of the conserved state (e = E/rho).
 template <class T>
-DGB_HD void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
+DGB_HD T heat_y(const T* S, const T* g)
+{
+  const T ir = T(1) / S[0];
+  const T e = S[4] * ir, u = S[1] * ir, v = S[2] * ir, w = S[3] * ir;
+  return ir * (g[4] - e * g[0] - (u * g[1] + v * g[2] + w * g[3]) + (u * u + v * v + w * w) * g[0]);
+}
+
+// Viscous (Stokes) flux Q[c][r] = A(S, grad S) (flux.cpp:156-202), plus the
+// optional heat flux kq Y_c in the energy row.  G[c][r] = d S_r / d x_c.
+template <class T>
+DGB_HD void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5], T kq = T(0))
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -85,6 +99,10 @@ DGB_HD void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
     Q[c][3] = tau[2][c];
     Q[c][4] = u * tau[0][c] + v * tau[1][c] + w * tau[2][c];
   }
+  if (kq != T(0)) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Q[c][4] += kq * heat_y(S, G[c]);
+  }
 }
 
 // A(S, d (x) n): the viscous flux of a rank-one "gradient" d n^T, the argument
@@ -92,7 +110,7 @@ DGB_HD void visc_flux(const T* S, const T G[3][5], T mu, T Q[3][5])
 // 657-667).  With a_i = (d_{1+i} - d_0 vel_i) / rho the velocity gradient is
 // a n^T, so tau = mu (a n^T + n a^T) + lam (a.n) I.
 template <class T>
-DGB_HD void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5])
+DGB_HD void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5], T kq = T(0))
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -114,11 +132,16 @@ DGB_HD void visc_rank1(const T* S, const T* d, const T* n, T mu, T Q[3][5])
     }
     Q[c][4] = e;
   }
+  if (kq != T(0)) {  // the heat flux of the gradient d n^T: kq Y(d) n
+    const T h = kq * heat_y(S, d);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Q[c][4] += h * n[c];
+  }
 }
 
 // A(S, d (x) n) . n, the normal component only.
 template <class T>
-DGB_HD void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
+DGB_HD void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn, T kq = T(0))
 {
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
@@ -137,6 +160,7 @@ DGB_HD void visc_jump_n(const T* S, const T* d, const T* n, T mu, T* Qn)
     e += vel[i] * t;
   }
   Qn[4] = e;
+  if (kq != T(0)) Qn[4] += kq * heat_y(S, d) * nn;
 }
 
 // Roe flux with the entropy fix at 5% of the Roe sound speed (flux.cpp:56-154).

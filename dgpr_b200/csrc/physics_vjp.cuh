@@ -71,10 +71,42 @@ DGB_HD void euler_flux_n_vjp(const T* U, T gamma, const T* n, const T* Fnbar, T*
   euler_flux_vjp(U, gamma, Fbar, Ubar);
 }
 
+// Heat-flux scalar Y(S, g) (heat_y): ybar -> Sbar[5], gbar[5].  With
+// ir = 1/S_0, v = S_{1..3} ir, e = S_4 ir and
+// B = g_4 + g_0 (|v|^2 - e) - v . g_{1..3}, Y = ir B.
+template <class T>
+DGB_HD void heat_y_vjp(const T* S, const T* g, T yb, T* Sbar, T* gbar)
+{
+  const T ir = T(1) / S[0];
+  const T e = S[4] * ir, v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
+  const T q2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const T B = g[4] + g[0] * (q2 - e) - (v[0] * g[1] + v[1] * g[2] + v[2] * g[3]);
+  const T yi = yb * ir;
+  gbar[4] += yi;
+  gbar[0] += yi * (q2 - e);
+  T irbar = yb * B;
+  const T ebar = -yi * g[0];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    gbar[1 + i] += -yi * v[i];
+    const T vb = yi * (T(2) * g[0] * v[i] - g[1 + i]);
+    Sbar[1 + i] += vb * ir;
+    irbar += vb * S[1 + i];
+  }
+  Sbar[4] += ebar * ir;
+  irbar += ebar * S[4];
+  Sbar[0] += -irbar * ir * ir;
+}
+
 // Viscous flux Q = A(S, G) (visc_flux): Qbar[3][5] -> Sbar[5], Gbar[3][5]
 template <class T>
-DGB_HD void visc_flux_vjp(const T* S, const T G[3][5], T mu, const T Qbar[3][5], T* Sbar, T Gbar[3][5])
+DGB_HD void visc_flux_vjp(const T* S, const T G[3][5], T mu, const T Qbar[3][5], T* Sbar, T Gbar[3][5],
+                          T kq = T(0))
 {
+  if (kq != T(0)) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) heat_y_vjp(S, G[c], kq * Qbar[c][4], Sbar, Gbar[c]);
+  }
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
   const T v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
@@ -142,8 +174,10 @@ DGB_HD void rank1_tail_vjp(const T* S, const T* d, const T* v, T ir, const T* ab
 
 // Rank-one viscous flux Q = A(S, d n^T) (visc_rank1): Qbar[3][5] -> Sbar, dbar
 template <class T>
-DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qbar[3][5], T* Sbar, T* dbar)
+DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qbar[3][5], T* Sbar, T* dbar,
+                           T kq = T(0))
 {
+  if (kq != T(0)) heat_y_vjp(S, d, kq * (Qbar[0][4] * n[0] + Qbar[1][4] * n[1] + Qbar[2][4] * n[2]), Sbar, dbar);
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
   const T v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
@@ -177,8 +211,11 @@ DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qba
 
 // Normal component A(S, d n^T).n (visc_jump_n): Qnbar[5] -> Sbar, dbar
 template <class T>
-DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Qnbar, T* Sbar, T* dbar)
+DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Qnbar, T* Sbar, T* dbar,
+                            T kq = T(0))
 {
+  if (kq != T(0))
+    heat_y_vjp(S, d, kq * Qnbar[4] * (n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), Sbar, dbar);
   const T lam = -(T(2) / T(3)) * mu;
   const T ir = T(1) / S[0];
   const T v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};

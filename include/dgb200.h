@@ -107,6 +107,15 @@ int dgb_set_stream(dgb_handle* h, void* stream);
 /* Waits for the work the handle has queued on its stream. */
 int dgb_synchronize(dgb_handle* h);
 
+/* Optional heat conduction, an extension the reference does not have (its
+ * viscous flux carries no heat flux, flux.cpp:185-201): the energy flux gains
+ * kappa grad T with kappa = mu c_p / Pr, in the volume, trace, dual-consistency
+ * and lifting terms and in their adjoint.  Pr = 0 (the default) or +inf turns
+ * it off, which is the reference's physics bit for bit; Pr < 0 or NaN is an
+ * argument error.  Discards captured step graphs and any recorded forward run
+ * (dgb_forward_record), which used the old physics. */
+int dgb_set_prandtl(dgb_handle* h, double prandtl);
+
 /* Number of doubles in one state array: nx*ny*nz * 5 * (p+1)^3. */
 long long dgb_state_size(const dgb_handle* h);
 

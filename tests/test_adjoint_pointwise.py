@@ -1,6 +1,7 @@
 """The hand-written reverse mode of every pointwise function in the residual
-(Euler flux, viscous flux and its rank-one forms, Roe flux with entropy fix,
-wall ghost states) against central finite differences, on the CPU through the
+(Euler flux, viscous flux and its rank-one forms, with and without the
+optional heat flux, Roe flux with entropy fix, ghost states) against central
+finite differences, on the CPU through the
 check hooks (include/dgb200_check.h).  Also pins the forward functions to the
 reference's own implementations where it is built here.
 
@@ -28,8 +29,8 @@ def _p(a):
     return a.ctypes.data_as(_dp)
 
 
-NOUT = {0: 15, 1: 5, 2: 15, 3: 15, 4: 5, 5: 5, 6: 5}
-NIN = {0: 5, 1: 5, 2: 20, 3: 10, 4: 10, 5: 10, 6: 5}
+NOUT = {0: 15, 1: 5, 2: 15, 3: 15, 4: 5, 5: 5, 6: 5, 7: 15, 8: 15, 9: 5}
+NIN = {0: 5, 1: 5, 2: 20, 3: 10, 4: 10, 5: 10, 6: 5, 7: 20, 8: 10, 9: 10}
 
 
 def call(which, x, aux, ybar=None):
@@ -159,3 +160,72 @@ def test_forward_pointwise_matches_reference():
         Q, _ = call(2, np.concatenate([UL, G]), [0.02])
         Qr = ref.A(UL, G[:5], G[5:10], G[10:], 0.02)
         assert np.max(np.abs(Q.reshape(3, 5) - Qr)) <= 1e-14 * max(1, np.max(np.abs(Qr)))
+
+
+# ---------------------------------------------------------------- heat flux
+# The optional heat flux kq = mu gamma / Pr (an extension: the reference's
+# viscous flux conducts no heat): hooks 7-9 are hooks 2-4 with kq appended.
+
+def _temperature(S, g=1.4, R=287.0):
+    return (g - 1) * (S[4] - 0.5 * (S[1:4] @ S[1:4]) / S[0]) / (S[0] * R)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_heat_flux_vjps(seed):
+    rng = np.random.default_rng(500 + seed)
+    kq = 0.02 * 1.4 / 0.71
+    x = np.concatenate([state(rng), 0.5 * rng.standard_normal(15)])
+    fd_check(7, x, [0.02, kq], rng)
+    x = np.concatenate([state(rng), 0.1 * rng.standard_normal(5)])
+    aux = [0.02, *unit(rng), kq]
+    fd_check(8, x, aux, rng)
+    fd_check(9, x, aux, rng)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_heat_flux_is_kappa_grad_T(seed):
+    """A(S, G) with the heat flux minus A(S, G) without it is kappa dT/dx_c in
+    the energy row only, kappa = mu c_p / Pr with c_p = gamma R / (gamma - 1);
+    dT/dx_c = grad_S T . G[c] with grad_S T by central differences of the
+    temperature of the state (independent of the closed form in the kernels)."""
+    rng = np.random.default_rng(600 + seed)
+    g, R, mu, Pr = 1.4, 287.0, 0.015, 0.71
+    S = state(rng)
+    G = 0.5 * rng.standard_normal((3, 5))
+    x = np.concatenate([S, G.reshape(-1)])
+    Qh, _ = call(7, x, [mu, mu * g / Pr])
+    Q0, _ = call(2, x, [mu])
+    dT = np.zeros(5)
+    for r in range(5):
+        e = np.zeros(5)
+        e[r] = 1e-6 * max(1.0, abs(S[r]))
+        dT[r] = (_temperature(S + e, g, R) - _temperature(S - e, g, R)) / (2 * e[r])
+    kappa = mu * g * R / ((g - 1) * Pr)
+    diff = (Qh - Q0).reshape(3, 5)
+    assert np.all(diff[:, :4] == 0.0)
+    np.testing.assert_allclose(diff[:, 4], kappa * (G @ dT), rtol=1e-7, atol=1e-12)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_heat_flux_rank_one_forms_agree_with_the_full_flux(seed):
+    """A(S, d n^T) (hook 8) and its normal component (hook 9) equal the full
+    flux (hook 7) of the gradient G[c] = n_c d."""
+    rng = np.random.default_rng(700 + seed)
+    S, d, n = state(rng), 0.1 * rng.standard_normal(5), unit(rng) * (0.5 + rng.random())
+    mu, kq = 0.02, 0.02 * 1.4 / 0.71
+    Qf, _ = call(7, np.concatenate([S, np.outer(n, d).reshape(-1)]), [mu, kq])
+    Q1, _ = call(8, np.concatenate([S, d]), [mu, *n, kq])
+    Qn, _ = call(9, np.concatenate([S, d]), [mu, *n, kq])
+    np.testing.assert_allclose(Q1, Qf, rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(Qn, Qf.reshape(3, 5).T @ n, rtol=1e-12, atol=1e-15)
+
+
+def test_zero_heat_flux_is_the_plain_flux_bit_for_bit():
+    rng = np.random.default_rng(9)
+    for _ in range(10):
+        x = np.concatenate([state(rng), 0.5 * rng.standard_normal(15)])
+        assert np.array_equal(call(7, x, [0.02, 0.0])[0], call(2, x, [0.02])[0])
+        x = np.concatenate([state(rng), 0.1 * rng.standard_normal(5)])
+        n = unit(rng)
+        assert np.array_equal(call(8, x, [0.02, *n, 0.0])[0], call(3, x, [0.02, *n])[0])
+        assert np.array_equal(call(9, x, [0.02, *n, 0.0])[0], call(4, x, [0.02, *n])[0])
