@@ -345,6 +345,25 @@ def _curved_block(dg, torch, steps):
     return out
 
 
+def _heat_block(dg, torch, steps):
+    """The headline workload with the configuration's Pr = 0.71 heat flux
+    (dgb_set_prandtl; the reference has no heat conduction, so this is not
+    comparable to its arm).  Device time per step of both forms."""
+    nodes, prm, U0, dt = tgv_case(N_EL, P_ORD)
+    mesh = dg.Mesh(N_EL, N_EL, N_EL, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
+    stream = torch.cuda.Stream()
+    out = {"workload": f"TGV {N_EL}^3 p = {P_ORD} RK4 with heat conduction, Pr = 0.71"}
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_stream(stream.cuda_stream)
+            s.set_prandtl(0.71)
+            s.set_state(U0)
+            _warm(dg, torch, s, dt, 3)
+            ms = _timed_steps(dg, torch, s, stream, dt, steps) / steps
+        out[name] = {"ms_per_step": ms, "value": 5 * (P_ORD + 1) ** 3 * N_EL ** 3 * 4 / (ms * 1e-3), "unit": UNIT}
+    return out
+
+
 def run_reverse_steps(args):
     """Warm-up plus `steps` reverse RK4 steps of the FP64 adjoint at the
     workload's state (a short, profilable run of the adjoint kernels)."""
@@ -453,6 +472,7 @@ def run_ours(args, rank, world, local_rank):
                "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
     curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
+    heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
@@ -498,6 +518,7 @@ def run_ours(args, rank, world, local_rank):
                       "accuracy": acc},
             "adjoint": adj,
             "curved": curved,
+            "heat": heat,
             "clocks": clocks,
         }
         if cpu:
@@ -513,6 +534,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-curved", action="store_true", help="skip the curved-mesh block")
+    ap.add_argument("--no-heat", action="store_true", help="skip the heat-conduction block")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")

@@ -11,7 +11,8 @@
 // Differences: the arithmetic is FP64 (or -precision mixed), not the
 // reference GPU build's FP32; -npx/-npy/-npz must be 1 (one GPU).  The
 // running mean (-mean_start) follows the reference's CPU driver dg.cpp, which
-// has it (cudg.cu does not).
+// has it (cudg.cu does not).  -prandtl adds the optional heat flux (an
+// extension; 0, the default, is the reference's physics).
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
@@ -41,6 +42,7 @@ struct Inputs {
   double source[5] = {0., 0., 0., 0., 0.};
   bool turb = false;
   int precision = DGB_FP64;
+  double prandtl = 0.;
 };
 
 enum Kind { K_U64, K_DBL, K_STR, K_BOOL, K_BTYPE, K_SCHEME, K_PREC };
@@ -116,6 +118,7 @@ int parse(int argc, char** argv, Inputs& in)
       {"ofile", "output file prefix", K_STR, &in.ofile},
       {"ifile", "input file prefix", K_STR, &in.ifile},
       {"precision", "arithmetic: fp64 or mixed", K_PREC, &in.precision},
+      {"prandtl", "Prandtl number of the heat flux (0: none)", K_DBL, &in.prandtl},
   };
   const int nopt = (int)(sizeof opts / sizeof opts[0]);
   if (argc > 1 && !strcmp(argv[1], "-h")) {
@@ -293,6 +296,7 @@ int main(int argc, char** argv)
 
   dgb_handle* h = nullptr;
   if ((rc = dgb_create(&mesh, &prm, in.precision, &h))) die("dgb_create", rc);
+  if ((rc = dgb_set_prandtl(h, in.prandtl))) die("dgb_set_prandtl", rc);
   if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
 
   // running mean (dg.cpp:123-131): an input file may carry one to continue

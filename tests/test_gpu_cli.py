@@ -84,3 +84,18 @@ def test_dgb_running_mean_matches_the_reference_driver(tmp_path):
             _, _, a = dg.read_state(str(tmp_path / f"ours_{suffix}"), key)
             _, _, b = dg.read_state(str(tmp_path / f"ref_{suffix}"), key)
             assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12, (suffix, key)
+
+
+def test_dgb_prandtl_option(tmp_path):
+    """-prandtl turns the optional heat flux on (the bump channel's no-slip
+    wall and turbulent state have temperature gradients); -prandtl 0 is the
+    default physics, bit for bit."""
+    _run(DGB, "plain_", tmp_path)
+    _run(DGB, "zero_", tmp_path, ["-prandtl", "0"])
+    _run(DGB, "heat_", tmp_path, ["-prandtl", "0.71"])
+    plain, zero, heat = (dg.read_state(str(tmp_path / f"{k}_.dg"))[2] for k in ("plain", "zero", "heat"))
+    assert np.array_equal(plain, zero)
+    assert np.linalg.norm(heat - plain) > 1e-12 * np.linalg.norm(plain)
+    out = subprocess.run([DGB] + ARGS + ["-prandtl", "-1", "-ofile", "bad_"], cwd=tmp_path, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode != 0
