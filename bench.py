@@ -319,6 +319,21 @@ def _adjoint_config(dg, torch, nsteps, budgets):
         an = float((torch.tensor(grad, device="cuda") * d).sum())
         out["fd_check"] = {"directional_adjoint": an, "directional_fd": fd, "rel_err": abs(an - fd) / abs(fd),
                            "h": h}
+        # the same sweep with dJ/d[mu, source] (dgb_backward_params), stage-keeping record
+        s.set_state(U0.cpu().numpy())
+        s.forward_record_stages(dg.RK4, dt, nsteps, norms=False)
+        UN = torch.tensor(s.get_state(), device="cuda", requires_grad=True)
+        F.enstrophy(UN, quad).backward()
+        lamN = UN.grad.cpu().numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, dpar = s.backward_params(lamN)
+        tp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s.backward(lamN)
+        tb = time.perf_counter() - t0
+        out["param_gradient"] = {"dJ_dmu": float(dpar[0]), "backward_params_s": tp, "backward_s": tb,
+                                 "over_backward": tp / tb}
     return out
 
 

@@ -20,6 +20,7 @@ INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW
     -1, -2, -3, -4, -5, -6, -7
 RK4, TVDRK3 = 0, 1
 FP64, MIXED_FP32 = 0, 1
+DPARAM_MU, DPARAM_SOURCE, NDPARAMS = 0, 1, 6  # dgb_backward_params: dJ/d[mu, source[0..4]]
 
 BOUNDARY_TYPES = {  # the reference's boundary_types map (boundaries.cpp:37-44)
     "periodic": PERIODIC, "freestream": FREESTREAM, "inviscid_wall": INVISCID_WALL,
@@ -107,6 +108,9 @@ def lib():
                                                          _dp]),
             "dgb_backward": (ctypes.c_int, [vp, _dp, _dp]),
             "dgb_backward_device": (ctypes.c_int, [vp, vp, vp]),
+            "dgb_backward_params": (ctypes.c_int, [vp, _dp, _dp, _dp]),
+            "dgb_backward_params_device": (ctypes.c_int, [vp, vp, vp, vp]),
+            "dgb_set_params": (ctypes.c_int, [vp, ctypes.POINTER(Params)]),
             "dgb_adjoint_stats": (ctypes.c_int, [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3),
             "dgb_checkpoint_plan": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong,
@@ -406,6 +410,25 @@ class Solver:
 
     def backward_device(self, lamN_ptr, out_ptr):
         _check(lib().dgb_backward_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr)))
+
+    def backward_params(self, lamN):
+        """(dJ/dU_0, dJ/d[mu, source[0..4]]) for J with dJ/dU_N = lamN."""
+        lamN = np.ascontiguousarray(lamN, dtype=np.float64).ravel()
+        out = np.zeros(self.n)
+        dpar = np.zeros(NDPARAMS)
+        _check(lib().dgb_backward_params(self.h, _p(lamN), _p(out), _p(dpar)))
+        return out, dpar
+
+    def backward_params_device(self, lamN_ptr, out_ptr, dpar_ptr):
+        _check(lib().dgb_backward_params_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr),
+                                                ctypes.c_void_p(dpar_ptr)))
+
+    def set_params(self, params):
+        """New physical parameters (Params or its 17-vector) for this handle;
+        mesh, state and Prandtl number stay.  Drops the recorded run."""
+        p = params if isinstance(params, Params) else Params.from_array(params)
+        _check(lib().dgb_set_params(self.h, ctypes.byref(p)))
+        self.params = p
 
     def adjoint_stats(self):
         """(steps recomputed, steps reversed) by the last backward sweep and

@@ -60,6 +60,105 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
   return v;
 }
 
+// ---- parameter gradient (dgb_backward_params)
+// Per element e: part[e][0] = sum W . (F1 - F0) * inv_mu1 and
+// part[e][1 + r] = sum_b W[r][b], with W = cx X + cy Y + cz Z the adjoint
+// weight of one residual VJP; fixed-order block sums.
+__global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __restrict__ F1,
+                                 const double* __restrict__ F0, double inv_mu1, double* __restrict__ part)
+{
+  __shared__ double red[DGB_NDPARAMS][128];
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  double acc[DGB_NDPARAMS] = {0., 0., 0., 0., 0., 0.};
+  for (int i = tid; i < 5 * nb; i += blockDim.x) {
+    const long g = e * 5 * nb + i;
+    double w = v.cx * v.X[g];
+    if (v.Y) w = fma(v.cy, v.Y[g], w);
+    if (v.Z) w = fma(v.cz, v.Z[g], w);
+    acc[0] = fma(w, (F1[g] - F0[g]) * inv_mu1, acc[0]);
+    acc[1 + i / nb] += w;
+  }
+  for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] = acc[k];
+  __syncthreads();
+  for (int wdt = blockDim.x / 2; wdt > 0; wdt >>= 1) {
+    if (tid < wdt)
+      for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] += red[k][tid + wdt];
+    __syncthreads();
+  }
+  if (tid < DGB_NDPARAMS) part[e * DGB_NDPARAMS + tid] = red[tid][0];
+}
+
+// dpar[k] += sum_e part[e][k], fixed order
+__global__ void param_reduce_kernel(long E, const double* __restrict__ part, double* dpar)
+{
+  __shared__ double red[DGB_NDPARAMS][256];
+  const int tid = threadIdx.x;
+  double acc[DGB_NDPARAMS] = {0., 0., 0., 0., 0., 0.};
+  for (long e = tid; e < E; e += blockDim.x)
+    for (int k = 0; k < DGB_NDPARAMS; ++k) acc[k] += part[e * DGB_NDPARAMS + k];
+  for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] = acc[k];
+  __syncthreads();
+  for (int wdt = blockDim.x / 2; wdt > 0; wdt >>= 1) {
+    if (tid < wdt)
+      for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] += red[k][tid + wdt];
+    __syncthreads();
+  }
+  if (tid < DGB_NDPARAMS) dpar[tid] += red[tid][0];
+}
+
+// d_pg: F1 [n], F0 [n], FP64 traces [E][60][NQF], partials [E][DGB_NDPARAMS],
+// the host entry point's device copy of dJ/dparams [DGB_NDPARAMS]
+size_t pgrad_doubles(const dgb_handle* h)
+{
+  return 2 * (size_t)h->n + (size_t)h->E * 60 * h->NQF + (size_t)h->E * DGB_NDPARAMS + DGB_NDPARAMS;
+}
+
+int ensure_pgrad(dgb_handle* h)
+{
+  if (h->d_pg) return DGB_OK;
+  CK(cudaMalloc(&h->d_pg, sizeof(double) * pgrad_doubles(h)));
+  return DGB_OK;
+}
+
+// W^T df/dtheta for one residual VJP v (before it runs: it may overwrite
+// v.Y in place), added into dpar.  f is affine in mu (the viscous flux and
+// the heat flux at fixed Pr are linear in it), so df/dmu = (f(mu1) - f(0)) /
+// mu1, both FP64 residuals of v.U; df/dsource[r] = 1 on variable r.
+int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar)
+{
+  KLaunch L = klaunch(h);
+  L.precision = DGB_FP64;
+  L.ops = L.opsd;
+  KLaunch L1 = L, L0 = L;
+  const double mu1 = h->dprm.mu != 0. ? h->dprm.mu : 1.;
+  if (h->dprm.mu == 0.) {
+    dgb_params p1 = h->prm;
+    p1.mu = mu1;
+    L1.prm = device_params(p1, h->prandtl);
+  }
+  L0.prm.mu = 0.;
+  L0.prm.kq = 0.;
+  double* F1 = h->d_pg;
+  double* F0 = F1 + h->n;
+  double* trp = F0 + h->n;
+  double* part = trp + (size_t)h->E * 60 * h->NQF;
+  const KLaunch* Ls[2] = {&L1, &L0};
+  double* Fs[2] = {F1, F0};
+  for (int k = 0; k < 2; ++k) {
+    CK(launch_trace(*Ls[k], v.U, trp, h->stream));
+    StageArgs a = stage_args(MODE_RESIDUAL, 0.);
+    a.fout = Fs[k];
+    a.flag = h->d_flag;
+    CK(launch_stage(*Ls[k], v.U, trp, a, h->stream));
+  }
+  param_dot_kernel<<<(unsigned)h->E, 128, 0, h->stream>>>(h->E, h->NB, v, F1, F0, 1. / mu1, part);
+  CK(cudaGetLastError());
+  param_reduce_kernel<<<1, 256, 0, h->stream>>>(h->E, part, dpar);
+  CK(cudaGetLastError());
+  return DGB_OK;
+}
+
 // Reverse of one RK step from U_i (device, unchanged) with lam = adjoint of
 // U_{i+1} in, adjoint of U_i out (in place).  The stage states are recomputed
 // in the handle's precision, then one residual VJP per stage runs backwards.
@@ -80,7 +179,7 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
 // With `stored` (the recorded stage states of this step) nothing is
 // recomputed: an FP64 handle takes the traces of the stored states.
 int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl,
-                         double* const* stored = nullptr)
+                         double* const* stored = nullptr, double* dpar = nullptr)
 {
   const KLaunch L = klaunch(h);
   double* S[3] = {h->d_adj[dgb_handle::ADJ_S0], h->d_adj[dgb_handle::ADJ_S1], h->d_adj[dgb_handle::ADJ_S2]};
@@ -119,6 +218,15 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     if (!f64) return nullptr;
     return (const double*)(s < 0 ? TU : tout_f64[s]);
   };
+  int rc;
+  auto run_vjp = [&](const VjpArgs& w) -> int {
+    if (dpar) {
+      const int r = enqueue_param_terms(h, w, dpar);
+      if (r) return r;
+    }
+    CK(launch_residual_vjp(L, w, sc, h->stream));
+    return DGB_OK;
+  };
   VjpArgs v{};
   if (scheme == DGB_RK4) {
     v = vjp(S[2], dt / 6., lam);
@@ -126,19 +234,19 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     v.a_out = A0;
     v.acc_in = lam;
     v.acc_out = ACC;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if ((rc = run_vjp(v))) return rc;
     v = vjp(S[1], dt / 3., lam, dt, A0);
     v.Tr = tr(1);
     v.a_out = A0;
     v.acc_in = ACC;
     v.acc_out = ACC;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if ((rc = run_vjp(v))) return rc;
     v = vjp(S[0], dt / 3., lam, dt / 2., A0);
     v.Tr = tr(0);
     v.a_out = A0;
     v.acc_in = ACC;
     v.acc_out = ACC;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if ((rc = run_vjp(v))) return rc;
     v = vjp(Ui, dt / 6., lam, dt / 2., A0);
   } else {
     v = vjp(S[1], 2. * dt / 3., lam);
@@ -146,20 +254,20 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     v.a_out = A0;
     v.acc_in = lam;
     v.acc_out = ACC;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if ((rc = run_vjp(v))) return rc;
     v = vjp(S[0], dt / 6., lam, dt / 4., A0);
     v.Tr = tr(0);
     v.a_out = A1;
     v.acc_in = ACC;
     v.acc_out = ACC;
-    CK(launch_residual_vjp(L, v, sc, h->stream));
+    if ((rc = run_vjp(v))) return rc;
     v = vjp(Ui, dt / 6., lam, dt / 4., A0, dt, A1);
   }
   v.Tr = tr(-1);
   v.acc_in = ACC;
   v.acc_out = lam;
-  CK(launch_residual_vjp(L, v, sc, h->stream));
-  if (nl) *nl += (stored && !f64 ? 0 : 1 + nst) + (nst + 1) * (f64 ? 2 : 3);
+  if ((rc = run_vjp(v))) return rc;
+  if (nl) *nl += (stored && !f64 ? 0 : 1 + nst) + (nst + 1) * ((f64 ? 2 : 3) + (dpar ? 6 : 0));
   return DGB_OK;
 }
 
@@ -225,6 +333,8 @@ void dgb::free_adjoint(dgb_handle* h)
   if (h->d_adj_tr) cudaFree(h->d_adj_tr);
   if (h->d_adj_ta) cudaFree(h->d_adj_ta);
   h->d_adj_tr = h->d_adj_ta = nullptr;
+  if (h->d_pg) cudaFree(h->d_pg);
+  h->d_pg = nullptr;
   for (double* p : h->d_slots)
     if (p) cudaFree(p);
   h->d_slots.clear();
@@ -440,11 +550,22 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
   return DGB_OK;
 }
 
-int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
+}  // extern "C"
+
+namespace {
+
+// the backward sweep of dgb_backward_device; with dpar (device,
+// DGB_NDPARAMS doubles, zeroed here) also the parameter gradient
+int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, double* dpar)
 {
   if (!h || !lamN_dev || !lam0_dev) return fail(DGB_ERR_ARG, "null argument");
   if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
   CK(cudaSetDevice(h->device));
+  if (dpar) {
+    const int rc = ensure_pgrad(h);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(dpar, 0, sizeof(double) * DGB_NDPARAMS, h->stream));
+  }
   if (h->rec_stages) {  // every state and stage state was kept: reverse only
     const int nst = h->rec_scheme == DGB_RK4 ? 4 : 3;
     double* lam = h->d_adj[dgb_handle::ADJ_LAM];
@@ -455,7 +576,8 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
     for (unsigned long long k = h->rec_steps; k-- > 0;) {
       double* Si = h->d_stage_store + (size_t)k * (nst - 1) * (size_t)h->n;
       double* stored[3] = {Si, Si + (size_t)h->n, nst > 3 ? Si + 2 * (size_t)h->n : nullptr};
-      if ((rc = enqueue_reverse_step(h, h->rec_scheme, h->rec_dt, h->d_slots[k], lam, &nl, stored))) return rc;
+      if ((rc = enqueue_reverse_step(h, h->rec_scheme, h->rec_dt, h->d_slots[k], lam, &nl, stored, dpar)))
+        return rc;
     }
     if ((rc = copy_state(h, lam0_dev, lam))) return rc;
     h->last_launches = nl;
@@ -497,8 +619,12 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
     const CkOp& op = h->plan.ops[k];
     switch (op.kind) {
       case CK_REVERSE:
-        CK(cudaGraphLaunch(h->rev_graph, h->stream));
-        nl += h->rev_launches;
+        if (dpar) {  // the captured reverse step has no parameter terms
+          if ((rc = enqueue_reverse_step(h, scheme, dt, h->d_U, lam, &nl, nullptr, dpar))) return rc;
+        } else {
+          CK(cudaGraphLaunch(h->rev_graph, h->stream));
+          nl += h->rev_launches;
+        }
         ++rev;
         break;
       case CK_RESTORE:
@@ -523,6 +649,40 @@ int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
   h->adj_forward_steps = fwd;
   h->adj_reverse_steps = rev;
   return read_flag(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgb_backward_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev)
+{
+  return backward_impl(h, lamN_dev, lam0_dev, nullptr);
+}
+
+int dgb_backward_params_device(dgb_handle* h, const double* lamN_dev, double* lam0_dev, double* dpar_dev)
+{
+  if (!dpar_dev) return fail(DGB_ERR_ARG, "null argument");
+  return backward_impl(h, lamN_dev, lam0_dev, dpar_dev);
+}
+
+int dgb_backward_params(dgb_handle* h, const double* lamN_host, double* lam0_host, double* dpar_host)
+{
+  if (!h || !lamN_host || !lam0_host || !dpar_host) return fail(DGB_ERR_ARG, "null argument");
+  if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_pgrad(h);
+  if (rc) return rc;
+  const size_t sb = sizeof(double) * (size_t)h->n;
+  double* in = h->d_adj[dgb_handle::ADJ_IN];
+  double* out = h->d_adj[dgb_handle::ADJ_OUT];
+  double* dpar = h->d_pg + pgrad_doubles(h) - DGB_NDPARAMS;
+  CK(cudaMemcpyAsync(in, lamN_host, sb, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = backward_impl(h, in, out, dpar))) return rc;
+  CK(cudaMemcpyAsync(lam0_host, out, sb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(dpar_host, dpar, sizeof(double) * DGB_NDPARAMS, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
 }
 
 int dgb_backward(dgb_handle* h, const double* lamN_host, double* lam0_host)

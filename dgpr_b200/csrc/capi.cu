@@ -115,6 +115,45 @@ void free_all(dgb_handle* h)
 
 int dgb::set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 
+DevParams dgb::device_params(const dgb_params& p, double prandtl)
+{
+  DevParams d{};
+  d.gamma = p.gamma;
+  d.R = p.R;
+  d.mu = p.mu;
+  d.P = p.P;
+  d.eta = p.eta;
+  total_conditions(p, &d.Tt, &d.Pt);
+  for (int r = 0; r < 5; ++r) {
+    d.Ufr[r] = p.Ufr[r];
+    d.src[r] = p.source[r];
+  }
+  d.kq = (prandtl == 0. || std::isinf(prandtl)) ? 0. : p.mu * p.gamma / prandtl;
+  return d;
+}
+
+namespace {
+
+// a new DevParams for the handle: captured graphs hold the kernel parameters
+// by value, and a recorded forward run was made with the old ones
+int replace_device_params(dgb_handle* h, const DevParams& d)
+{
+  if (!std::memcmp(&d, &h->dprm, sizeof d)) return DGB_OK;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->dprm = d;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_scheme = -1;
+  if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
+  h->rev_graph = nullptr;
+  h->rev_scheme = -1;
+  h->recorded = false;
+  return DGB_OK;
+}
+
+}  // namespace
+
 // The captured graph of one step for (scheme, dt), with room for `cap` norms.
 int dgb::ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap)
 {
@@ -212,16 +251,7 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
     delete h;
     return fail(rc, why);
   }
-  h->dprm.gamma = params->gamma;
-  h->dprm.R = params->R;
-  h->dprm.mu = params->mu;
-  h->dprm.P = params->P;
-  h->dprm.eta = params->eta;
-  total_conditions(*params, &h->dprm.Tt, &h->dprm.Pt);
-  for (int r = 0; r < 5; ++r) {
-    h->dprm.Ufr[r] = params->Ufr[r];
-    h->dprm.src[r] = params->source[r];
-  }
+  h->dprm = device_params(*params, 0.);
 
   cudaError_t e = cudaGetDevice(&h->device);
   if (e != cudaSuccess) {
@@ -312,20 +342,17 @@ int dgb_set_prandtl(dgb_handle* h, double prandtl)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
   if (!(prandtl >= 0.)) return fail(DGB_ERR_ARG, "Prandtl number must be >= 0 (0: no heat flux)");
-  const double kq = (prandtl == 0. || std::isinf(prandtl)) ? 0. : h->dprm.mu * h->dprm.gamma / prandtl;
-  if (kq == h->dprm.kq) return DGB_OK;
-  CK(cudaSetDevice(h->device));
-  CK(cudaStreamSynchronize(h->stream));
-  h->dprm.kq = kq;
-  // captured graphs hold the kernel parameters by value; a recorded forward
-  // run was made with the old physics
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  h->graph = nullptr;
-  h->graph_scheme = -1;
-  if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
-  h->rev_graph = nullptr;
-  h->recorded = false;
-  return DGB_OK;
+  const int rc = replace_device_params(h, device_params(h->prm, prandtl));
+  if (rc == DGB_OK) h->prandtl = prandtl;
+  return rc;
+}
+
+int dgb_set_params(dgb_handle* h, const dgb_params* params)
+{
+  if (!h || !params) return fail(DGB_ERR_ARG, "null argument");
+  const int rc = replace_device_params(h, device_params(*params, h->prandtl));
+  if (rc == DGB_OK) h->prm = *params;
+  return rc;
 }
 
 int dgb_synchronize(dgb_handle* h)

@@ -116,6 +116,13 @@ int dgb_synchronize(dgb_handle* h);
  * (dgb_forward_record), which used the old physics. */
 int dgb_set_prandtl(dgb_handle* h, double prandtl);
 
+/* Replaces the physical parameters given to dgb_create (gamma, R, mu, the
+ * reference state, source, eta) on an existing handle; the mesh, geometry,
+ * state and Prandtl number stay.  Lets a caller vary viscosity or forcing
+ * (e.g. with dgb_backward_params) without rebuilding the geometry.  Discards
+ * captured step graphs and any recorded forward run. */
+int dgb_set_params(dgb_handle* h, const dgb_params* params);
+
 /* Number of doubles in one state array: nx*ny*nz * 5 * (p+1)^3. */
 long long dgb_state_size(const dgb_handle* h);
 
@@ -235,6 +242,23 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
  * overwritten checkpoints the next one first recomputes them from U_0. */
 int dgb_backward(dgb_handle* h, const double* dJdUN_host, double* dJdU0_host);
 int dgb_backward_device(dgb_handle* h, const double* dJdUN_dev, double* dJdU0_dev);
+
+/* Parameters the backward sweep can differentiate: dJdparams[DGB_DPARAM_MU]
+ * = dJ/dmu (dynamic viscosity, at a fixed Prandtl number: the heat flux
+ * scales with mu) and dJdparams[DGB_DPARAM_SOURCE + r] = dJ/dsource[r]. */
+enum { DGB_DPARAM_MU = 0, DGB_DPARAM_SOURCE = 1, DGB_NDPARAMS = 6 };
+
+/* dgb_backward plus the gradient of J with respect to the parameters above
+ * over the recorded run, into dJdparams[DGB_NDPARAMS] (host).  Each residual
+ * is affine in mu, so df/dmu = (f(mu1) - f(0)) / mu1 (mu1 = mu, or 1 for an
+ * inviscid handle), two FP64 residuals per stage; df/dsource[r] = 1 at every
+ * node of variable r (the source is tested with the mass matrix's
+ * quadrature).  About twice the cost of dgb_backward.  The reference has no
+ * counterpart (it has no adjoint). */
+int dgb_backward_params(dgb_handle* h, const double* dJdUN_host, double* dJdU0_host, double* dJdparams_host);
+/* Same on device arrays; dJdparams_dev (DGB_NDPARAMS doubles) is overwritten. */
+int dgb_backward_params_device(dgb_handle* h, const double* dJdUN_dev, double* dJdU0_dev,
+                               double* dJdparams_dev);
 
 /* Steps recomputed and reversed by the last backward sweep, and the forward
  * steps of the whole checkpoint plan (recorded run included). */
