@@ -18,13 +18,15 @@ LIB_PATH = os.environ.get("DGB200_LIB") or os.path.join(HERE, "_lib", "libdgb200
 OK, ERR_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_GEOMETRY, ERR_NONFINITE, ERR_IO, ERR_BOUNDARY = range(8)
 INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW, NO_SLIP_WALL = \
     -1, -2, -3, -4, -5, -6, -7
+ISOTHERMAL_WALL = -8  # an extension: no-slip wall at Solver.set_wall_temperature (default: params T)
 RK4, TVDRK3 = 0, 1
 FP64, MIXED_FP32 = 0, 1
-DPARAM_MU, DPARAM_SOURCE, NDPARAMS = 0, 1, 6  # dgb_backward_params: dJ/d[mu, source[0..4]]
+DPARAM_MU, DPARAM_SOURCE, DPARAM_TWALL, NDPARAMS = 0, 1, 6, 7  # dgb_backward_params: dJ/d[mu, source[0..4], Tw]
 
 BOUNDARY_TYPES = {  # the reference's boundary_types map (boundaries.cpp:37-44)
     "periodic": PERIODIC, "freestream": FREESTREAM, "inviscid_wall": INVISCID_WALL,
     "subsonic_inflow": SUBSONIC_INFLOW, "subsonic_outflow": SUBSONIC_OUTFLOW, "no_slip_wall": NO_SLIP_WALL,
+    "isothermal_wall": ISOTHERMAL_WALL,
 }
 TIME_SCHEMES = {"RK4": RK4, "tvdRK3": TVDRK3}  # multistage_schemes (time.cpp:29-31)
 
@@ -111,6 +113,7 @@ def lib():
             "dgb_backward_params": (ctypes.c_int, [vp, _dp, _dp, _dp]),
             "dgb_backward_params_device": (ctypes.c_int, [vp, vp, vp, vp]),
             "dgb_set_params": (ctypes.c_int, [vp, ctypes.POINTER(Params)]),
+            "dgb_set_wall_temperature": (ctypes.c_int, [vp, ctypes.c_double]),
             "dgb_adjoint_stats": (ctypes.c_int, [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3),
             "dgb_checkpoint_plan": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong,
@@ -412,7 +415,7 @@ class Solver:
         _check(lib().dgb_backward_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr)))
 
     def backward_params(self, lamN):
-        """(dJ/dU_0, dJ/d[mu, source[0..4]]) for J with dJ/dU_N = lamN."""
+        """(dJ/dU_0, dJ/d[mu, source[0..4], Tw]) for J with dJ/dU_N = lamN."""
         lamN = np.ascontiguousarray(lamN, dtype=np.float64).ravel()
         out = np.zeros(self.n)
         dpar = np.zeros(NDPARAMS)
@@ -422,6 +425,10 @@ class Solver:
     def backward_params_device(self, lamN_ptr, out_ptr, dpar_ptr):
         _check(lib().dgb_backward_params_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr),
                                                 ctypes.c_void_p(dpar_ptr)))
+
+    def set_wall_temperature(self, Tw):
+        """Temperature of the isothermal walls (> 0); drops the recorded run."""
+        _check(lib().dgb_set_wall_temperature(self.h, float(Tw)))
 
     def set_params(self, params):
         """New physical parameters (Params or its 17-vector) for this handle;

@@ -4,8 +4,9 @@
 (torch float64 CUDA tensor in the reference layout U[e][r][b]) by nsteps RK
 steps through dgb_forward_record; its backward is dgb_backward_device, the
 hand-written discrete adjoint with binomial checkpointing.  With
-`theta` = [mu, source[0..4]] (a float64 tensor of 6) the run uses those
-parameters (dgb_set_params) and is differentiable in them too
+`theta` = [mu, source[0..4]] or [mu, source[0..4], Tw] (a float64 tensor of
+6 or 7; Tw: the isothermal walls' temperature) the run uses those parameters
+(dgb_set_params, dgb_set_wall_temperature) and is differentiable in them too
 (dgb_backward_params_device).  `residual(U,
 solver)` is f = -Minv R(U) with dgb_residual_vjp_device as its backward.
 
@@ -65,13 +66,15 @@ class _IntegrateParams(torch.autograd.Function):
     def forward(ctx, U0, theta, solver, scheme, dt, nsteps, slots):
         from . import Params
         th = [float(v) for v in theta.detach().cpu().reshape(-1)]
-        if len(th) != 6:
-            raise ValueError("theta must hold [mu, source[0..4]]")
+        if len(th) not in (6, 7):
+            raise ValueError("theta must hold [mu, source[0..4]] or [mu, source[0..4], Tw]")
         p = Params.from_array(solver.params.as_array())
         p.mu = th[0]
         for r in range(5):
             p.source[r] = th[1 + r]
         solver.set_params(p)
+        if len(th) == 7:
+            solver.set_wall_temperature(th[6])
         UN = _Integrate.forward(ctx, U0, solver, scheme, dt, nsteps, slots)
         ctx.theta_like = theta
         return UN
@@ -84,10 +87,11 @@ class _IntegrateParams(torch.autograd.Function):
         gUN = _dev_f64(gUN, solver.n, "grad")
         torch.cuda.current_stream().synchronize()
         g0 = torch.empty_like(gUN)
-        dpar = torch.empty(6, dtype=torch.float64, device=gUN.device)
+        dpar = torch.empty(7, dtype=torch.float64, device=gUN.device)
         solver.backward_params_device(gUN.data_ptr(), g0.data_ptr(), dpar.data_ptr())
         solver.synchronize()
-        gth = dpar.to(device=ctx.theta_like.device, dtype=ctx.theta_like.dtype).reshape(ctx.theta_like.shape)
+        k = ctx.theta_like.numel()
+        gth = dpar[:k].to(device=ctx.theta_like.device, dtype=ctx.theta_like.dtype).reshape(ctx.theta_like.shape)
         return g0, gth, None, None, None, None, None
 
 
@@ -119,7 +123,8 @@ def integrate(U0, solver, scheme, dt, nsteps, slots=None, theta=None):
     """U_N after nsteps RK steps from U0, differentiable in U0.  slots: number
     of state checkpoints held on the device (default: every state), or STAGES
     to keep every stage state as well.  theta: optional float64 tensor
-    [mu, source[0..4]] of the run's parameters, then also differentiable."""
+    [mu, source[0..4]] or [mu, source[0..4], Tw] of the run's parameters,
+    then also differentiable."""
     slots = int(slots if slots is not None else nsteps)
     if theta is None:
         return _Integrate.apply(U0, solver, int(scheme), float(dt), int(nsteps), slots)

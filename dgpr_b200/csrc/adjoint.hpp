@@ -28,7 +28,8 @@ struct VjpArgs {
 // per-handle scratch of a VJP
 struct VjpScratch {
   double* trace;  // FP64 face traces [E][6][10][P*P]
-  double* ta;     // face-trace adjoints [E][6][20][P*P]
+  double* ta;     // face-trace adjoints [E][6][20][P*P]; an isothermal-wall face keeps its points'
+                  // dJ/dTw terms in [10][P*P]
   double* part;   // volume part of a, [E][5][P^3]
   int* flag;      // bit 3: a boundary type without an adjoint
 };

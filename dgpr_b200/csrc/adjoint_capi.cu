@@ -70,7 +70,7 @@ __global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __rest
   __shared__ double red[DGB_NDPARAMS][128];
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
-  double acc[DGB_NDPARAMS] = {0., 0., 0., 0., 0., 0.};
+  double acc[DGB_NDPARAMS] = {};
   for (int i = tid; i < 5 * nb; i += blockDim.x) {
     const long g = e * 5 * nb + i;
     double w = v.cx * v.X[g];
@@ -89,12 +89,33 @@ __global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __rest
   if (tid < DGB_NDPARAMS) part[e * DGB_NDPARAMS + tid] = red[tid][0];
 }
 
+// dpar[0] += the isothermal-wall points' dJ/dTw terms, which adjA leaves in
+// ta[e][lf][10][NQF] of every face with nbr == -8; fixed order
+__global__ void wall_terms_kernel(long E, int nqf, const int* __restrict__ nbr, const double* __restrict__ ta,
+                                  double* dpar)
+{
+  __shared__ double red[256];
+  const int tid = threadIdx.x;
+  double acc = 0.;
+  for (long i = tid; i < E * 6 * nqf; i += blockDim.x) {
+    const long ef = i / nqf;
+    if (nbr[ef] == -8) acc += ta[(ef * 20 + 10) * nqf + i % nqf];
+  }
+  red[tid] = acc;
+  __syncthreads();
+  for (int wdt = blockDim.x / 2; wdt > 0; wdt >>= 1) {
+    if (tid < wdt) red[tid] += red[tid + wdt];
+    __syncthreads();
+  }
+  if (tid == 0) dpar[0] += red[0];
+}
+
 // dpar[k] += sum_e part[e][k], fixed order
 __global__ void param_reduce_kernel(long E, const double* __restrict__ part, double* dpar)
 {
   __shared__ double red[DGB_NDPARAMS][256];
   const int tid = threadIdx.x;
-  double acc[DGB_NDPARAMS] = {0., 0., 0., 0., 0., 0.};
+  double acc[DGB_NDPARAMS] = {};
   for (long e = tid; e < E; e += blockDim.x)
     for (int k = 0; k < DGB_NDPARAMS; ++k) acc[k] += part[e * DGB_NDPARAMS + k];
   for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] = acc[k];
@@ -135,7 +156,7 @@ int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar)
   if (h->dprm.mu == 0.) {
     dgb_params p1 = h->prm;
     p1.mu = mu1;
-    L1.prm = device_params(p1, h->prandtl);
+    L1.prm = device_params(p1, h->prandtl, h->twall);
   }
   L0.prm.mu = 0.;
   L0.prm.kq = 0.;
@@ -220,11 +241,17 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   };
   int rc;
   auto run_vjp = [&](const VjpArgs& w) -> int {
-    if (dpar) {
-      const int r = enqueue_param_terms(h, w, dpar);
-      if (r) return r;
+    if (!dpar) {
+      CK(launch_residual_vjp(L, w, sc, h->stream));
+      return DGB_OK;
     }
+    const int r = enqueue_param_terms(h, w, dpar);
+    if (r) return r;
     CK(launch_residual_vjp(L, w, sc, h->stream));
+    if (h->isothermal) {  // the VJP left the isothermal walls' dJ/dTw terms in its trace adjoints
+      wall_terms_kernel<<<1, 256, 0, h->stream>>>(h->E, h->NQF, h->d_nbr, sc.ta, dpar + DGB_DPARAM_TWALL);
+      CK(cudaGetLastError());
+    }
     return DGB_OK;
   };
   VjpArgs v{};

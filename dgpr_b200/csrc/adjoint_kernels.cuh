@@ -510,12 +510,15 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             Ubb[r] -= dbar[r];
           }
         }
+        // an isothermal wall point leaves its dJ/dTw term (Ub[4] = r R Tw / (gamma - 1)) in the
+        // first slot of the neighbour half of TA, which no element reads for a boundary face
+        const double wall_term = nb == -8 ? Ubb[4] * Uo[0] * (prm.R / (prm.gamma - 1.)) : 0.;
         if (boundary_state_vjp(nb, Uo, n, prm, Ubb, Uob) && flag) atomicOr(flag, 8);
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
           TAe[r * NQF + fq] = Uob[r];
           TAe[(5 + r) * NQF + fq] = Qob[r];
-          TAe[(10 + r) * NQF + fq] = 0.;
+          TAe[(10 + r) * NQF + fq] = r == 0 ? wall_term : 0.;
           TAe[(15 + r) * NQF + fq] = 0.;
         }
       }

@@ -115,7 +115,7 @@ void free_all(dgb_handle* h)
 
 int dgb::set_last_error(int code, const std::string& msg) { return fail(code, msg); }
 
-DevParams dgb::device_params(const dgb_params& p, double prandtl)
+DevParams dgb::device_params(const dgb_params& p, double prandtl, double twall)
 {
   DevParams d{};
   d.gamma = p.gamma;
@@ -129,6 +129,7 @@ DevParams dgb::device_params(const dgb_params& p, double prandtl)
     d.src[r] = p.source[r];
   }
   d.kq = (prandtl == 0. || std::isinf(prandtl)) ? 0. : p.mu * p.gamma / prandtl;
+  d.Tw = twall < 0. ? p.T : twall;
   return d;
 }
 
@@ -251,7 +252,8 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
     delete h;
     return fail(rc, why);
   }
-  h->dprm = device_params(*params, 0.);
+  h->dprm = device_params(*params, 0., -1.);
+  for (int s = 0; s < 6; ++s) h->isothermal = h->isothermal || mesh->bounds[s] == DGB_BT_ISOTHERMAL_WALL;
 
   cudaError_t e = cudaGetDevice(&h->device);
   if (e != cudaSuccess) {
@@ -342,15 +344,24 @@ int dgb_set_prandtl(dgb_handle* h, double prandtl)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
   if (!(prandtl >= 0.)) return fail(DGB_ERR_ARG, "Prandtl number must be >= 0 (0: no heat flux)");
-  const int rc = replace_device_params(h, device_params(h->prm, prandtl));
+  const int rc = replace_device_params(h, device_params(h->prm, prandtl, h->twall));
   if (rc == DGB_OK) h->prandtl = prandtl;
+  return rc;
+}
+
+int dgb_set_wall_temperature(dgb_handle* h, double Tw)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (!(Tw > 0.) || std::isinf(Tw)) return fail(DGB_ERR_ARG, "wall temperature must be finite and > 0");
+  const int rc = replace_device_params(h, device_params(h->prm, h->prandtl, Tw));
+  if (rc == DGB_OK) h->twall = Tw;
   return rc;
 }
 
 int dgb_set_params(dgb_handle* h, const dgb_params* params)
 {
   if (!h || !params) return fail(DGB_ERR_ARG, "null argument");
-  const int rc = replace_device_params(h, device_params(*params, h->prandtl));
+  const int rc = replace_device_params(h, device_params(*params, h->prandtl, h->twall));
   if (rc == DGB_OK) h->prm = *params;
   return rc;
 }

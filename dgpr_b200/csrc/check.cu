@@ -82,7 +82,7 @@ extern "C" int dgb_check_pointwise(int which, const double* x, const double* yba
       }
       return DGB_OK;
     }
-    case DGB_CHECK_BOUNDARY_STATE: {  // x = UL[5], aux = {btype, n[3], gamma, R, P, Pt, Tt, Ufr[5]}
+    case DGB_CHECK_BOUNDARY_STATE: {  // x = UL[5], aux = {btype, n[3], gamma, R, P, Pt, Tt, Ufr[5] (, Tw)}
       DevParams prm{};
       prm.gamma = aux[4];
       prm.R = aux[5];
@@ -91,6 +91,7 @@ extern "C" int dgb_check_pointwise(int which, const double* x, const double* yba
       prm.Tt = aux[8];
       for (int r = 0; r < 5; ++r) prm.Ufr[r] = aux[9 + r];
       const int bt = (int)aux[0];
+      if (bt == -8) prm.Tw = aux[14];
       if (boundary_state(bt, x, aux + 1, prm, y)) return DGB_ERR_BOUNDARY;
       if (xbar && ybar) {
         for (int i = 0; i < 5; ++i) xbar[i] = 0.;

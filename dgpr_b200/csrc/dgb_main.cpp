@@ -43,6 +43,7 @@ struct Inputs {
   bool turb = false;
   int precision = DGB_FP64;
   double prandtl = 0.;
+  double twall = -1.;  // isothermal walls' temperature (< 0: the reference temperature)
 };
 
 enum Kind { K_U64, K_DBL, K_STR, K_BOOL, K_BTYPE, K_SCHEME, K_PREC };
@@ -65,7 +66,8 @@ bool btype_of(const char* s, long long* out)
              {"inviscid_wall", DGB_BT_INVISCID_WALL},
              {"subsonic_inflow", DGB_BT_SUBSONIC_INFLOW},
              {"subsonic_outflow", DGB_BT_SUBSONIC_OUTFLOW},
-             {"no_slip_wall", DGB_BT_NO_SLIP_WALL}};
+             {"no_slip_wall", DGB_BT_NO_SLIP_WALL},
+             {"isothermal_wall", DGB_BT_ISOTHERMAL_WALL}};  // an extension (-twall)
   for (const auto& m : map)
     if (!strcmp(s, m.n)) {
       *out = m.v;
@@ -119,6 +121,7 @@ int parse(int argc, char** argv, Inputs& in)
       {"ifile", "input file prefix", K_STR, &in.ifile},
       {"precision", "arithmetic: fp64 or mixed", K_PREC, &in.precision},
       {"prandtl", "Prandtl number of the heat flux (0: none)", K_DBL, &in.prandtl},
+      {"twall", "temperature of isothermal_wall sides (default: reference T)", K_DBL, &in.twall},
   };
   const int nopt = (int)(sizeof opts / sizeof opts[0]);
   if (argc > 1 && !strcmp(argv[1], "-h")) {
@@ -297,6 +300,7 @@ int main(int argc, char** argv)
   dgb_handle* h = nullptr;
   if ((rc = dgb_create(&mesh, &prm, in.precision, &h))) die("dgb_create", rc);
   if ((rc = dgb_set_prandtl(h, in.prandtl))) die("dgb_set_prandtl", rc);
+  if (in.twall > 0. && (rc = dgb_set_wall_temperature(h, in.twall))) die("dgb_set_wall_temperature", rc);
   if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
 
   // running mean (dg.cpp:123-131): an input file may carry one to continue

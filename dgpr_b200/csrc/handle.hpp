@@ -25,6 +25,8 @@ struct dgb_handle {
   dgb_params prm{};
   dgb::DevParams dprm{};
   double prandtl = 0.;  // heat flux off (0) or its Prandtl number (dgb_set_prandtl)
+  double twall = -1.;   // isothermal-wall temperature (dgb_set_wall_temperature); < 0: the parameters' T
+  bool isothermal = false;  // the mesh has isothermal-wall sides
   dgb::Ops1D ops;
   double* d_ops = nullptr;
   float* d_opsf = nullptr;    // operator table for the mixed form
@@ -62,7 +64,7 @@ struct dgb_handle {
   double* d_adj[ADJ_NBUF] = {};
   double* d_adj_tr = nullptr;  // FP64 face traces [E][6][10][NQF]
   double* d_adj_ta = nullptr;  // face-trace adjoints [E][6][20][NQF]
-  double* d_pg = nullptr;      // parameter gradient: residuals F1, F0 [n], partials [E][DGB_NDPARAMS]
+  double* d_pg = nullptr;      // parameter gradient scratch (adjoint_capi.cu, pgrad_doubles)
   std::vector<double*> d_slots;  // checkpoints
   double* d_stage_store = nullptr;  // recorded stage states [nsteps][stages - 1][n] (dgb_forward_record_stages)
   size_t stage_store_cap = 0;       // doubles
@@ -116,8 +118,8 @@ inline int cuda_status(cudaError_t e, const char* what)
 
 void free_adjoint(dgb_handle* h);
 // DevParams of the reference parameters, with the heat flux of Prandtl number
-// `prandtl` (0: none)
-DevParams device_params(const dgb_params& p, double prandtl);
+// `prandtl` (0: none) and isothermal walls at `twall` (< 0: p.T)
+DevParams device_params(const dgb_params& p, double prandtl, double twall);
 int ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap);
 int enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace);
 

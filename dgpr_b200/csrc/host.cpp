@@ -323,8 +323,8 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     return DGB_ERR_ARG;
   }
   for (int s = 0; s < 6; ++s)
-    if (m.bounds[s] > -2 || m.bounds[s] < -7) {
-      why = "boundary codes must be btype values -2..-7";
+    if (m.bounds[s] > -2 || m.bounds[s] < -8) {
+      why = "boundary codes must be btype values -2..-7 (or -8, the isothermal wall)";
       return DGB_ERR_ARG;
     }
   for (int a = 0; a < 3; ++a)

@@ -132,6 +132,7 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   L.prm.mu = params->mu;
   L.prm.P = params->P;
   L.prm.eta = params->eta;
+  L.prm.Tw = params->T;  // isothermal walls at the reference temperature
   total_conditions(*params, &L.prm.Tt, &L.prm.Pt);
   for (int r = 0; r < 5; ++r) {
     L.prm.Ufr[r] = params->Ufr[r];

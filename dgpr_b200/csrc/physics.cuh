@@ -17,6 +17,7 @@ namespace dgb {
 struct DevParams {
   double gamma, R, mu, P, Pt, Tt, eta;
   double kq;  // heat-flux coefficient mu gamma / Pr (0: no heat conduction, the reference's physics)
+  double Tw;  // temperature of isothermal walls (btype -8, an extension)
   double Ufr[5];
   double src[5];
 };
@@ -209,8 +210,9 @@ DGB_HD void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
 }
 
 // Ghost state for a boundary face (bound_states.cpp:24-130, selected as in
-// solve.cpp:235-252).  Returns 1 when subsonic inflow has no non-negative
-// boundary Mach root (the reference aborts there on the host, :80-83).
+// solve.cpp:235-252), plus the isothermal wall -8 the reference lacks.
+// Returns 1 when subsonic inflow has no non-negative boundary Mach root (the
+// reference aborts there on the host, :80-83).
 template <class T>
 DGB_HD int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm, T* Ub)
 {
@@ -228,6 +230,14 @@ DGB_HD int boundary_state(int bt, const T* UL, const T* n, const DevParams& prm,
     Ub[2] = UL[0] * (v - vn * n[1]);
     Ub[3] = UL[0] * (w - vn * n[2]);
     Ub[4] = UL[4];
+    return 0;
+  }
+  if (bt == -8) {  // isothermal no-slip wall (an extension): zero velocity, interior density, wall temperature
+    Ub[0] = UL[0];
+    Ub[1] = T(0);
+    Ub[2] = T(0);
+    Ub[3] = T(0);
+    Ub[4] = UL[0] * T(prm.R) * T(prm.Tw) / gm1;
     return 0;
   }
   if (bt == -7) {  // no-slip wall: zero velocity, interior total energy

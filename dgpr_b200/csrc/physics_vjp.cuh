@@ -465,6 +465,10 @@ DGB_HD int boundary_state_vjp(int bt, const T* UL, const T* n, const DevParams& 
     ULbar[4] += Ubbar[4];
     return 0;
   }
+  if (bt == -8) {  // Ub = (r, 0, 0, 0, r R Tw / (gamma - 1))
+    ULbar[0] += Ubbar[0] + Ubbar[4] * T(prm.R) * T(prm.Tw) / (T(prm.gamma) - T(1));
+    return 0;
+  }
   if (bt != -5 && bt != -6) return 1;
 
   // forward quantities shared by inflow and outflow

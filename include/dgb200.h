@@ -42,7 +42,12 @@ enum {
   DGB_BT_INVISCID_WALL = -4,
   DGB_BT_SUBSONIC_INFLOW = -5,
   DGB_BT_SUBSONIC_OUTFLOW = -6,
-  DGB_BT_NO_SLIP_WALL = -7
+  DGB_BT_NO_SLIP_WALL = -7,
+  /* An extension the reference lacks (its no-slip wall keeps the interior
+   * energy, bound_states.cpp:42-49): a no-slip wall at the temperature set by
+   * dgb_set_wall_temperature (default: the reference temperature T).  Ghost
+   * state: interior density, zero velocity, E = rho R Tw / (gamma - 1). */
+  DGB_BT_ISOTHERMAL_WALL = -8
 };
 
 /* time schemes, same order as the reference's time_scheme enum (time.cpp:23-27) */
@@ -122,6 +127,11 @@ int dgb_set_prandtl(dgb_handle* h, double prandtl);
  * (e.g. with dgb_backward_params) without rebuilding the geometry.  Discards
  * captured step graphs and any recorded forward run. */
 int dgb_set_params(dgb_handle* h, const dgb_params* params);
+
+/* Temperature of the isothermal walls (DGB_BT_ISOTHERMAL_WALL), > 0; until
+ * set it is the parameters' reference temperature T.  Discards captured
+ * graphs and any recorded forward run. */
+int dgb_set_wall_temperature(dgb_handle* h, double Tw);
 
 /* Number of doubles in one state array: nx*ny*nz * 5 * (p+1)^3. */
 long long dgb_state_size(const dgb_handle* h);
@@ -245,8 +255,10 @@ int dgb_backward_device(dgb_handle* h, const double* dJdUN_dev, double* dJdU0_de
 
 /* Parameters the backward sweep can differentiate: dJdparams[DGB_DPARAM_MU]
  * = dJ/dmu (dynamic viscosity, at a fixed Prandtl number: the heat flux
- * scales with mu) and dJdparams[DGB_DPARAM_SOURCE + r] = dJ/dsource[r]. */
-enum { DGB_DPARAM_MU = 0, DGB_DPARAM_SOURCE = 1, DGB_NDPARAMS = 6 };
+ * scales with mu), dJdparams[DGB_DPARAM_SOURCE + r] = dJ/dsource[r] and
+ * dJdparams[DGB_DPARAM_TWALL] = dJ/dTw, the isothermal walls' temperature
+ * (0 on a mesh without them). */
+enum { DGB_DPARAM_MU = 0, DGB_DPARAM_SOURCE = 1, DGB_DPARAM_TWALL = 6, DGB_NDPARAMS = 7 };
 
 /* dgb_backward plus the gradient of J with respect to the parameters above
  * over the recorded run, into dJdparams[DGB_NDPARAMS] (host).  Each residual

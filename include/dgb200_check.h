@@ -17,7 +17,8 @@ enum {
   DGB_CHECK_VISC_JUMP_N = 4,     /* x = S[5], d[5];    aux = {mu, n[3]};    y = A(S, d n^T).n[5] */
   DGB_CHECK_ROE = 5,             /* x = Ul[5], Ur[5];  aux = {gamma, n[3]}; y = Roe flux[5] (flux.cpp:56-154) */
   DGB_CHECK_BOUNDARY_STATE = 6,  /* x = UL[5]; aux = {btype, n[3], gamma, R, P, Pt, Tt, Ufr[5]}; y = Ub[5]
-                                    (bound_states.cpp:24-130); reverse mode for btype -3 .. -7 */
+                                    (bound_states.cpp:24-130); reverse mode for btype -3 .. -8;
+                                    btype -8 (isothermal wall) reads Tw from aux[14] */
   /* The viscous forms 2-4 with the optional heat flux kq = mu gamma / Pr
    * in the energy row (an extension: the reference conducts no heat). */
   DGB_CHECK_VISC_FLUX_HEAT = 7,    /* x as 2; aux = {mu, kq} */

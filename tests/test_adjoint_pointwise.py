@@ -105,10 +105,11 @@ def test_roe_vjp(seed):
     fd_check(5, np.concatenate([UL, UR]), [1.4, *unit(rng)], rng, h=1e-7, tol=2e-6)
 
 
-@pytest.mark.parametrize("bt", [-3, -4, -7])
+@pytest.mark.parametrize("bt", [-3, -4, -7, -8])
 def test_wall_and_freestream_state_vjp(bt):
+    """-8: the isothermal wall (an extension), wall temperature in aux[14]."""
     rng = np.random.default_rng(17)
-    aux = [bt, *unit(rng), 1.4, 287.0, 0.7, 0.9, 0.003, 1.0, 0.1, 0.0, 0.0, 1.8]
+    aux = [bt, *unit(rng), 1.4, 287.0, 0.7, 0.9, 0.003, 1.0, 0.1, 0.0, 0.0, 1.8, 0.0021]
     for _ in range(4):
         fd_check(6, state(rng), aux, rng)
 
@@ -229,3 +230,15 @@ def test_zero_heat_flux_is_the_plain_flux_bit_for_bit():
         n = unit(rng)
         assert np.array_equal(call(8, x, [0.02, *n, 0.0])[0], call(3, x, [0.02, *n])[0])
         assert np.array_equal(call(9, x, [0.02, *n, 0.0])[0], call(4, x, [0.02, *n])[0])
+
+
+def test_isothermal_wall_ghost_state():
+    """Interior density, zero velocity, temperature Tw: p_b = rho R Tw."""
+    rng = np.random.default_rng(18)
+    g, R, Tw = 1.4, 287.0, 0.0021
+    for _ in range(5):
+        UL = state(rng)
+        aux = [-8, *unit(rng), g, R, 0.7, 0.9, 0.003, 1.0, 0.1, 0.0, 0.0, 1.8, Tw]
+        Ub, _ = call(6, UL, aux)
+        assert Ub[0] == UL[0] and np.all(Ub[1:4] == 0.0)
+        np.testing.assert_allclose((g - 1) * Ub[4] / (Ub[0] * R), Tw, rtol=1e-14)

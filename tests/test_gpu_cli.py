@@ -99,3 +99,25 @@ def test_dgb_prandtl_option(tmp_path):
     out = subprocess.run([DGB] + ARGS + ["-prandtl", "-1", "-ofile", "bad_"], cwd=tmp_path, capture_output=True,
                          text=True, timeout=300)
     assert out.returncode != 0
+
+
+def test_dgb_isothermal_wall_option(tmp_path):
+    """An isothermal_wall side with -twall: the wall temperature changes the
+    run; the option without such a side changes nothing."""
+    iso = ["-bpy", "isothermal_wall"]
+    base = [a for a in ARGS]
+    i = base.index("-bpy")
+    del base[i:i + 2]
+
+    def run(prefix, extra):
+        out = subprocess.run([DGB] + base + extra + ["-ofile", prefix], cwd=tmp_path, capture_output=True,
+                             text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        return dg.read_state(str(tmp_path / f"{prefix}.dg"))[2]
+
+    a = run("a_", iso + ["-prandtl", "0.71", "-twall", "0.003"])
+    b = run("b_", iso + ["-prandtl", "0.71", "-twall", "0.004"])
+    assert np.linalg.norm(a - b) > 1e-12 * np.linalg.norm(a)
+    c = run("c_", ["-bpy", "inviscid_wall", "-twall", "0.003"])
+    d = run("d_", ["-bpy", "inviscid_wall"])
+    assert np.array_equal(c, d)

@@ -229,3 +229,121 @@ def test_changing_prandtl_drops_graphs_and_the_record():
         s.set_prandtl(PR)
         with pytest.raises(dg.DgbError):
             s.backward(np.ones(case.U.size))
+
+
+# ------------------------------------------------------ isothermal walls (-8)
+# An extension: the reference's no-slip wall keeps the interior energy
+# (bound_states.cpp:42-49).  Ghost state: interior density, zero velocity,
+# temperature Tw.
+
+ISO = dg.ISOTHERMAL_WALL
+
+
+def _channel(T_gas_over_Tw=1.0, n=(3, 4, 2), p=3, mu=2e-2, rng_amp=0.0, seed=0):
+    """Periodic x/z, isothermal walls at y = 0, 1; gas at rest at uniform
+    pressure and temperature T_gas_over_Tw * Tw (Tw = the reference T)."""
+    nx, ny, nz = n
+    prm = C.params(mu=mu, c=1.0, u=0.0)
+    p0, Tref = prm[5], prm[4]
+    nodes = C.box_nodes(nx, ny, nz, 1, 1.0, 1.0, 1.0)
+    E, nb = nx * ny * nz, (p + 1) ** 3
+    Tg = T_gas_over_Tw * Tref
+    rho = np.full((E, nb), p0 / (prm[1] * Tg))
+    z = np.zeros((E, nb))
+    U = C.state_from_primitives(rho, z, z, z, p0 + z, prm[0])
+    if rng_amp:
+        rng = np.random.default_rng(seed)
+        U = U * (1 + rng_amp * rng.standard_normal(U.shape))
+        U[:, 1:4] += rng_amp * rng.standard_normal(U[:, 1:4].shape)
+    return C.Case("iso", nx, ny, nz, p, 1, nodes, [C.P_, C.P_, ISO, ISO, C.P_, C.P_], prm, U.reshape(-1))
+
+
+@pytest.mark.parametrize("Pr", [0.0, PR])
+def test_isothermal_wall_keeps_gas_at_its_temperature_at_rest(Pr):
+    case = _channel(1.0)
+    with solver(case) as s:
+        s.set_prandtl(Pr)
+        _, f = s.residual(case.U)
+    assert np.abs(f).max() < 1e-12 * np.abs(case.U).max()
+
+
+def test_hot_isothermal_wall_heats_only_with_a_heat_flux():
+    """Walls at twice the gas temperature: with the heat flux the total
+    energy rises; without it the walls only push (momentum), mass and energy
+    stay (sum over nodes of R is the rate of each integral)."""
+    case = _channel(0.5)
+    tot = {}
+    for Pr in (0.0, PR):
+        with solver(case) as s:
+            s.set_prandtl(Pr)
+            R, _ = s.residual(case.U)
+        R = R.reshape(case.nelem, 5, case.nb)
+        tot[Pr] = (R.sum(axis=(0, 2)), np.abs(R).sum(axis=(0, 2)))
+    rate, scale = tot[0.0]
+    assert abs(rate[0]) <= 1e-12 * scale[0] and abs(rate[4]) <= 1e-12 * scale[4]
+    rate, scale = tot[PR]
+    assert abs(rate[0]) <= 1e-12 * scale[0]
+    assert -rate[4] > 1e-3 * scale[4], "energy flows in (R is minus the rate)"
+
+
+def test_wall_temperature_setter():
+    case = _channel(1.0)
+    with solver(case) as s:
+        _, f0 = s.residual(case.U)
+        s.set_wall_temperature(2.0 * case.prm[4])
+        _, f1 = s.residual(case.U)
+        assert np.abs(f1).max() > 0.0
+        s.set_wall_temperature(case.prm[4])
+        assert np.array_equal(s.residual(case.U)[1], f0)
+        for bad in (0.0, -1.0, math.nan, math.inf):
+            with pytest.raises(dg.DgbError):
+                s.set_wall_temperature(bad)
+
+
+@pytest.mark.parametrize("Pr", [0.0, PR])
+def test_residual_vjp_dot_product_with_isothermal_walls(Pr):
+    case = _channel(0.8, rng_amp=0.05)
+    rng = np.random.default_rng(15)
+    with solver(case) as s:
+        s.set_prandtl(Pr)
+        s.set_wall_temperature(1.2 * case.prm[4])
+        U = case.U
+        for _ in range(2):
+            lam = rng.standard_normal(U.size)
+            v = rng.standard_normal(U.size) * np.maximum(np.abs(U), 1.0)
+            h = 1e-6
+            fd = lam @ (s.residual(U + h * v)[1] - s.residual(U - h * v)[1]) / (2 * h)
+            an = s.residual_vjp(U, lam) @ v
+            assert abs(fd - an) <= 1e-7 * abs(an), (fd, an)
+
+
+def test_wall_temperature_gradient_matches_fd():
+    """dJ/dTw (dgb_backward_params) against central differences of the run
+    with the wall temperature moved, with the heat flux on; J = w . U_N."""
+    case = _channel(0.8, rng_amp=0.02)
+    N, dt = 6, 1e-3
+    Tw = 1.2 * case.prm[4]
+    w = np.random.default_rng(16).standard_normal(case.U.size)
+    with solver(case) as s:
+        s.set_prandtl(PR)
+        s.set_wall_temperature(Tw)
+        s.set_state(case.U)
+        s.forward_record(dg.TVDRK3, dt, N, 2)
+        _, dp = s.backward_params(w)
+
+        def J(t):
+            s.set_wall_temperature(t)
+            return float(w @ _step(s, case.U, dg.TVDRK3, dt, N))
+
+        h = 1e-4 * Tw
+        fd = (J(Tw + h) - J(Tw - h)) / (2 * h)
+    assert abs(dp[dg.DPARAM_TWALL] - fd) <= 1e-6 * abs(fd), (dp[dg.DPARAM_TWALL], fd)
+
+
+def test_mesh_without_isothermal_walls_has_zero_wall_gradient():
+    case = _tgv_case()
+    with solver(case) as s:
+        s.set_state(case.U)
+        s.forward_record(dg.RK4, 5e-3, 2, 2)
+        _, dp = s.backward_params(np.ones(case.U.size))
+    assert dp[dg.DPARAM_TWALL] == 0.0
