@@ -190,23 +190,25 @@ def replica_rate(world, dof_stage, stages_per_step, steps, ms):
     return world * dof_stage * stages_per_step * steps / (ms * 1e-3)
 
 
-def _timed_steps(dg, torch, s, stream, dt, steps):
-    """Device time (ms) of `steps` graph-launched RK4 steps on the handle's stream."""
+def _timed_steps(dg, torch, s, stream, dt, steps, scheme=None):
+    """Device time (ms) of `steps` graph-launched RK steps (default RK4) on the handle's stream."""
+    scheme = dg.RK4 if scheme is None else scheme
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         ev0.record(stream)
-        s.step(dg.RK4, dt, steps, norms=True)
+        s.step(scheme, dt, steps, norms=True)
         ev1.record(stream)
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1)
 
 
-def _warm(dg, torch, s, dt, min_steps, min_seconds=0.5):
+def _warm(dg, torch, s, dt, min_steps, min_seconds=0.5, scheme=None):
+    scheme = dg.RK4 if scheme is None else scheme
     t_w = time.perf_counter()
     warm = 0
     while warm < min_steps or time.perf_counter() - t_w < min_seconds:
-        s.step(dg.RK4, dt, 1, norms=False)
+        s.step(scheme, dt, 1, norms=False)
         warm += 1
     torch.cuda.synchronize()
     return warm
@@ -379,6 +381,45 @@ def _heat_block(dg, torch, steps):
     return out
 
 
+def _channel_block(dg, torch, steps):
+    """Config 5's channel: [0,4 pi] x [0,2] x [0,2 pi], 64 x 32 x 32 hexes,
+    p = 3, q = 2 nodes sinusoidally mapped (y displaced by 0.1 sin(x/2) sin z,
+    damped to flat walls), periodic x/z, isothermal walls in y at the
+    reference temperature, Pr 0.71, body force fx for Re_tau ~ 180 (bulk Re
+    5600, Ma 0.2), seeded perturbations of a parabolic profile, TVD-RK3 with
+    dt from CFL 0.2.  Device time per step of both forms.  The isothermal wall
+    and the heat flux are extensions (no reference counterpart)."""
+    from tests import cases as C
+    nx, ny, nz, p, q = 64, 32, 32, P_ORD, 2
+    lx, ly, lz = 4 * math.pi, 2.0, 2 * math.pi
+    nu = ly / 5600.0
+    utau = 180.0 * nu / (ly / 2)
+    c = 5.0
+    prm = C.params(mu=nu, c=c, u=0.0, v=0.0, w=0.0, source=(0.0, utau * utau / (ly / 2), 0.0, 0.0, 0.0))
+    nodes = C.sine_nodes(nx, ny, nz, q, lx, ly, lz, 0.1, walls=True)
+    xyz = C.node_coords(nx, ny, nz, p, q, nodes)
+    rng = np.random.default_rng(5)
+    y = xyz[..., 1]
+    u = 1.5 * (1.0 - (y - 1.0) ** 2) * (1.0 + 0.05 * rng.standard_normal(y.shape))
+    vv = 0.05 * rng.standard_normal(y.shape) * (1.0 - (y - 1.0) ** 2)
+    U0 = C.state_from_primitives(1.0 + 0 * y, u, vv, 0 * y, prm[5] + 0 * y, prm[0]).reshape(-1)
+    dt = 0.2 * (ly / ny) / ((2 * p + 1) * (c + 1.5))
+    iso = dg.ISOTHERMAL_WALL
+    mesh = dg.Mesh(nx, ny, nz, p, q, nodes, [dg.PERIODIC, dg.PERIODIC, iso, iso, dg.PERIODIC, dg.PERIODIC])
+    stream = torch.cuda.Stream()
+    out = {"workload": f"channel {nx}x{ny}x{nz} hexes, p = {p}, q = {q} sinusoidal map, isothermal walls, Pr 0.71, "
+                       f"body force, TVD-RK3 dt={dt:.3e} (CFL 0.2)"}
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_stream(stream.cuda_stream)
+            s.set_prandtl(0.71)
+            s.set_state(U0)
+            _warm(dg, torch, s, dt, 3, scheme=dg.TVDRK3)
+            ms = _timed_steps(dg, torch, s, stream, dt, steps, scheme=dg.TVDRK3) / steps
+        out[name] = {"ms_per_step": ms, "value": 5 * (p + 1) ** 3 * nx * ny * nz * 3 / (ms * 1e-3), "unit": UNIT}
+    return out
+
+
 def run_reverse_steps(args):
     """Warm-up plus `steps` reverse RK4 steps of the FP64 adjoint at the
     workload's state (a short, profilable run of the adjoint kernels)."""
@@ -488,6 +529,7 @@ def run_ours(args, rank, world, local_rank):
 
     curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
     heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
+    channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
@@ -534,6 +576,7 @@ def run_ours(args, rank, world, local_rank):
             "adjoint": adj,
             "curved": curved,
             "heat": heat,
+            "channel": channel,
             "clocks": clocks,
         }
         if cpu:
@@ -550,6 +593,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-curved", action="store_true", help="skip the curved-mesh block")
     ap.add_argument("--no-heat", action="store_true", help="skip the heat-conduction block")
+    ap.add_argument("--no-channel", action="store_true", help="skip the channel (isothermal walls) block")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")

@@ -74,6 +74,37 @@ def enstrophy(U, quad):
     return quad.integrate(0.5 * rho * (wx * wx + wy * wy + wz * wz)) / quad.volume
 
 
+def wall_shear(U, quad, mu, wall="-y"):
+    """Mean wall shear stress tau_xy = mu (du/dy + dv/dx) over the wall y = 0
+    ("-y") or y = ly ("+y") of a box mesh, from the wall elements' own
+    polynomials (one-sided, as the solver's face terms take the interior
+    trace), integrated with the P x P Gauss points of the face.  The channel
+    diagnostic (config 5's skin friction); u = m / rho."""
+    P = quad.p + 1
+    nx, ny, nz = quad.nx, quad.ny, quad.nz
+    hx, hy, hz = quad.h
+    Ue = U.reshape(nz, ny, nx, 5, P, P, P)  # [k][j][i][r][z][y][x]
+    j, end = (0, 0.0) if wall == "-y" else (ny - 1, 1.0)
+    Uw = Ue[:, j]  # [k][i][r][z][y][x]
+    dd = dict(dtype=torch.float64, device=U.device)
+    p = quad.p
+    Ev = torch.tensor([lagrange1d(a, p, end) for a in range(P)], **dd)
+    Dv = torch.tensor([lagrange1d_deriv(a, p, end) for a in range(P)], **dd)
+    B, Bd = quad.B, quad.Bd
+    V = torch.einsum("cz,y,ax,kirzyx->kirca", B, Ev, B, Uw)
+    Vy = torch.einsum("cz,y,ax,kirzyx->kirca", B, Dv, B, Uw) / hy
+    Vx = torch.einsum("cz,y,ax,kirzyx->kirca", B, Ev, Bd, Uw) / hx
+    rho = V[:, :, 0]
+    u, v = V[:, :, 1] / rho, V[:, :, 2] / rho
+    dudy = (Vy[:, :, 1] - u * Vy[:, :, 0]) / rho
+    dvdx = (Vx[:, :, 2] - v * Vx[:, :, 0]) / rho
+    x, w = gauss_legendre(P, 0.0, 1.0)
+    wq = torch.tensor(w, **dd)
+    W = torch.einsum("c,a->ca", wq, wq) * (hx * hz)
+    area = nx * hx * nz * hz
+    return (mu * (dudy + dvdx) * W).sum() / area
+
+
 def box_node_coords(nx, ny, nz, p, lx, ly, lz):
     """Physical coordinates of the solution nodes of a uniform box mesh,
     [E][(p+1)^3][3], element e = i + nx (j + ny k), node b = x + P (y + P z)."""
