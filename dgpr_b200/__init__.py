@@ -21,6 +21,7 @@ INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW
 ISOTHERMAL_WALL = -8  # an extension: no-slip wall at Solver.set_wall_temperature (default: params T)
 RK4, TVDRK3 = 0, 1
 FP64, MIXED_FP32 = 0, 1
+STEP_GAUSS, STEP_NODAL = 0, 1  # dgb_set_step_form
 DPARAM_MU, DPARAM_SOURCE, DPARAM_TWALL, NDPARAMS = 0, 1, 6, 7  # dgb_backward_params: dJ/d[mu, source[0..4], Tw]
 
 BOUNDARY_TYPES = {  # the reference's boundary_types map (boundaries.cpp:37-44)
@@ -114,6 +115,7 @@ def lib():
             "dgb_backward_params_device": (ctypes.c_int, [vp, vp, vp, vp]),
             "dgb_set_params": (ctypes.c_int, [vp, ctypes.POINTER(Params)]),
             "dgb_set_wall_temperature": (ctypes.c_int, [vp, ctypes.c_double]),
+            "dgb_set_step_form": (ctypes.c_int, [vp, ctypes.c_int]),
             "dgb_adjoint_stats": (ctypes.c_int, [vp] + [ctypes.POINTER(ctypes.c_longlong)] * 3),
             "dgb_checkpoint_plan": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_longlong), ctypes.c_longlong,
@@ -425,6 +427,10 @@ class Solver:
     def backward_params_device(self, lamN_ptr, out_ptr, dpar_ptr):
         _check(lib().dgb_backward_params_device(self.h, ctypes.c_void_p(lamN_ptr), ctypes.c_void_p(out_ptr),
                                                 ctypes.c_void_p(dpar_ptr)))
+
+    def set_step_form(self, form):
+        """STEP_GAUSS (default: dgb_step at the Gauss points) or STEP_NODAL."""
+        _check(lib().dgb_set_step_form(self.h, int(form)))
 
     def set_wall_temperature(self, Tw):
         """Temperature of the isothermal walls (> 0); drops the recorded run."""

@@ -432,6 +432,7 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
                        double* norms_host)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
+  h->v_current = false;  // the recorded run steps the nodal state d_U
   int rc = check_scheme(scheme, dt);
   if (rc) return rc;
   if (nsteps < 1 || slots < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1 and slots >= 1");
@@ -496,6 +497,7 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
 int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, double* norms_host)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
+  h->v_current = false;  // the recorded run steps the nodal state d_U
   int rc = check_scheme(scheme, dt);
   if (rc) return rc;
   if (nsteps < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1");
@@ -588,6 +590,7 @@ int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, doubl
   if (!h || !lamN_dev || !lam0_dev) return fail(DGB_ERR_ARG, "null argument");
   if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
   CK(cudaSetDevice(h->device));
+  h->v_current = false;  // the sweep works on the nodal state d_U
   if (dpar) {
     const int rc = ensure_pgrad(h);
     if (rc) return rc;

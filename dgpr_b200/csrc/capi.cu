@@ -53,9 +53,12 @@ int enqueue_residual(dgb_handle* h, const double* Uin, double* R, double* f)
 // Traces of the resident state, read by the first stage of the next step.
 // Every dgb_step call starts with this one launch; later stages and steps get
 // their traces from the epilogue of the stage before.
-int enqueue_initial_traces(dgb_handle* h)
+int enqueue_initial_traces(dgb_handle* h, bool gauss)
 {
-  CK(launch_trace(klaunch(h), h->d_U, h->d_trace[0], h->stream));
+  if (gauss)
+    CK(launch_vtrace(klaunch(h), h->d_V, h->d_trace[0], h->stream));
+  else
+    CK(launch_trace(klaunch(h), h->d_U, h->d_trace[0], h->stream));
   return DGB_OK;
 }
 
@@ -65,9 +68,11 @@ int enqueue_initial_traces(dgb_handle* h)
 //   RK4      T0 -> T1 -> T0 -> T1 -> T0
 //   TVD-RK3  T0 -> T1 -> T2 -> T0
 // With ev != null, ev[i] is recorded before launch i and ev[nlaunch] after the
-// last one (per-kernel timing by dgb_profile_step).
-int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr)
+// last one (per-kernel timing by dgb_profile_step).  gauss: the Gauss-point
+// form on d_V (vspace.cuh), else the nodal form on d_U.
+int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr, bool gauss = false)
 {
+  double* Ures = gauss ? h->d_V : h->d_U;
   const KLaunch L = klaunch(h);
   const int nst = scheme == DGB_RK4 ? 4 : 3;
   const int modes4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
@@ -76,17 +81,20 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
   const int tin3[3] = {0, 1, 2}, tout3[3] = {1, 2, 0};
   int k = 0;
   for (int s = 0; s < nst; ++s) {
-    const double* in = s == 0 ? h->d_U : h->d_Us;
+    const double* in = s == 0 ? Ures : h->d_Us;
     StageArgs a = stage_args(scheme == DGB_RK4 ? modes4[s] : modes3[s], dt);
-    a.Ubase = h->d_U;
+    a.Ubase = Ures;
     a.acc = h->d_acc;
-    a.Uout = s == nst - 1 ? h->d_U : h->d_Us;
+    a.Uout = s == nst - 1 ? Ures : h->d_Us;
     a.part = s == 0 ? h->d_part : nullptr;
     a.flag = h->d_flag;
     a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
     const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-    CK(launch_stage(L, in, tin, a, h->stream));
+    if (gauss)
+      CK(launch_vstage(L, in, tin, a, h->stream));
+    else
+      CK(launch_stage(L, in, tin, a, h->stream));
     if (s == 0) {
       if (ev) CK(cudaEventRecord(ev[k++], h->stream));
       CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
@@ -101,8 +109,8 @@ long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == D
 
 void free_all(dgb_handle* h)
 {
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_mean, h->d_U, h->d_Us, h->d_acc, h->d_trace[0],
+  drop_step_graphs(h);
+  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_mean, h->d_U, h->d_V, h->d_Us, h->d_acc, h->d_trace[0],
                   h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
                   h->d_counter, h->d_flag};
   for (void* p : ptrs)
@@ -143,9 +151,7 @@ int replace_device_params(dgb_handle* h, const DevParams& d)
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   h->dprm = d;
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  h->graph = nullptr;
-  h->graph_scheme = -1;
+  drop_step_graphs(h);
   if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
   h->rev_graph = nullptr;
   h->rev_scheme = -1;
@@ -155,49 +161,58 @@ int replace_device_params(dgb_handle* h, const DevParams& d)
 
 }  // namespace
 
-// The captured graph of one step for (scheme, dt), with room for `cap` norms.
-int dgb::ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap)
+void dgb::drop_step_graphs(dgb_handle* h)
+{
+  for (dgb_handle::StepGraph* g : {&h->graph, &h->ggraph}) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    g->exec = nullptr;
+    g->scheme = -1;
+  }
+}
+
+// The captured graph of one step for (scheme, dt) in the nodal or the
+// Gauss-point form, with room for `cap` norms.
+int dgb::ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap, bool gauss)
 {
   if (cap > h->norms_cap) {
     if (h->d_norms) CK(cudaFree(h->d_norms));
     h->d_norms = nullptr;
     CK(cudaMalloc(&h->d_norms, sizeof(double) * cap));
     h->norms_cap = cap;
-    if (h->graph) {  // the captured graph holds the old norms pointer and capacity
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-      h->graph_scheme = -1;
-    }
+    drop_step_graphs(h);  // the captured graphs hold the old norms pointer and capacity
   }
-  if (h->graph && h->graph_scheme == scheme && h->graph_dt == dt) return DGB_OK;
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  h->graph = nullptr;
-  h->graph_scheme = -1;
+  dgb_handle::StepGraph& sg = gauss ? h->ggraph : h->graph;
+  if (sg.exec && sg.scheme == scheme && sg.dt == dt) return DGB_OK;
+  if (sg.exec) cudaGraphExecDestroy(sg.exec);
+  sg.exec = nullptr;
+  sg.scheme = -1;
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_step(h, scheme, dt);
+  int rc = enqueue_step(h, scheme, dt, nullptr, gauss);
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
   if (rc) return rc;
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-  ce = cudaGraphInstantiate(&h->graph, g, 0);
+  ce = cudaGraphInstantiate(&sg.exec, g, 0);
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-  h->graph_scheme = scheme;
-  h->graph_dt = dt;
+  sg.scheme = scheme;
+  sg.dt = dt;
   h->launches_per_step = launches_per_step(h, scheme);
   return DGB_OK;
 }
 
-// k replays of the step graph; with initial_trace the face traces of the
-// resident state are computed first (otherwise the last step's epilogue left
-// them in trace buffer 0).  Norms go to d_norms[*d_counter ...].
-int dgb::enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace)
+// k replays of the step graph of the form; with initial_trace the face
+// traces of the resident state (d_U, or d_V in the Gauss-point form) are
+// computed first (otherwise the last step's epilogue left them in trace
+// buffer 0).  Norms go to d_norms[*d_counter ...].
+int dgb::enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace, bool gauss)
 {
   if (initial_trace) {
-    int rc = enqueue_initial_traces(h);
+    int rc = enqueue_initial_traces(h, gauss);
     if (rc) return rc;
   }
-  for (unsigned long long s = 0; s < k; ++s) CK(cudaGraphLaunch(h->graph, h->stream));
+  cudaGraphExec_t g = gauss ? h->ggraph.exec : h->graph.exec;
+  for (unsigned long long s = 0; s < k; ++s) CK(cudaGraphLaunch(g, h->stream));
   return DGB_OK;
 }
 
@@ -279,6 +294,7 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMalloc(&h->d_geo, sizeof(double) * geo.size()));
   CKF(cudaMalloc(&h->d_nbr, sizeof(int) * nbr.size()));
   CKF(cudaMalloc(&h->d_U, sb));
+  CKF(cudaMalloc(&h->d_V, sb));
   CKF(cudaMalloc(&h->d_Us, sb));
   CKF(cudaMalloc(&h->d_acc, sb));
   for (int t = 0; t < 3; ++t)
@@ -304,6 +320,7 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
     CKF(cudaMemcpy(h->d_opsf, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice));
   }
   CKF(prepare_kernels(h->P, precision));
+  CKF(prepare_gauss(h->P, precision));
 #undef CKF
   *out = h;
   return DGB_OK;
@@ -332,11 +349,7 @@ int dgb_set_stream(dgb_handle* h, void* stream)
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
   }
-  if (h->graph) {
-    cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-    h->graph_scheme = -1;
-  }
+  drop_step_graphs(h);
   return DGB_OK;
 }
 
@@ -384,6 +397,7 @@ int dgb_set_state(dgb_handle* h, const double* U_host)
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(h->d_U, U_host, sizeof(double) * (size_t)h->n, cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  h->v_current = false;
   return DGB_OK;
 }
 
@@ -402,6 +416,7 @@ int dgb_set_state_device(dgb_handle* h, const double* U_dev)
   CK(cudaSetDevice(h->device));
   CK(cudaMemcpyAsync(h->d_U, U_dev, sizeof(double) * (size_t)h->n, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  h->v_current = false;
   return DGB_OK;
 }
 
@@ -452,6 +467,16 @@ int dgb_state_device_ptr(dgb_handle* h, double** U_dev)
 {
   if (!h || !U_dev) return fail(DGB_ERR_ARG, "null argument");
   *U_dev = h->d_U;
+  h->v_current = false;  // the caller may write through it before the next dgb_step
+  return DGB_OK;
+}
+
+int dgb_set_step_form(dgb_handle* h, int form)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (form != DGB_STEP_GAUSS && form != DGB_STEP_NODAL) return fail(DGB_ERR_ARG, "unknown step form");
+  h->gauss_step = form == DGB_STEP_GAUSS;
+  h->v_current = false;
   return DGB_OK;
 }
 
@@ -495,12 +520,18 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
   if (!(dt == dt)) return fail(DGB_ERR_ARG, "dt is NaN");
   CK(cudaSetDevice(h->device));
   if (nsteps == 0) return DGB_OK;
-  int rc = ensure_step_graph(h, scheme, dt, nsteps);
+  const bool gauss = h->gauss_step;
+  int rc = ensure_step_graph(h, scheme, dt, nsteps, gauss);
   if (rc) return rc;
   CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  if ((rc = enqueue_steps(h, nsteps, true))) return rc;
-  h->last_launches = 1 + (long long)nsteps * h->launches_per_step;
+  const KLaunch L = klaunch(h);
+  const bool convert_in = gauss && !h->v_current;
+  if (convert_in) CK(launch_gauss_basis(L, h->d_U, h->d_V, true, h->stream));
+  if ((rc = enqueue_steps(h, nsteps, true, gauss))) return rc;
+  if (gauss) CK(launch_gauss_basis(L, h->d_V, h->d_U, false, h->stream));
+  h->v_current = gauss;
+  h->last_launches = 1 + (long long)nsteps * h->launches_per_step + (convert_in ? 1 : 0) + (gauss ? 1 : 0);
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (norms_host)
@@ -530,12 +561,18 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
   std::vector<cudaEvent_t> ev((size_t)reps * (nl + 1));
   for (auto& e : ev) CK(cudaEventCreate(&e));
   int rc = DGB_OK;
+  const bool gauss = h->gauss_step;  // the form dgb_step runs
+  if (gauss && !h->v_current) CK(launch_gauss_basis(klaunch(h), h->d_U, h->d_V, true, h->stream));
   for (int r = 0; r < reps && rc == DGB_OK; ++r) {
     cudaEvent_t* er = &ev[(size_t)r * (nl + 1)];
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(er[0], h->stream));
-    rc = enqueue_initial_traces(h);
-    if (rc == DGB_OK) rc = enqueue_step(h, scheme, dt, er + 1);
+    rc = enqueue_initial_traces(h, gauss);
+    if (rc == DGB_OK) rc = enqueue_step(h, scheme, dt, er + 1, gauss);
+  }
+  if (gauss && rc == DGB_OK) {
+    CK(launch_gauss_basis(klaunch(h), h->d_V, h->d_U, false, h->stream));
+    h->v_current = true;
   }
   CK(cudaStreamSynchronize(h->stream));
   for (int k = 0; k < nl; ++k) ms_out[k] = 0.;

@@ -336,6 +336,9 @@ int main(int argc, char** argv)
       char f[1100];
       snprintf(f, sizeof f, "%s%" PRIu64 ".dg", in.ofile.c_str(), (uint64_t)tstep);
       write(f, tstep);
+      // continue from the state as written, as a restart from this file
+      // would (dgb_step otherwise continues from its Gauss-point copy)
+      if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
     }
     unsigned long long n = tfinal - tstep;
     if (in.chkint) {  // up to, not including, the next checkpointing step

@@ -48,9 +48,20 @@ struct dgb_handle {
   int* d_counter = nullptr;
   int* d_flag = nullptr;
   unsigned long long norms_cap = 0;
-  cudaGraphExec_t graph = nullptr;
-  int graph_scheme = -1;
-  double graph_dt = 0.;
+  // captured RK steps: nodal form (the recorded runs of the adjoint) and
+  // Gauss-point form (dgb_step, vspace.cuh), each for one (scheme, dt)
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    int scheme = -1;
+    double dt = 0.;
+  };
+  StepGraph graph, ggraph;
+  bool gauss_step = true;    // dgb_step in the Gauss-point form (dgb_set_step_form)
+  double* d_V = nullptr;     // Gauss-point values of the state during dgb_step
+  // d_V holds the state that d_U is the nodal image of (set by dgb_step,
+  // cleared by everything that writes d_U otherwise): consecutive dgb_step
+  // calls continue from d_V, so splitting a run into calls changes nothing
+  bool v_current = false;
   long long launches_per_step = 0;
   long long last_launches = 0;
 
@@ -120,7 +131,8 @@ void free_adjoint(dgb_handle* h);
 // DevParams of the reference parameters, with the heat flux of Prandtl number
 // `prandtl` (0: none) and isothermal walls at `twall` (< 0: p.T)
 DevParams device_params(const dgb_params& p, double prandtl, double twall);
-int ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap);
-int enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace);
+int ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long long cap, bool gauss = false);
+int enqueue_steps(dgb_handle* h, unsigned long long k, bool initial_trace, bool gauss = false);
+void drop_step_graphs(dgb_handle* h);
 
 }  // namespace dgb

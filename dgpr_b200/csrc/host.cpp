@@ -161,10 +161,15 @@ int build_ops(int p, Ops1D& o)
       for (int j = 0; j < P; ++j) s += o.E[e][i] * o.M1i[P * i + j] * o.E[e][j];
     o.cend[e] = s;
     o.EL[e].assign(P, 0.);
+    o.DL[e].assign(P, 0.);
     for (int q = 0; q < P; ++q) {
-      double v = 0.;
-      for (int i = 0; i < P; ++i) v += o.E[e][i] * o.Bi[P * i + q];
+      double v = 0., d = 0.;
+      for (int i = 0; i < P; ++i) {
+        v += o.E[e][i] * o.Bi[P * i + q];
+        d += o.D[e][i] * o.Bi[P * i + q];
+      }
       o.EL[e][q] = v;
+      o.DL[e][q] = d;
     }
   }
   o.Wb.assign(P, 0.);

@@ -39,6 +39,7 @@ struct Ops1D {
   double cend[2] = {0, 0};    // E[end]^T M1i E[end]
   std::vector<double> EL[2];  // EL[end][q] = (E[end] B^-1)[q]: value at xi = end of the
                               // Lagrange polynomial through the GL nodes that is 1 at node q
+  std::vector<double> DL[2];  // DL[end][q] = (D[end] B^-1)[q]: its derivative there
 };
 
 // Curved (non-affine) elements carry their geometry per point:

@@ -61,11 +61,14 @@ struct Cfg {
   static constexpr int FPP = DGB_FACES_PER_PASS;
   static constexpr int NF = FPP * NQF;
   static constexpr int NTS = (((NB > NF ? NB : NF) + 31) / 32) * 32;
-  // operator table: B Bd Dq M1i Bi (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2]
+  // operator table: B Bd Dq M1i Bi (P*P each), E0 E1 D0 D1 Wb w (P each), cend[2],
+  // EL0 EL1 DL0 DL1 (P each: value / derivative at xi = 0, 1 of the Lagrange
+  // polynomials through the Gauss points, for the Gauss-point stage kernel)
   static constexpr int oB = 0, oBd = P * P, oDq = 2 * P * P, oMi = 3 * P * P, oBi = 4 * P * P;
   static constexpr int oE = 5 * P * P, oD = oE + 2 * P, oWb = oD + 2 * P, oW = oWb + P;
   static constexpr int oC = oW + P;
-  static constexpr int OPS = oC + 2;
+  static constexpr int oEh = oC + 2, oDh = oEh + 2 * P;
+  static constexpr int OPS = oDh + 2 * P;
 };
 
 constexpr int align16(int bytes) { return (bytes + 15) & ~15; }
@@ -232,6 +235,46 @@ __device__ __forceinline__ void dual_consistency_ref(const T* S, const T* d, con
 
 // ------------------------------------------------------------- face traces
 
+// The trace of one face point: the 5 values S and A(S, grad S).n_out from
+// the reference-space gradient g[c][r] = dS_r/dxi_c, into Te[(lf*10 + r)*NQF + fq].
+template <int P, class T, bool CV>
+__device__ __forceinline__ void trace_point_store(int lf, int fq, const T* S, const T (*g)[5], const T* sg,
+                                                  const double* __restrict__ gfe, T mu, T kq,
+                                                  T* __restrict__ Te)
+{
+  constexpr int NQF = P * P;
+  T Qn[5] = {T(0), T(0), T(0), T(0), T(0)};
+  if (mu != T(0)) {
+    T Ji[9], n[3];
+    if constexpr (CV) {
+      const double* gp = gfe + lf * kFaceC * NQF + fq;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Ji[c] = T(gp[c * NQF]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) n[c] = T(gp[(kFaceN + c) * NQF]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Ji[c] = sg[kGeoJinv + c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) n[c] = sg[kGeoN + 3 * lf + c];
+    }
+    T G[3][5], Q[3][5];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 5; ++r) G[c][r] = Ji[c] * g[0][r] + Ji[3 + c] * g[1][r] + Ji[6 + c] * g[2][r];
+    visc_flux(S, G, mu, Q, kq);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
+  }
+  T* Tq = Te + lf * 10 * NQF;
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    Tq[r * NQF + fq] = S[r];
+    Tq[(5 + r) * NQF + fq] = Qn[r];
+  }
+}
+
 // Traces of a nodal state sUx[5][NB] (shared memory) on the FPP faces
 // lf = FPP*half + j, j < FPP: at every face quadrature point the 5 conserved values
 // and the viscous normal flux A(U, grad U).n_out, written to
@@ -312,36 +355,7 @@ __device__ __forceinline__ void trace_half(int half, const T* sUx, T* sN, T* sY,
       g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
       g[2][r] = a == 2 ? dn : d2;
     }
-    T Qn[5] = {T(0), T(0), T(0), T(0), T(0)};
-    if (mu != T(0)) {
-      T Ji[9], n[3];
-      if constexpr (CV) {
-        const double* gp = gfe + lf * kFaceC * NQF + fq;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) Ji[c] = T(gp[c * NQF]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) n[c] = T(gp[(kFaceN + c) * NQF]);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 9; ++c) Ji[c] = sg[kGeoJinv + c];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) n[c] = sg[kGeoN + 3 * lf + c];
-      }
-      T G[3][5], Q[3][5];
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int r = 0; r < 5; ++r) G[c][r] = Ji[c] * g[0][r] + Ji[3 + c] * g[1][r] + Ji[6 + c] * g[2][r];
-      visc_flux(S, G, mu, Q, kq);
-#pragma unroll
-      for (int r = 0; r < 5; ++r) Qn[r] = Q[0][r] * n[0] + Q[1][r] * n[1] + Q[2][r] * n[2];
-    }
-    T* Tq = Te + lf * 10 * NQF;
-#pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      Tq[r * NQF + fq] = S[r];
-      Tq[(5 + r) * NQF + fq] = Qn[r];
-    }
+    trace_point_store<P, T, CV>(lf, fq, S, g, sg, gfe, mu, kq, Te);
   }
 }
 
@@ -385,6 +399,130 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
     if (half) __syncthreads();  // the scratch of the previous pass is reused
     trace_half<P, T, CV>(half, sU, sN, sY, so, sg, T(prm.mu), HT ? T(prm.kq) : T(0), Te, CV ? gf + e * 6 * kFaceC * NQF : nullptr);
   }
+}
+
+// ------------------------------------------------------------- face fluxes
+
+// The face terms of one face point (lf, fq) of element e (solve.cpp:393-794):
+// fa[r * NQF] = the coefficient of the test function phi (Roe or boundary
+// flux, minus the viscous normal flux, plus the BR2 lifting), times fJ w;
+// fb[(i * 4 + r - 1) * NQF] = the dual-consistency coefficient of
+// d(phi)/d(xi_i) for variables 1..4.  The traces of the element (own) and of
+// its neighbours come from Tr.  Shared by the nodal and the Gauss-point
+// stage kernels, so their face arithmetic is the same.
+template <int P, class T, bool CV>
+__device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const T* __restrict__ Tr,
+                                                  const int* __restrict__ nbr, const T* so, const T* sg,
+                                                  const double* __restrict__ geo, const double* __restrict__ gf,
+                                                  const double* __restrict__ gfe, const DevParams& prm, T gamma,
+                                                  T mu, T kq, T detJ, const T* Ji, int* flag, T* fa, T* fb)
+{
+  using C = Cfg<P>;
+  constexpr int NQF = C::NQF;
+  const int q1 = fq % P, q2 = fq / P, end = lf & 1;
+  const T* w1 = so + C::oW;
+  const T eta = T(prm.eta);
+  // geometry of this face point (affine elements: the element's, in shared
+  // memory; curved ones: per point, each value loaded where it is used)
+  const double* gp = CV ? gfe + lf * kFaceC * NQF + fq : nullptr;
+  T nbuf[3];
+  if constexpr (CV) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) nbuf[c] = T(gp[(kFaceN + c) * NQF]);
+  }
+  const T* n = CV ? nbuf : sg + kGeoN + 3 * lf;
+  const T fJ = CV ? T(gp[kFaceFJ * NQF]) : sg[kGeoFJ + lf];
+  const T fw = fJ * w1[q1] * w1[q2];
+  const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
+  T Uo[5], Qo[5];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    Uo[r] = To[r * NQF + fq];
+    Qo[r] = To[(5 + r) * NQF + fq];
+  }
+  const int nb = nbr[e * 6 + lf];
+  if (nb >= 0) {
+    const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+    T Un[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
+    {
+      // Roe flux in one orientation for both sides: the element that sees
+      // the face on its high side is "left"; the other side negates it
+      T UL[5], UR[5], F[5];
+      const T sgn = end ? T(1) : T(-1);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        UL[r] = end ? Uo[r] : Un[r];
+        UR[r] = end ? Un[r] : Uo[r];
+      }
+      const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
+      roe_flux(UL, UR, nn, gamma, F);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) fa[r * NQF] = sgn * F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
+    }
+    if (mu != T(0)) {
+      T d[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) d[r] = Uo[r] - T(0.5) * (Uo[r] + Un[r]);  // Uo - Uhat
+      {
+        T Jbuf[9];
+        if constexpr (CV) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
+        }
+        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
+      T ro[5], rn[5];
+      visc_jump_n(Uo, d, n, mu, ro, kq);  // BR2 lifting sources of both sides
+      visc_jump_n(Un, d, n, mu, rn, kq);
+      T lift_n;  // the neighbour's lifting scale at this face point
+      if constexpr (CV)
+        lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
+      else
+        lift_n = so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+      const T lift = CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ;
+      const T lo = T(0.5) * eta * T(0.5) * fJ * lift;
+      const T ln = T(0.5) * eta * T(0.5) * fJ * lift_n;
+#pragma unroll
+      for (int r = 1; r < 5; ++r) fa[r * NQF] += lo * ro[r] + ln * rn[r];
+    }
+  } else {
+    T Ub[5];
+    const int bad = boundary_state(nb, Uo, n, prm, Ub);
+    if (bad && flag) atomicOr(flag, 2);
+    {
+      T F[5];
+      euler_flux_n(Ub, gamma, n, F);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - Qo[r];
+    }
+    if (mu != T(0)) {
+      T d[5], rb[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ub[r];
+      {
+        T Jbuf[9];
+        if constexpr (CV) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
+        }
+        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
+      }
+      visc_jump_n(Ub, d, n, mu, rb, kq);
+      const T lb = eta * fJ * (CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ);
+#pragma unroll
+      for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
+    }
+  }
+  if (mu == T(0)) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) fb[i * NQF] = T(0);
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r) fa[r * NQF] *= fw;
 }
 
 // ------------------------------------------------------------- stage kernel
@@ -580,115 +718,12 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   T* Fb = Fa + FPP * 5 * NQF;  // [FPP][12][NQF]
   T* Su = Fb + FPP * 12 * NQF; // [FPP][13][NQF]
   T* Sc = Fb;                // [FPP][9][NQF]
-  const T* w1 = so + C::oW;
-  const T eta = T(prm.eta);
 #pragma unroll 1
   for (int half = 0; half < 6 / FPP; ++half) {
     if (tid < NH) {
-      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
-      // geometry of this face point (affine elements: the element's, in shared
-      // memory; curved ones: per point, each value loaded where it is used)
-      const double* gp = CV ? gfe + lf * kFaceC * NQF + fq : nullptr;
-      T nbuf[3];
-      if constexpr (CV) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) nbuf[c] = T(gp[(kFaceN + c) * NQF]);
-      }
-      const T* n = CV ? nbuf : sg + kGeoN + 3 * lf;
-      const T fJ = CV ? T(gp[kFaceFJ * NQF]) : sg[kGeoFJ + lf];
-      const T fw = fJ * w1[q1] * w1[q2];
-      const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
-      T Uo[5], Qo[5];
-#pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        Uo[r] = To[r * NQF + fq];
-        Qo[r] = To[(5 + r) * NQF + fq];
-      }
-      const int nb = nbr[e * 6 + lf];
-      T* fa = Fa + j * 5 * NQF + fq;
-      T* fb = Fb + j * 12 * NQF + fq;
-      if (nb >= 0) {
-        const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
-        T Un[5];
-#pragma unroll
-        for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
-        {
-          // Roe flux in one orientation for both sides: the element that sees
-          // the face on its high side is "left"; the other side negates it
-          T UL[5], UR[5], F[5];
-          const T sgn = end ? T(1) : T(-1);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            UL[r] = end ? Uo[r] : Un[r];
-            UR[r] = end ? Un[r] : Uo[r];
-          }
-          const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
-          roe_flux(UL, UR, nn, gamma, F);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) fa[r * NQF] = sgn * F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
-        }
-        if (mu != T(0)) {
-          T d[5];
-#pragma unroll
-          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - T(0.5) * (Uo[r] + Un[r]);  // Uo - Uhat
-          {
-            T Jbuf[9];
-            if constexpr (CV) {
-#pragma unroll
-              for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
-            }
-            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
-          }
-#pragma unroll
-          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
-          T ro[5], rn[5];
-          visc_jump_n(Uo, d, n, mu, ro, kq);  // BR2 lifting sources of both sides
-          visc_jump_n(Un, d, n, mu, rn, kq);
-          T lift_n;  // the neighbour's lifting scale at this face point
-          if constexpr (CV)
-            lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
-          else
-            lift_n = so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
-          const T lift = CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ;
-          const T lo = T(0.5) * eta * T(0.5) * fJ * lift;
-          const T ln = T(0.5) * eta * T(0.5) * fJ * lift_n;
-#pragma unroll
-          for (int r = 1; r < 5; ++r) fa[r * NQF] += lo * ro[r] + ln * rn[r];
-        }
-      } else {
-        T Ub[5];
-        const int bad = boundary_state(nb, Uo, n, prm, Ub);
-        if (bad && sa.flag) atomicOr(sa.flag, 2);
-        {
-          T F[5];
-          euler_flux_n(Ub, gamma, n, F);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - Qo[r];
-        }
-        if (mu != T(0)) {
-          T d[5], rb[5];
-#pragma unroll
-          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ub[r];
-          {
-            T Jbuf[9];
-            if constexpr (CV) {
-#pragma unroll
-              for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
-            }
-            dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
-          }
-          visc_jump_n(Ub, d, n, mu, rb, kq);
-          const T lb = eta * fJ * (CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ);
-#pragma unroll
-          for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
-        }
-      }
-      if (mu == T(0)) {
-#pragma unroll
-        for (int i = 0; i < 12; ++i) fb[i * NQF] = T(0);
-      }
-#pragma unroll
-      for (int r = 0; r < 5; ++r) fa[r * NQF] *= fw;
+      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF;
+      face_point_fluxes<P, T, CV>(e, lf, fq, Tr, nbr, so, sg, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag,
+                                  Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
     __syncthreads();
     if (tid < NH) {  // test functions, first tangential direction: items (j, t1, q2)

@@ -84,4 +84,30 @@ cudaError_t launch_trace_fp32_heat(const KLaunch& L, const double* U, void* Tout
 cudaError_t launch_stage_fp32_heat(const KLaunch& L, const double* Us, const void* Tin, const StageArgs& sa,
                                    cudaStream_t st);
 
+// Gauss-point form of the stage (vspace.cuh), used by dgb_step: states,
+// stage states and the RK accumulator are values at the P^3 Gauss points
+cudaError_t prepare_gauss(int P, int precision);
+cudaError_t launch_vtrace(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
+cudaError_t launch_vstage(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                          cudaStream_t st);
+// V = B3 U (to_gauss) or U = B3^-1 V, FP64, per element
+cudaError_t launch_gauss_basis(const KLaunch& L, const double* in, double* out, bool to_gauss, cudaStream_t st);
+// per compute type and heat flag (vspace_*.cu)
+cudaError_t vprepare_fp64(int P, bool heat);
+cudaError_t vlaunch_trace_fp64(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
+cudaError_t vlaunch_stage_fp64(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                               cudaStream_t st);
+cudaError_t vprepare_fp32(int P, bool heat);
+cudaError_t vlaunch_trace_fp32(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
+cudaError_t vlaunch_stage_fp32(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                               cudaStream_t st);
+cudaError_t vprepare_fp64_heat(int P);
+cudaError_t vlaunch_trace_fp64_heat(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
+cudaError_t vlaunch_stage_fp64_heat(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                                    cudaStream_t st);
+cudaError_t vprepare_fp32_heat(int P);
+cudaError_t vlaunch_trace_fp32_heat(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
+cudaError_t vlaunch_stage_fp32_heat(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                                    cudaStream_t st);
+
 }  // namespace dgb

@@ -6,7 +6,7 @@
 
 namespace dgb {
 
-int ops_table_size(int P) { return 5 * P * P + 6 * P + 2; }
+int ops_table_size(int P) { return 5 * P * P + 10 * P + 2; }
 
 void pack_ops(const Ops1D& o, double* t)
 {
@@ -29,6 +29,13 @@ void pack_ops(const Ops1D& o, double* t)
   }
   t[oC] = o.cend[0];
   t[oC + 1] = o.cend[1];
+  const int oEh = oC + 2, oDh = oEh + 2 * P;
+  for (int q = 0; q < P; ++q) {
+    t[oEh + q] = o.EL[0][q];
+    t[oEh + P + q] = o.EL[1][q];
+    t[oDh + q] = o.DL[0][q];
+    t[oDh + P + q] = o.DL[1][q];
+  }
 }
 
 size_t trace_elem_bytes(int precision) { return precision == DGB_MIXED_FP32 ? sizeof(float) : sizeof(double); }

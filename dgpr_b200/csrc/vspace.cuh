@@ -1,0 +1,537 @@
+// Gauss-point form of the RK stage, used by dgb_step.
+//
+// The nodal state U (equispaced Lagrange coefficients, the reference's
+// layout, basis.cpp:91-148) and its values at the P^3 Gauss points,
+// V = (B x B x B) U, describe the same polynomial: B is square and
+// invertible.  Written in V, the discretisation of solve.cpp:150-807 keeps
+// every integral and changes only the algebra around them:
+//   mass matrix     M = B3^T diag(w detJ) B3  ->  f_V = -Y / (w detJ), Y = B3^-T R
+//                   (diagonal: the Gauss points integrate the mass exactly)
+//   volume term     R_vol = B3^T sum_i Dq_i^T Ghat_i  ->  Y_vol = sum_i Dq_i^T Ghat_i
+//   face terms      phi_node(face point) = (E_end x B x B) -> (EL_end x I x I):
+//                   a face point's coefficient reaches the P Gauss points on
+//                   its normal line through EL = E B^-1 (values) and
+//                   DL = D B^-1 (normal derivatives); the tangential
+//                   derivative terms become Dq^T along the face
+//   face traces     value / normal derivative at a face point from the normal
+//                   line through EL / DL, tangential derivatives by Dq on the
+//                   face; no tangential interpolation
+// Against the nodal stage kernel this drops the interpolation to the Gauss
+// points, the B^T and M1^-1 contractions and one of the two tangential
+// passes of the face test functions.  dgb_step converts U -> V before its
+// steps and V -> U after them (gauss_basis_kernel); the
+// state, stage states and RK accumulator in between are Gauss-point values.
+// The face-point fluxes (face_point_fluxes) and the pointwise physics are
+// the nodal kernel's own functions.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace dgb {
+
+// Shared memory: [operators (T) | element geometry (T)] followed by one
+// scratch region reused by the phases:
+//   volume  V1[5NB] values, G[3][5][NB] gradients then contravariant fluxes
+//   faces   Fa[FPP][5][NQF] Fb[FPP][12][NQF] Gt[FPP][9][NQF]
+//   norm    Y0[5NB] Y1[5NB] (nodal residual for the printed norm), red[NTS] (FP64)
+//   traces  sN[FPP][10][NQF], then the new state at oTrU
+template <int P, class T>
+struct VStageSmem {
+  using C = Cfg<P>;
+  static constexpr int NB = C::NB, NQF = C::NQF;
+  static constexpr int ST = (int)sizeof(T);
+  static constexpr int oOps = 0;
+  static constexpr int oGeo = align16(C::OPS * ST);
+  static constexpr int oX = oGeo + align16(kGeoStride * ST);
+  static constexpr int VOL = 20 * NB * ST;
+  static constexpr int FACE = C::FPP * (5 + 12 + 9) * NQF * ST;
+  static constexpr int oRed = align16(10 * NB * ST);
+  static constexpr int NORM = oRed + C::NTS * 8;
+  static constexpr int oTrU = align16(10 * C::FPP * NQF * ST);
+  static constexpr int TRACE = oTrU + 5 * NB * ST;
+  static constexpr int X0 = VOL > FACE ? VOL : FACE;
+  static constexpr int X1 = NORM > TRACE ? NORM : TRACE;
+  static constexpr int X = X0 > X1 ? X0 : X1;
+  static constexpr int TOTAL = oX + align16(X);
+};
+
+template <int P, class T>
+struct VTraceSmem {
+  using C = Cfg<P>;
+  static constexpr int ST = (int)sizeof(T);
+  static constexpr int oOps = 0;
+  static constexpr int oGeo = align16(C::OPS * ST);
+  static constexpr int oU = oGeo + align16(kGeoStride * ST);
+  static constexpr int oN = oU + align16(5 * C::NB * ST);
+  static constexpr int TOTAL = oN + align16(10 * C::FPP * C::NQF * ST);
+};
+
+// Traces of a Gauss-point state sV[5][NB] (shared memory) on the FPP faces
+// lf = FPP*half + j, into Te (this element's slice of the trace buffer), in
+// the trace format of trace_half.  Scratch sN[FPP][10][NQF].
+template <int P, class T, bool CV>
+__device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const T* so, const T* sg, T mu, T kq,
+                                            T* __restrict__ Te, const double* __restrict__ gfe)
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
+  const int tid = threadIdx.x;
+  if (tid < NH) {  // along the normal line: value and normal derivative at the face point
+    const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P;
+    const int a = lf >> 1, end = lf & 1;
+    const T* Ev = so + C::oEh + end * P;
+    const T* Dv = so + C::oDh + end * P;
+    T* out = sN + j * 10 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      T v = T(0), dn = T(0);
+#pragma unroll
+      for (int qa = 0; qa < P; ++qa) {
+        const T u = sV[r * NB + face_node<P>(a, qa, t1, t2)];
+        v = fma(Ev[qa], u, v);
+        dn = fma(Dv[qa], u, dn);
+      }
+      out[r * NQF + fq] = v;
+      out[(5 + r) * NQF + fq] = dn;
+    }
+  }
+  __syncthreads();
+  if (tid < NH) {  // tangential derivatives on the face, then the viscous normal flux
+    const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+    const T* in = sN + j * 10 * NQF;
+    const T* Dq = so + C::oDq;
+    T S[5], g[3][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      T d1 = T(0), d2 = T(0);
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        d1 = fma(Dq[q1 * P + k], in[r * NQF + k + P * q2], d1);
+        d2 = fma(Dq[q2 * P + k], in[r * NQF + q1 + P * k], d2);
+      }
+      const T dn = in[(5 + r) * NQF + fq];
+      S[r] = in[r * NQF + fq];
+      g[0][r] = a == 0 ? dn : d1;
+      g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
+      g[2][r] = a == 2 ? dn : d2;
+    }
+    trace_point_store<P, T, CV>(lf, fq, S, g, sg, gfe, mu, kq, Te);
+  }
+}
+
+// Face traces of a Gauss-point state V (FP64 in HBM) into Tr[e][lf][10][P*P].
+template <int P, class T, bool CV, bool HT>
+__global__ void __launch_bounds__(Cfg<P>::NTS)
+vtrace_kernel(long E, const double* __restrict__ V, const T* __restrict__ opsg, const double* __restrict__ geo,
+              const double* __restrict__ gf, T* __restrict__ Tr, DevParams prm)
+{
+  using C = Cfg<P>;
+  using L = VTraceSmem<P, T>;
+  constexpr int NB = C::NB, NQF = C::NQF;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw + L::oOps);
+  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
+  T* sV = reinterpret_cast<T*>(smraw + L::oU);
+  T* sN = reinterpret_cast<T*>(smraw + L::oN);
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
+  const double* Ve = V + e * 5 * NB;
+  for (int i = tid; i < 5 * NB; i += blockDim.x) sV[i] = T(Ve[i]);
+  __syncthreads();
+  T* Te = Tr + e * 60 * NQF;
+#pragma unroll 1
+  for (int half = 0; half < 6 / C::FPP; ++half) {
+    if (half) __syncthreads();
+    vtrace_half<P, T, CV>(half, sV, sN, so, sg, T(prm.mu), HT ? T(prm.kq) : T(0), Te,
+                          CV ? gf + e * 6 * kFaceC * NQF : nullptr);
+  }
+}
+
+// The RK stage value of one entry (time_distributed.cpp:46-102, stage 3 of
+// RK4 with dt as the reference's CPU solver): updates the accumulator and
+// returns the new stage state.  ue: the stage input state at this entry.
+__device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, double fr, double ue)
+{
+  const double dt = sa.dt;
+  double un = 0.;
+  switch (sa.mode) {
+    case MODE_RK4_0:
+      sa.acc[i] = fr;
+      un = sa.Ubase[i] + dt * fr * 0.5;
+      break;
+    case MODE_RK4_1:
+      sa.acc[i] = sa.acc[i] + 2. * fr;
+      un = sa.Ubase[i] + dt * fr * 0.5;
+      break;
+    case MODE_RK4_2:
+      sa.acc[i] = sa.acc[i] + 2. * fr;
+      un = sa.Ubase[i] + dt * fr;
+      break;
+    case MODE_RK4_3:
+      un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
+      break;
+    case MODE_TVD_0:
+      un = sa.Ubase[i] + dt * fr;
+      break;
+    case MODE_TVD_1:
+      un = 0.75 * sa.Ubase[i] + 0.25 * ue + 0.25 * dt * fr;
+      break;
+    case MODE_TVD_2:
+      un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * ue + (2. / 3.) * dt * fr;
+      break;
+  }
+  return un;
+}
+
+// One RK stage on Gauss-point states: Vs (stage input), sa.Ubase / sa.acc /
+// sa.Uout are Gauss-point arrays, Tr the traces of Vs; sa.mode is an RK mode
+// (MODE_RESIDUAL writes f_V to sa.fout).  sa.part gets the element's sum of
+// the squared nodal residual, the reference's printed norm.
+template <int P, class T, bool CV, bool HT>
+__global__ void __launch_bounds__(Cfg<P>::NTS, (MinBlocks<P, T>::value))
+vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
+              const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
+              const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm, StageArgs sa)
+{
+  using C = Cfg<P>;
+  using L = VStageSmem<P, T>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw + L::oOps);
+  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
+  unsigned char* sXb = smraw + L::oX;
+  T* sX = reinterpret_cast<T*>(sXb);
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  const bool node = tid < NB;  // thread owns Gauss point `tid`
+  const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+
+  T* V1 = sX;
+  T* G = sX + 5 * NB;
+  if (DGB_PREFETCH_L2 && sizeof(T) == 8) {  // data of the face phase and the RK update, read much later
+    const int nt = blockDim.x;
+    prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), tid, nt);
+    if (tid < 6) {
+      const int nb = nbr[e * 6 + tid];
+      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (tid ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
+    }
+    if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, tid, nt);
+    if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
+      prefetch_range(sa.acc + e * 5 * NB, 40L * NB, tid, nt);
+  }
+  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
+  const double* Ve = Vs + e * 5 * NB;
+  for (int i = tid; i < 5 * NB; i += blockDim.x) V1[i] = T(Ve[i]);
+  __syncthreads();
+
+  const T* Dq = so + C::oDq;
+  const double detJd = geo[e * kGeoStride + kGeoDetJ];
+  const T detJ = sg[kGeoDetJ];
+  const T* Ji = sg + kGeoJinv;
+  const T gamma = T(prm.gamma), mu = T(prm.mu), kq = HT ? T(prm.kq) : T(0);
+  T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // Y = B3^-T R at Gauss point tid
+  const double* gve = CV ? gv + e * kVolC * NB : nullptr;
+  const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
+
+  // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
+  if (node) {  // reference gradients at the Gauss points
+    contract<P, 0, false, false>(Dq, V1, G, tid);
+    contract<P, 1, false, false>(Dq, V1, G + 5 * NB, tid);
+    contract<P, 2, false, false>(Dq, V1, G + 10 * NB, tid);
+  }
+  __syncthreads();
+  T wJq = T(0);
+  if (node) {  // pointwise flux at Gauss point tid
+    const T* w = so + C::oW;
+    T Jbuf[9];
+    if constexpr (CV) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) Jbuf[c] = T(gve[c * NB + tid]);
+      wJq = w[qx] * w[qy] * w[qz] * T(gve[kVolDetJ * NB + tid]);
+    } else {
+      wJq = w[qx] * w[qy] * w[qz] * detJ;
+    }
+    const T* Jq = CV ? Jbuf : Ji;
+    T S[5], Gp[3][5], H[3][5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      S[r] = V1[r * NB + tid];
+      const T g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Gp[c][r] = Jq[c] * g0 + Jq[3 + c] * g1 + Jq[6 + c] * g2;
+    }
+    euler_flux(S, gamma, H);
+    if (mu != T(0)) {
+      T Q[3][5];
+      visc_flux(S, Gp, mu, Q, kq);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+        G[i * 5 * NB + r * NB + tid] = wJq * (Jq[3 * i] * H[0][r] + Jq[3 * i + 1] * H[1][r] + Jq[3 * i + 2] * H[2][r]);
+  }
+  __syncthreads();
+  if (node) {  // Y = sum_i Dq_i^T Ghat_i, minus the source tested with w detJ
+    T y[5];
+    contract_reg<P, 0, true>(Dq, G, tid, Rv);
+    contract_reg<P, 1, true>(Dq, G + 5 * NB, tid, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Rv[r] += y[r];
+    contract_reg<P, 2, true>(Dq, G + 10 * NB, tid, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Rv[r] = Rv[r] + y[r] - T(prm.src[r]) * wJq;
+  }
+  __syncthreads();
+
+  // ---------------- faces (solve.cpp:393-794), FPP at a time
+  T* Fa = sX;                    // [FPP][5][NQF]
+  T* Fb = Fa + FPP * 5 * NQF;    // [FPP][12][NQF]
+  T* Gt = Fb + FPP * 12 * NQF;   // [FPP][9][NQF]
+#pragma unroll 1
+  for (int half = 0; half < 6 / FPP; ++half) {
+    if (tid < NH) {
+      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF;
+      face_point_fluxes<P, T, CV>(e, lf, fq, Tr, nbr, so, sg, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag,
+                                  Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
+    }
+    __syncthreads();
+    if (tid < NH) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
+      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
+      const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+      const T* fa = Fa + j * 5 * NQF;
+      const T* fb = Fb + j * 12 * NQF;
+      T* gt = Gt + j * 9 * NQF;
+      gt[fq] = fa[fq];
+#pragma unroll
+      for (int r = 1; r < 5; ++r) {
+        T s = fa[r * NQF + fq];
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          s = fma(Dq[k * P + t1], fb[(ax1 * 4 + r - 1) * NQF + k + P * t2], s);
+          s = fma(Dq[k * P + t2], fb[(ax2 * 4 + r - 1) * NQF + t1 + P * k], s);
+        }
+        gt[r * NQF + fq] = s;
+        gt[(4 + r) * NQF + fq] = fb[(a * 4 + r - 1) * NQF + fq];
+      }
+    }
+    __syncthreads();
+    if (node) {  // each Gauss point gathers from the face points on its normal lines
+      const T* Ev = so + C::oEh;
+      const T* Dv = so + C::oDh;
+#pragma unroll
+      for (int j = 0; j < FPP; ++j) {
+        const int lf = FPP * half + j, a = lf >> 1, end = lf & 1;
+        const int qa = a == 0 ? qx : a == 1 ? qy : qz;
+        const int t1 = a == 0 ? qy : qx, t2 = a == 2 ? qy : qz;
+        const T ev = Ev[end * P + qa], dv = Dv[end * P + qa];
+        const T* gt = Gt + j * 9 * NQF + t1 + P * t2;
+        Rv[0] += ev * gt[0];
+#pragma unroll
+        for (int r = 1; r < 5; ++r) Rv[r] += ev * gt[r * NQF] + dv * gt[(4 + r) * NQF];
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---------------- norm partial: the nodal residual R = B3^T Y
+  if (sa.part) {
+    const T* B = so + C::oB;
+    T* Y0 = sX;
+    T* Y1 = sX + 5 * NB;
+    if (node) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Y0[r * NB + tid] = Rv[r];
+    }
+    __syncthreads();
+    if (node) contract<P, 0, true, false>(B, Y0, Y1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, true, false>(B, Y1, Y0, tid);
+    __syncthreads();
+    double s = 0.;
+    if (node) {
+      T rn[5];
+      contract_reg<P, 2, true>(B, Y0, tid, rn);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) s += double(rn[r]) * double(rn[r]);
+    }
+    double* red = reinterpret_cast<double*>(sXb + L::oRed);
+    red[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.;
+      for (int i = 0; i < C::NTS; ++i) t += red[i];
+      sa.part[e] = t;
+    }
+    __syncthreads();
+  }
+
+  // ---------------- f_V = -Y / (w detJ) in FP64, RK update
+  T* sVn = reinterpret_cast<T*>(sXb + L::oTrU);  // new state for the epilogue traces
+  if (node) {
+    const double* w = opsd + C::oW;
+    const double jd = CV ? gve[kVolDetJ * NB + tid] : detJd;
+    const double sc = -1.0 / (w[qx] * w[qy] * w[qz] * jd);
+    const long base = e * 5 * NB;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const long i = base + r * NB + tid;
+      const double fr = double(Rv[r]) * sc;
+      if (sa.mode == MODE_RESIDUAL) {
+        sa.fout[i] = fr;
+      } else {
+        const double un = rk_stage_value(sa, i, fr, Ve[r * NB + tid]);
+        sa.Uout[i] = un;
+        sVn[r * NB + tid] = T(un);
+      }
+    }
+  }
+  // ---------------- face traces of the new state for the next stage
+  if (sa.Tnext) {
+    __syncthreads();
+    T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
+#pragma unroll 1
+    for (int half = 0; half < 6 / FPP; ++half) {
+      if (half) __syncthreads();
+      vtrace_half<P, T, CV>(half, sVn, sX, so, sg, mu, kq, Te, gfe);
+    }
+  }
+}
+
+// V = (B x B x B) U (to_gauss) or U = (B^-1 x B^-1 x B^-1) V (from_gauss),
+// per element, FP64: the basis change at the edges of dgb_step.
+template <int P, bool TO>
+__global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const double* __restrict__ in,
+                                                                 double* __restrict__ out,
+                                                                 const double* __restrict__ opsd)
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB;
+  __shared__ __align__(16) double sm[2 * P * P + 10 * NB];
+  double* M = sm;  // B or B^-1
+  double* A = sm + 2 * P * P;
+  double* Bf = A + 5 * NB;
+  const long e = blockIdx.x;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < P * P; i += blockDim.x) M[i] = opsd[(TO ? C::oB : C::oBi) + i];
+  for (int i = tid; i < 5 * NB; i += blockDim.x) A[i] = in[e * 5 * NB + i];
+  __syncthreads();
+  if (tid < NB) contract<P, 0, false, false>(M, A, Bf, tid);
+  __syncthreads();
+  if (tid < NB) contract<P, 1, false, false>(M, Bf, A, tid);
+  __syncthreads();
+  if (tid < NB) {
+    double v[5];
+    contract_reg<P, 2, false>(M, A, tid, v);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) out[e * 5 * NB + r * NB + tid] = v[r];
+  }
+}
+
+// ------------------------------------------------------------ host launchers
+
+template <int P, class T, bool HT>
+cudaError_t vprepare_p()
+{
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vtrace_kernel<P, T, false, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             VTraceSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vtrace_kernel<P, T, true, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             VTraceSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vstage_kernel<P, T, false, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             VStageSmem<P, T>::TOTAL);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vstage_kernel<P, T, true, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             VStageSmem<P, T>::TOTAL);
+  return e;
+}
+
+template <int P, class T, bool HT>
+cudaError_t vlaunch_trace_p(const KLaunch& L, const double* V, void* Tout, cudaStream_t st)
+{
+  if (L.gf)
+    vtrace_kernel<P, T, true, HT><<<(unsigned)L.E, Cfg<P>::NTS, VTraceSmem<P, T>::TOTAL, st>>>(
+        L.E, V, reinterpret_cast<const T*>(L.ops), L.geo, L.gf, reinterpret_cast<T*>(Tout), L.prm);
+  else
+    vtrace_kernel<P, T, false, HT><<<(unsigned)L.E, Cfg<P>::NTS, VTraceSmem<P, T>::TOTAL, st>>>(
+        L.E, V, reinterpret_cast<const T*>(L.ops), L.geo, nullptr, reinterpret_cast<T*>(Tout), L.prm);
+  return cudaGetLastError();
+}
+
+template <int P, class T, bool HT>
+cudaError_t vlaunch_stage_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                            cudaStream_t st)
+{
+  if (L.gv)
+    vstage_kernel<P, T, true, HT><<<(unsigned)L.E, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
+        L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
+        L.nbr, L.prm, sa);
+  else
+    vstage_kernel<P, T, false, HT><<<(unsigned)L.E, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
+        L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
+        nullptr, L.nbr, L.prm, sa);
+  return cudaGetLastError();
+}
+
+template <class T, bool HT>
+cudaError_t vprepare_t(int P)
+{
+  switch (P) {
+    case 1: return vprepare_p<1, T, HT>();
+    case 2: return vprepare_p<2, T, HT>();
+    case 3: return vprepare_p<3, T, HT>();
+    case 4: return vprepare_p<4, T, HT>();
+    case 5: return vprepare_p<5, T, HT>();
+    case 6: return vprepare_p<6, T, HT>();
+    case 7: return vprepare_p<7, T, HT>();
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class T, bool HT>
+cudaError_t vlaunch_trace_t(const KLaunch& L, const double* V, void* Tout, cudaStream_t st)
+{
+  switch (L.P) {
+    case 1: return vlaunch_trace_p<1, T, HT>(L, V, Tout, st);
+    case 2: return vlaunch_trace_p<2, T, HT>(L, V, Tout, st);
+    case 3: return vlaunch_trace_p<3, T, HT>(L, V, Tout, st);
+    case 4: return vlaunch_trace_p<4, T, HT>(L, V, Tout, st);
+    case 5: return vlaunch_trace_p<5, T, HT>(L, V, Tout, st);
+    case 6: return vlaunch_trace_p<6, T, HT>(L, V, Tout, st);
+    case 7: return vlaunch_trace_p<7, T, HT>(L, V, Tout, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class T, bool HT>
+cudaError_t vlaunch_stage_t(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                            cudaStream_t st)
+{
+  switch (L.P) {
+    case 1: return vlaunch_stage_p<1, T, HT>(L, Vs, Tin, sa, st);
+    case 2: return vlaunch_stage_p<2, T, HT>(L, Vs, Tin, sa, st);
+    case 3: return vlaunch_stage_p<3, T, HT>(L, Vs, Tin, sa, st);
+    case 4: return vlaunch_stage_p<4, T, HT>(L, Vs, Tin, sa, st);
+    case 5: return vlaunch_stage_p<5, T, HT>(L, Vs, Tin, sa, st);
+    case 6: return vlaunch_stage_p<6, T, HT>(L, Vs, Tin, sa, st);
+    case 7: return vlaunch_stage_p<7, T, HT>(L, Vs, Tin, sa, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace dgb

@@ -158,8 +158,21 @@ int dgb_set_mean(dgb_handle* h, const double* mean_host);
 int dgb_get_mean(dgb_handle* h, double* mean_host);
 
 /* Device pointer of the handle's resident state (for callers that keep data
- * on the GPU). */
+ * on the GPU).  Writes through it count from the next dgb_step on: the
+ * handle drops its Gauss-point copy of the state when it hands it out. */
 int dgb_state_device_ptr(dgb_handle* h, double** U_dev);
+
+/* The form dgb_step computes in.  DGB_STEP_GAUSS (the default) keeps the
+ * state at the (p+1)^3 Gauss points of each element while it steps, V = (B x
+ * B x B) U, where the mass matrix is diagonal and the interpolations to and
+ * from the Gauss points drop out; it converts U -> V before its first step
+ * and V -> U after its last (and continues from V across calls while the
+ * state is not set otherwise, so a run split into calls is the same run).
+ * DGB_STEP_NODAL steps the nodal coefficients, with the kernels the recorded
+ * runs of the adjoint (dgb_forward_record) use.  Both are the reference's
+ * discretisation; they agree to rounding. */
+enum { DGB_STEP_GAUSS = 0, DGB_STEP_NODAL = 1 };
+int dgb_set_step_form(dgb_handle* h, int form);
 
 /* One residual evaluation of U: R = un-inverted residual (may be NULL) and
  * f = dU/dt = -Minv R.  Host pointers; copies in and out.

@@ -43,14 +43,19 @@ def test_residual_matches_oracle_and_reference(case):
     assert rel(f, GOLD[f"{case.name}/f"]) < 1e-11
 
 
+@pytest.mark.parametrize("form", [dg.STEP_GAUSS, dg.STEP_NODAL], ids=["gauss", "nodal"])
 @pytest.mark.parametrize("case", C.run_cases(), ids=lambda c: c.name)
-def test_time_steps_match_reference(case):
+def test_time_steps_match_reference(case, form):
+    """dgb_step in both forms (Gauss-point state, the default, and nodal)."""
     with solver(case) as s:
+        s.set_step_form(form)
         s.set_state(case.U)
         norms = s.step(case.scheme, case.dt, case.nsteps)
         U = s.get_state()
-        # one trace launch per call, then per step the stages and the norm
-        assert s.last_launch_count == 1 + case.nsteps * (5 if case.scheme == dg.RK4 else 4)
+        # one trace launch per call, then per step the stages and the norm;
+        # the Gauss-point form converts the state in and out
+        extra = 2 if form == dg.STEP_GAUSS else 0
+        assert s.last_launch_count == 1 + case.nsteps * (5 if case.scheme == dg.RK4 else 4) + extra
     assert rel(U, GOLD[f"{case.name}/UN"]) < 1e-12, rel(U, GOLD[f"{case.name}/UN"])
     assert rel(norms, GOLD[f"{case.name}/norms"]) < 1e-10
     Uo, no = oracle.restatement().run(oracle.Mesh(case.nx, case.ny, case.nz, case.p, case.q, case.nodes,
@@ -59,18 +64,48 @@ def test_time_steps_match_reference(case):
     assert rel(norms, no) < 1e-10
 
 
-def test_steps_split_equal_steps_joined():
-    """nsteps in one call equals the same steps in several calls, bit for bit."""
+@pytest.mark.parametrize("form", [dg.STEP_GAUSS, dg.STEP_NODAL], ids=["gauss", "nodal"])
+def test_steps_split_equal_steps_joined(form):
+    """nsteps in one call equals the same steps in several calls, bit for bit
+    (the Gauss-point form continues from its own copy of the state between
+    calls; get_state in between does not disturb it)."""
     c = C.run_cases()[1]
     with solver(c) as s:
+        s.set_step_form(form)
         s.set_state(c.U)
         s.step(c.scheme, c.dt, 4)
         U1 = s.get_state()
         s.set_state(c.U)
         for _ in range(4):
             s.step(c.scheme, c.dt, 1)
+            s.get_state()
         U2 = s.get_state()
     assert np.array_equal(U1, U2)
+
+
+def test_step_forms_agree_and_state_writes_are_seen():
+    """The Gauss-point and the nodal form are the same discretisation: they
+    agree to rounding over 10 steps of every run case.  A state set between
+    Gauss-point calls (host or device) is the one stepped."""
+    for c in C.run_cases():
+        out = {}
+        for form in (dg.STEP_GAUSS, dg.STEP_NODAL):
+            with solver(c) as s:
+                s.set_step_form(form)
+                s.set_state(c.U)
+                s.step(c.scheme, c.dt, 10)
+                out[form] = s.get_state()
+        assert rel(out[dg.STEP_GAUSS], out[dg.STEP_NODAL]) < 1e-13, (c.name, rel(out[dg.STEP_GAUSS], out[dg.STEP_NODAL]))
+    c = C.run_cases()[1]
+    with solver(c) as s:
+        s.set_state(c.U)
+        s.step(c.scheme, c.dt, 2)
+        s.set_state(c.U)  # back to the start
+        s.step(c.scheme, c.dt, 2)
+        a = s.get_state()
+        s.set_state(c.U)
+        s.step(c.scheme, c.dt, 2)
+        assert np.array_equal(s.get_state(), a)
 
 
 def test_residual_is_deterministic_and_device_api_matches_host_api():
