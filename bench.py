@@ -523,8 +523,15 @@ def run_ours(args, rank, world, local_rank):
         with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as sa:
             sa.set_stream(stream.cuda_stream)
             rev_ms, rev_launches = _reverse_step_ms(dg, torch, sa, stream, U0, dt, reps)
+            # the forward step the reverse step undoes: the recorded runs step
+            # the nodal form
+            sa.set_step_form(dg.STEP_NODAL)
+            sa.set_state(U0)
+            _warm(dg, torch, sa, dt, 3)
+            nodal_ms = _timed_steps(dg, torch, sa, stream, dt, min(args.steps, 20)) / min(args.steps, 20)
         adj = {"reverse_step_ms": rev_ms, "forward_step_ms": ms / args.steps,
-               "reverse_over_forward": rev_ms / (ms / args.steps), "reverse_step_launches": rev_launches,
+               "reverse_over_forward": rev_ms / (ms / args.steps), "forward_step_nodal_ms": nodal_ms,
+               "reverse_over_nodal_forward": rev_ms / nodal_ms, "reverse_step_launches": rev_launches,
                "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
     curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
@@ -565,7 +572,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "stage_kernel<4,double>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
+                         "kernel": "vstage_kernel<4,double>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
                          "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
                          if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
             "mixed": {"value": value_mixed, "unit": UNIT, "ms_per_step": ms_mixed / args.steps,
