@@ -40,5 +40,14 @@ cudaError_t launch_residual_vjp(const KLaunch& L, const VjpArgs& v, const VjpScr
 // the heat-conducting kernels (adjoint_heat.cu); launch_residual_vjp picks them when L.prm.kq != 0
 cudaError_t prepare_adjoint_heat(int P);
 cudaError_t launch_residual_vjp_heat(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
+// The Gauss-point form (U, lam and the result at the Gauss points: the VJP of
+// f_V, vspace.cuh), for the reverse steps of recorded runs in that form
+// (adjoint_gauss.cu, adjoint_gauss_heat.cu); prepared by prepare_adjoint
+cudaError_t launch_residual_vjp_gauss(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
+cudaError_t prepare_adjoint_gauss(int P);
+cudaError_t prepare_adj_t_gauss_heat(int P);
+cudaError_t launch_vjp_gauss_plain(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st);
+cudaError_t launch_residual_vjp_gauss_heat(const KLaunch& L, const VjpArgs& v, const VjpScratch& s,
+                                           cudaStream_t st);
 
 }  // namespace dgb

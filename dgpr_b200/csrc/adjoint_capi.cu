@@ -23,6 +23,8 @@ namespace {
 
 int fail(int code, const char* msg) { return set_last_error(code, msg); }
 
+int cuda_status_rc(cudaError_t e) { return e == cudaSuccess ? DGB_OK : cuda_status(e, "basis change"); }
+
 // every boundary type has an adjoint (physics_vjp.cuh); kept as the hook for
 // inputs the adjoint does not cover
 int check_bounds(const dgb_handle*) { return DGB_OK; }
@@ -146,7 +148,7 @@ int ensure_pgrad(dgb_handle* h)
 // v.Y in place), added into dpar.  f is affine in mu (the viscous flux and
 // the heat flux at fixed Pr are linear in it), so df/dmu = (f(mu1) - f(0)) /
 // mu1, both FP64 residuals of v.U; df/dsource[r] = 1 on variable r.
-int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar)
+int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar, bool gauss)
 {
   KLaunch L = klaunch(h);
   L.precision = DGB_FP64;
@@ -166,12 +168,17 @@ int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar)
   double* part = trp + (size_t)h->E * 60 * h->NQF;
   const KLaunch* Ls[2] = {&L1, &L0};
   double* Fs[2] = {F1, F0};
-  for (int k = 0; k < 2; ++k) {
-    CK(launch_trace(*Ls[k], v.U, trp, h->stream));
+  for (int k = 0; k < 2; ++k) {  // f (or f_V in the Gauss-point form: df_V/dsource is 1 as well)
     StageArgs a = stage_args(MODE_RESIDUAL, 0.);
     a.fout = Fs[k];
     a.flag = h->d_flag;
-    CK(launch_stage(*Ls[k], v.U, trp, a, h->stream));
+    if (gauss) {
+      CK(launch_vtrace(*Ls[k], v.U, trp, h->stream));
+      CK(launch_vstage(*Ls[k], v.U, trp, a, h->stream));
+    } else {
+      CK(launch_trace(*Ls[k], v.U, trp, h->stream));
+      CK(launch_stage(*Ls[k], v.U, trp, a, h->stream));
+    }
   }
   param_dot_kernel<<<(unsigned)h->E, 128, 0, h->stream>>>(h->E, h->NB, v, F1, F0, 1. / mu1, part);
   CK(cudaGetLastError());
@@ -199,10 +206,16 @@ int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar)
 // rotating trace buffers and each VJP takes its own FP64 traces.
 // With `stored` (the recorded stage states of this step) nothing is
 // recomputed: an FP64 handle takes the traces of the stored states.
+// gauss: Ui, lam, the stage states and the result are Gauss-point arrays
+// (the Gauss-point form of vspace.cuh, with its stage, trace and VJP
+// kernels), else nodal.
 int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui, double* lam, long long* nl,
-                         double* const* stored = nullptr, double* dpar = nullptr)
+                         double* const* stored = nullptr, double* dpar = nullptr, bool gauss = false)
 {
   const KLaunch L = klaunch(h);
+  auto trace = [&](const double* U, void* Tout) {
+    return gauss ? launch_vtrace(L, U, Tout, h->stream) : launch_trace(L, U, Tout, h->stream);
+  };
   double* S[3] = {h->d_adj[dgb_handle::ADJ_S0], h->d_adj[dgb_handle::ADJ_S1], h->d_adj[dgb_handle::ADJ_S2]};
   if (stored)
     for (int s = 0; s < 3; ++s) S[s] = stored[s];
@@ -213,7 +226,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   const bool f64 = h->precision == DGB_FP64;
   void* const* T = h->d_trace;
   void* TU = f64 ? (void*)h->d_adj_tr : T[0];
-  if (f64 || !stored) CK(launch_trace(L, Ui, TU, h->stream));
+  if (f64 || !stored) CK(trace(Ui, TU));
   const int nst = scheme == DGB_RK4 ? 3 : 2;  // recomputed stage states
   const int rk4[3] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2}, tvd[2] = {MODE_TVD_0, MODE_TVD_1};
   // trace buffers read / written by the recomputed stages
@@ -224,7 +237,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   if (scheme != DGB_RK4) tout_mix[1] = nullptr;
   for (int s = 0; s < nst; ++s) {
     if (stored) {  // the stage state is at hand; an FP64 handle still needs its traces
-      if (f64) CK(launch_trace(L, S[s], tout_f64[s], h->stream));
+      if (f64) CK(trace(S[s], tout_f64[s]));
       continue;
     }
     StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[s] : tvd[s], dt);
@@ -233,21 +246,27 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     a.Uout = S[s];
     a.flag = h->d_flag;
     a.Tnext = f64 ? tout_f64[s] : tout_mix[s];
-    CK(launch_stage(L, s == 0 ? Ui : S[s - 1], f64 ? tin_f64[s] : tin_mix[s], a, h->stream));
+    if (gauss)
+      CK(launch_vstage(L, s == 0 ? Ui : S[s - 1], f64 ? tin_f64[s] : tin_mix[s], a, h->stream));
+    else
+      CK(launch_stage(L, s == 0 ? Ui : S[s - 1], f64 ? tin_f64[s] : tin_mix[s], a, h->stream));
   }
   auto tr = [&](int s) -> const double* {  // FP64 traces of stage state s (-1: U_i)
     if (!f64) return nullptr;
     return (const double*)(s < 0 ? TU : tout_f64[s]);
   };
   int rc;
+  auto vjp_launch = [&](const VjpArgs& w) {
+    return gauss ? launch_residual_vjp_gauss(L, w, sc, h->stream) : launch_residual_vjp(L, w, sc, h->stream);
+  };
   auto run_vjp = [&](const VjpArgs& w) -> int {
     if (!dpar) {
-      CK(launch_residual_vjp(L, w, sc, h->stream));
+      CK(vjp_launch(w));
       return DGB_OK;
     }
-    const int r = enqueue_param_terms(h, w, dpar);
+    const int r = enqueue_param_terms(h, w, dpar, gauss);
     if (r) return r;
-    CK(launch_residual_vjp(L, w, sc, h->stream));
+    CK(vjp_launch(w));
     if (h->isothermal) {  // the VJP left the isothermal walls' dJ/dTw terms in its trace adjoints
       wall_terms_kernel<<<1, 256, 0, h->stream>>>(h->E, h->NQF, h->d_nbr, sc.ta, dpar + DGB_DPARAM_TWALL);
       CK(cudaGetLastError());
@@ -300,16 +319,17 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
 
 // The captured graph of one reverse step of the work state d_U with the
 // adjoint in ADJ_LAM (the backward sweep's REVERSE operation).
-int ensure_rev_graph(dgb_handle* h, int scheme, double dt)
+int ensure_rev_graph(dgb_handle* h, int scheme, double dt, bool gauss)
 {
-  if (h->rev_graph && h->rev_scheme == scheme && h->rev_dt == dt) return DGB_OK;
+  if (h->rev_graph && h->rev_scheme == scheme && h->rev_dt == dt && h->rev_gauss == gauss) return DGB_OK;
   if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
   h->rev_graph = nullptr;
   h->rev_scheme = -1;
   cudaGraph_t g;
   long long nl = 0;
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_reverse_step(h, scheme, dt, h->d_U, h->d_adj[dgb_handle::ADJ_LAM], &nl);
+  int rc = enqueue_reverse_step(h, scheme, dt, gauss ? h->d_V : h->d_U, h->d_adj[dgb_handle::ADJ_LAM], &nl,
+                                nullptr, nullptr, gauss);
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
   if (rc) return rc;
   if (ce != cudaSuccess) return cuda_status(ce, "cudaStreamEndCapture");
@@ -318,6 +338,7 @@ int ensure_rev_graph(dgb_handle* h, int scheme, double dt)
   if (ce != cudaSuccess) return cuda_status(ce, "cudaGraphInstantiate");
   h->rev_scheme = scheme;
   h->rev_dt = dt;
+  h->rev_gauss = gauss;
   h->rev_launches = nl;
   return DGB_OK;
 }
@@ -423,7 +444,18 @@ int dgb_step_vjp_device(dgb_handle* h, int scheme, double dt, const double* U_de
     if (U_dev == h->d_adj[b] || lam_dev == h->d_adj[b]) return fail(DGB_ERR_ARG, "argument aliases scratch");
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   long long nl = 0;
-  if ((rc = enqueue_reverse_step(h, scheme, dt, U_dev, lam_dev, &nl))) return rc;
+  if (h->gauss_step) {  // the VJP of dgb_step's map U -> B3^-1 Phi_V(B3 U)
+    const KLaunch L = klaunch(h);
+    double* V = h->d_adj[dgb_handle::ADJ_IN];
+    double* lamV = h->d_adj[dgb_handle::ADJ_OUT];
+    CK(launch_gauss_basis_mode(L, U_dev, V, GB_TO_GAUSS, h->stream));
+    CK(launch_gauss_basis_mode(L, lam_dev, lamV, GB_ADJ_TO_GAUSS, h->stream));
+    if ((rc = enqueue_reverse_step(h, scheme, dt, V, lamV, &nl, nullptr, nullptr, true))) return rc;
+    CK(launch_gauss_basis_mode(L, lamV, lam_dev, GB_ADJ_TO_NODAL, h->stream));
+    nl += 3;
+  } else {
+    if ((rc = enqueue_reverse_step(h, scheme, dt, U_dev, lam_dev, &nl))) return rc;
+  }
   h->last_launches = nl;
   return read_flag(h);
 }
@@ -432,7 +464,6 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
                        double* norms_host)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
-  h->v_current = false;  // the recorded run steps the nodal state d_U
   int rc = check_scheme(scheme, dt);
   if (rc) return rc;
   if (nsteps < 1 || slots < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1 and slots >= 1");
@@ -451,9 +482,13 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
     CK(cudaMalloc(&p, sizeof(double) * (size_t)h->n));
     h->d_slots.push_back(p);
   }
-  if ((rc = ensure_step_graph(h, scheme, dt, nsteps))) return rc;
+  // the run steps in dgb_step's form: on d_V (Gauss points) or on d_U
+  const bool gauss = h->gauss_step;
+  double* Ures = gauss ? h->d_V : h->d_U;
+  if ((rc = ensure_step_graph(h, scheme, dt, nsteps, gauss))) return rc;
   CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  if (gauss && !h->v_current) CK(launch_gauss_basis(klaunch(h), h->d_U, h->d_V, true, h->stream));
   // Between graph replays the face traces of the resident state stay valid
   // (each step's last stage writes them), and storing a checkpoint does not
   // change the state: only the first replay needs the trace kernel.
@@ -462,9 +497,9 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
   for (size_t k = 0; k < h->plan.first_reverse; ++k) {
     const CkOp& op = h->plan.ops[k];
     if (op.kind == CK_STORE) {
-      if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+      if ((rc = copy_state(h, h->d_slots[op.arg], Ures))) return rc;
     } else if (op.kind == CK_FORWARD) {
-      if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace))) return rc;
+      if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace, gauss))) return rc;
       launches += (need_trace ? 1 : 0) + op.arg * h->launches_per_step;
       need_trace = false;
     } else {
@@ -472,10 +507,12 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
     }
   }
   // work state is U_{N-1}: keep it, take the last step on the resident state
-  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_WORK], h->d_U))) return rc;
-  if ((rc = enqueue_steps(h, 1, need_trace))) return rc;
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_WORK], Ures))) return rc;
+  if ((rc = enqueue_steps(h, 1, need_trace, gauss))) return rc;
   launches += (need_trace ? 1 : 0) + h->launches_per_step;
-  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], h->d_U))) return rc;
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], Ures))) return rc;
+  if (gauss) CK(launch_gauss_basis(klaunch(h), h->d_V, h->d_U, false, h->stream));
+  h->v_current = gauss;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (norms_host)
@@ -486,6 +523,7 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
   h->plan_pos = h->plan.first_reverse;
   h->recorded = true;
   h->rec_stages = false;
+  h->rec_gauss = gauss;
   h->slots_dirty = false;
   h->rec_scheme = scheme;
   h->rec_dt = dt;
@@ -497,7 +535,6 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
 int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, double* norms_host)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
-  h->v_current = false;  // the recorded run steps the nodal state d_U
   int rc = check_scheme(scheme, dt);
   if (rc) return rc;
   if (nsteps < 1) return fail(DGB_ERR_ARG, "need nsteps >= 1");
@@ -530,29 +567,39 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
   }
   CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-  // the step of enqueue_step (capi.cu) launch by launch, with every stage
-  // state written to its own buffer: the same kernels on the same inputs,
-  // so the states are those dgb_step computes, bit for bit
+  // the step of enqueue_step (capi.cu) launch by launch, in dgb_step's form,
+  // with every stage state written to its own buffer: the same kernels on the
+  // same inputs, so the states are those dgb_step computes, bit for bit
   const KLaunch L = klaunch(h);
+  const bool gauss = h->gauss_step;
+  double* Ures = gauss ? h->d_V : h->d_U;
+  if (gauss && !h->v_current) CK(launch_gauss_basis(L, h->d_U, h->d_V, true, h->stream));
   const int rk4[4] = {MODE_RK4_0, MODE_RK4_1, MODE_RK4_2, MODE_RK4_3};
   const int tvd[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
   const int tin4[4] = {0, 1, 0, 1}, tout4[4] = {1, 0, 1, 0};
   const int tin3[3] = {0, 1, 2}, tout3[3] = {1, 2, 0};
-  CK(launch_trace(L, h->d_U, h->d_trace[0], h->stream));
+  if (gauss)
+    CK(launch_vtrace(L, Ures, h->d_trace[0], h->stream));
+  else
+    CK(launch_trace(L, Ures, h->d_trace[0], h->stream));
   long long launches = 1;
   for (unsigned long long i = 0; i < nsteps; ++i) {
-    if ((rc = copy_state(h, h->d_slots[i], h->d_U))) return rc;
+    if ((rc = copy_state(h, h->d_slots[i], Ures))) return rc;
     double* Si = h->d_stage_store + (size_t)i * (nst - 1) * (size_t)h->n;
     for (int st = 0; st < nst; ++st) {
       StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[st] : tvd[st], dt);
-      a.Ubase = h->d_U;
+      a.Ubase = Ures;
       a.acc = h->d_acc;
-      a.Uout = st == nst - 1 ? h->d_U : Si + (size_t)st * h->n;
+      a.Uout = st == nst - 1 ? Ures : Si + (size_t)st * h->n;
       a.part = st == 0 ? h->d_part : nullptr;
       a.flag = h->d_flag;
       a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[st] : tout3[st]];
-      const double* in = st == 0 ? h->d_U : Si + (size_t)(st - 1) * h->n;
-      CK(launch_stage(L, in, h->d_trace[scheme == DGB_RK4 ? tin4[st] : tin3[st]], a, h->stream));
+      const double* in = st == 0 ? Ures : Si + (size_t)(st - 1) * h->n;
+      const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[st] : tin3[st]];
+      if (gauss)
+        CK(launch_vstage(L, in, tin, a, h->stream));
+      else
+        CK(launch_stage(L, in, tin, a, h->stream));
       ++launches;
       if (st == 0) {
         CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
@@ -561,7 +608,9 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
       }
     }
   }
-  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], h->d_U))) return rc;
+  if ((rc = copy_state(h, h->d_adj[dgb_handle::ADJ_FINAL], Ures))) return rc;
+  if (gauss) CK(launch_gauss_basis(L, h->d_V, h->d_U, false, h->stream));
+  h->v_current = gauss;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (norms_host)
@@ -571,6 +620,7 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   h->recorded = true;
   h->rec_stages = true;
+  h->rec_gauss = gauss;
   h->rec_scheme = scheme;
   h->rec_dt = dt;
   h->rec_steps = nsteps;
@@ -590,7 +640,19 @@ int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, doubl
   if (!h || !lamN_dev || !lam0_dev) return fail(DGB_ERR_ARG, "null argument");
   if (!h->recorded) return fail(DGB_ERR_ARG, "no recorded forward run (dgb_forward_record)");
   CK(cudaSetDevice(h->device));
-  h->v_current = false;  // the sweep works on the nodal state d_U
+  // the sweep works in the recorded run's form; adjoint vectors cross the
+  // basis change as dJ/dV = B3^-T dJ/dU, dJ/dU = B3^T dJ/dV
+  const bool gauss = h->rec_gauss;
+  double* Ures = gauss ? h->d_V : h->d_U;
+  const KLaunch L = klaunch(h);
+  auto lam_in = [&](double* lam) {
+    return gauss ? cuda_status_rc(launch_gauss_basis_mode(L, lamN_dev, lam, GB_ADJ_TO_GAUSS, h->stream))
+                 : copy_state(h, lam, lamN_dev);
+  };
+  auto lam_out = [&](const double* lam) {
+    return gauss ? cuda_status_rc(launch_gauss_basis_mode(L, lam, lam0_dev, GB_ADJ_TO_NODAL, h->stream))
+                 : copy_state(h, lam0_dev, lam);
+  };
   if (dpar) {
     const int rc = ensure_pgrad(h);
     if (rc) return rc;
@@ -601,15 +663,15 @@ int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, doubl
     double* lam = h->d_adj[dgb_handle::ADJ_LAM];
     int rc;
     CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
-    if ((rc = copy_state(h, lam, lamN_dev))) return rc;
+    if ((rc = lam_in(lam))) return rc;
     long long nl = 0;
     for (unsigned long long k = h->rec_steps; k-- > 0;) {
       double* Si = h->d_stage_store + (size_t)k * (nst - 1) * (size_t)h->n;
       double* stored[3] = {Si, Si + (size_t)h->n, nst > 3 ? Si + 2 * (size_t)h->n : nullptr};
-      if ((rc = enqueue_reverse_step(h, h->rec_scheme, h->rec_dt, h->d_slots[k], lam, &nl, stored, dpar)))
+      if ((rc = enqueue_reverse_step(h, h->rec_scheme, h->rec_dt, h->d_slots[k], lam, &nl, stored, dpar, gauss)))
         return rc;
     }
-    if ((rc = copy_state(h, lam0_dev, lam))) return rc;
+    if ((rc = lam_out(lam))) return rc;
     h->last_launches = nl;
     h->adj_forward_steps = 0;
     h->adj_reverse_steps = (long long)h->rec_steps;
@@ -620,37 +682,38 @@ int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, doubl
   double* lam = h->d_adj[dgb_handle::ADJ_LAM];
   int rc;
   // dgb_step calls since the record may have replaced the step graph
-  if ((rc = ensure_step_graph(h, scheme, dt, h->rec_steps))) return rc;
-  if ((rc = ensure_rev_graph(h, scheme, dt))) return rc;
+  if ((rc = ensure_step_graph(h, scheme, dt, h->rec_steps, gauss))) return rc;
+  if ((rc = ensure_rev_graph(h, scheme, dt, gauss))) return rc;
   CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  h->v_current = false;  // the sweep moves the resident state
   long long nl = 0, fwd = 0, rev = 0;
   if (h->slots_dirty) {
     // an earlier sweep overwrote checkpoints: rebuild them from U_0 (buffer 0
     // is never overwritten) by replaying the recorded run's part of the plan
-    if ((rc = copy_state(h, h->d_U, h->d_slots[0]))) return rc;
+    if ((rc = copy_state(h, Ures, h->d_slots[0]))) return rc;
     bool need_trace = true;
     for (size_t k = 1; k < h->plan_pos; ++k) {
       const CkOp& op = h->plan.ops[k];
       if (op.kind == CK_STORE) {
-        if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+        if ((rc = copy_state(h, h->d_slots[op.arg], Ures))) return rc;
       } else {
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace))) return rc;
+        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, need_trace, gauss))) return rc;
         nl += (need_trace ? 1 : 0) + op.arg * h->launches_per_step;
         need_trace = false;
         fwd += op.arg;
       }
     }
   } else {
-    if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
+    if ((rc = copy_state(h, Ures, h->d_adj[dgb_handle::ADJ_WORK]))) return rc;
   }
-  if ((rc = copy_state(h, lam, lamN_dev))) return rc;
+  if ((rc = lam_in(lam))) return rc;
   for (size_t k = h->plan_pos; k < h->plan.ops.size(); ++k) {
     const CkOp& op = h->plan.ops[k];
     switch (op.kind) {
       case CK_REVERSE:
         if (dpar) {  // the captured reverse step has no parameter terms
-          if ((rc = enqueue_reverse_step(h, scheme, dt, h->d_U, lam, &nl, nullptr, dpar))) return rc;
+          if ((rc = enqueue_reverse_step(h, scheme, dt, Ures, lam, &nl, nullptr, dpar, gauss))) return rc;
         } else {
           CK(cudaGraphLaunch(h->rev_graph, h->stream));
           nl += h->rev_launches;
@@ -658,23 +721,25 @@ int backward_impl(dgb_handle* h, const double* lamN_dev, double* lam0_dev, doubl
         ++rev;
         break;
       case CK_RESTORE:
-        if ((rc = copy_state(h, h->d_U, h->d_slots[op.arg]))) return rc;
+        if ((rc = copy_state(h, Ures, h->d_slots[op.arg]))) return rc;
         break;
       case CK_STORE:
-        if ((rc = copy_state(h, h->d_slots[op.arg], h->d_U))) return rc;
+        if ((rc = copy_state(h, h->d_slots[op.arg], Ures))) return rc;
         h->slots_dirty = true;
         break;
       case CK_FORWARD:
         // the reverse steps reuse the trace buffers: recompute the traces
         CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, true))) return rc;
+        if ((rc = enqueue_steps(h, (unsigned long long)op.arg, true, gauss))) return rc;
         nl += 1 + op.arg * h->launches_per_step;
         fwd += op.arg;
         break;
     }
   }
-  if ((rc = copy_state(h, lam0_dev, lam))) return rc;
-  if ((rc = copy_state(h, h->d_U, h->d_adj[dgb_handle::ADJ_FINAL]))) return rc;
+  if ((rc = lam_out(lam))) return rc;
+  if ((rc = copy_state(h, Ures, h->d_adj[dgb_handle::ADJ_FINAL]))) return rc;
+  if (gauss) CK(launch_gauss_basis(L, h->d_V, h->d_U, false, h->stream));
+  h->v_current = gauss;
   h->last_launches = nl;
   h->adj_forward_steps = fwd;
   h->adj_reverse_steps = rev;

@@ -5,11 +5,11 @@
 
 namespace dgb {
 
-cudaError_t prepare_adjoint_heat(int P) { return prepare_adj_t<true>(P); }
+cudaError_t prepare_adjoint_heat(int P) { return prepare_adj_t<true, false>(P); }
 
 cudaError_t launch_residual_vjp_heat(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st)
 {
-  return launch_vjp_t<true>(L, v, s, st);
+  return launch_vjp_t<true, false>(L, v, s, st);
 }
 
 }  // namespace dgb

@@ -198,6 +198,107 @@ __device__ __forceinline__ void face_test_transpose(int half, const double* sv, 
   __syncthreads();
 }
 
+// Gauss-point form of face_value_grad: the field sVx[5][NB] holds values at
+// the Gauss points (vspace.cuh); the face value and normal derivative come
+// from the normal line through EL / DL, the tangential derivatives from Dq
+// on the face.  Scratch sN[3][10][NQF]; contains one barrier.
+template <int P>
+__device__ __forceinline__ void gface_value_grad(int half, const double* sVx, double* sN, const double* so,
+                                                 double S[5], double g[3][5])
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NH;
+  const int tid = threadIdx.x;
+  if (tid < NH) {
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P;
+    const int a = lf >> 1, end = lf & 1;
+    const double* Ev = so + C::oEh + end * P;
+    const double* Dv = so + C::oDh + end * P;
+    double* out = sN + j * 10 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double v = 0., dn = 0.;
+#pragma unroll
+      for (int qa = 0; qa < P; ++qa) {
+        const double u = sVx[r * NB + face_node<P>(a, qa, t1, t2)];
+        v = fma(Ev[qa], u, v);
+        dn = fma(Dv[qa], u, dn);
+      }
+      out[r * NQF + fq] = v;
+      out[(5 + r) * NQF + fq] = dn;
+    }
+  }
+  __syncthreads();
+  if (tid < NH) {
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+    const double* in = sN + j * 10 * NQF;
+    const double* Dq = so + C::oDq;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double d1 = 0., d2 = 0.;
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        d1 = fma(Dq[q1 * P + k], in[r * NQF + k + P * q2], d1);
+        d2 = fma(Dq[q2 * P + k], in[r * NQF + q1 + P * k], d2);
+      }
+      const double dn = in[(5 + r) * NQF + fq];
+      S[r] = in[r * NQF + fq];
+      g[0][r] = a == 0 ? dn : d1;
+      g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
+      g[2][r] = a == 2 ? dn : d2;
+    }
+  }
+}
+
+// Transpose of gface_value_grad for faces 3*half + j: accumulates into Racc
+// (the thread's Gauss point, tid < NB) the adjoints sv[3][5][NQF] of the face
+// values and sgr[3][15][NQF] of the reference gradients (component i*5 + r).
+// Scratch sc[3][10][NQF]; contains two barriers.
+template <int P>
+__device__ __forceinline__ void gface_test_transpose(int half, const double* sv, const double* sgr, double* sc,
+                                                     const double* so, double Racc[5])
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NH;
+  const int tid = threadIdx.x;
+  const double* Dq = so + C::oDq;
+  if (tid < NH) {  // value adjoint through the tangential derivatives; normal derivative adjoint
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
+    const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+    const double* fv = sv + j * 5 * NQF;
+    const double* fg = sgr + j * 15 * NQF;
+    double* o = sc + j * 10 * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double s = fv[r * NQF + fq];
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        s = fma(Dq[k * P + t1], fg[(ax1 * 5 + r) * NQF + k + P * t2], s);
+        s = fma(Dq[k * P + t2], fg[(ax2 * 5 + r) * NQF + t1 + P * k], s);
+      }
+      o[r * NQF + fq] = s;
+      o[(5 + r) * NQF + fq] = fg[(a * 5 + r) * NQF + fq];
+    }
+  }
+  __syncthreads();
+  if (tid < NB) {  // each Gauss point gathers from the face points on its normal lines
+    const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+    const double* Ev = so + C::oEh;
+    const double* Dv = so + C::oDh;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int lf = 3 * half + j, a = lf >> 1, end = lf & 1;
+      const int qa = a == 0 ? qx : a == 1 ? qy : qz;
+      const int t1 = a == 0 ? qy : qx, t2 = a == 2 ? qy : qz;
+      const double ev = Ev[end * P + qa], dv = Dv[end * P + qa];
+      const double* c = sc + j * 10 * NQF + t1 + P * t2;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Racc[r] += ev * c[r * NQF] + dv * c[(5 + r) * NQF];
+    }
+  }
+  __syncthreads();
+}
+
 template <int P>
 struct AdjASmem {
   using C = Cfg<P>;
@@ -219,7 +320,11 @@ struct AdjASmem {
 // CV (curved elements): per-point geometry from gv / gf as in the stage
 // kernel; the inverse mass matrix B3^-1 diag(1/(w detJ)) B3^-T is symmetric,
 // so mu takes the same operator.
-template <int P, bool CV, bool HT>
+// GS: the Gauss-point form (vspace.cuh): U, lam and the result hold values at
+// the Gauss points, the VJP of f_V = -Y(V) / (w detJ); mu = -lam / (w detJ)
+// pointwise, no interpolation to or from the Gauss points, and the face
+// values / gradients of mu through the normal lines.
+template <int P, bool CV, bool HT, bool GS>
 __global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJA_MINB>::value))
 adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr, VjpArgs v,
             const double* __restrict__ opsg, const double* __restrict__ geo, const double* __restrict__ gv,
@@ -261,7 +366,15 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
 
   // mu = -Minv^T lam  (f = -Minv R)
-  if constexpr (CV) {  // B3^-T, 1/(w detJ), B3^-1
+  if constexpr (GS) {  // diagonal: -lam / (w detJ) at each Gauss point
+    if (node) {
+      const double* w = so + C::oW;
+      const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+      const double iw = -1.0 / (w[qx] * w[qy] * w[qz] * (CV ? gve[kVolDetJ * NB + tid] : detJ));
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Mu[r * NB + tid] = V0[r * NB + tid] * iw;
+    }
+  } else if constexpr (CV) {  // B3^-T, 1/(w detJ), B3^-1
     if (node) contract<P, 0, true, false>(Mi, V0, V1, tid);
     __syncthreads();
     if (node) contract<P, 1, true, false>(Mi, V1, V0, tid);
@@ -288,32 +401,41 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     if (node) contract<P, 2, true, false>(Mi, V0, Mu, tid, -1.0 / detJ);
   }
   __syncthreads();
-  for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = U[e * 5 * NB + i];
+  if constexpr (GS) {  // the state is at the Gauss points already
+    for (int i = tid; i < 5 * NB; i += blockDim.x) Sq[i] = U[e * 5 * NB + i];
+  } else {
+    for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = U[e * 5 * NB + i];
+  }
   __syncthreads();
 
   // ---- volume: recompute S, grad S at the quadrature points; mu and its
   // gradient there; reverse the pointwise flux; transposed projections
-  if (node) contract<P, 0, false, false>(B, V0, V1, tid);
-  __syncthreads();
-  if (node) contract<P, 1, false, false>(B, V1, V0, tid);
-  __syncthreads();
-  if (node) contract<P, 2, false, false>(B, V0, Sq, tid);
-  __syncthreads();
+  if constexpr (!GS) {
+    if (node) contract<P, 0, false, false>(B, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, false, false>(B, V1, V0, tid);
+    __syncthreads();
+    if (node) contract<P, 2, false, false>(B, V0, Sq, tid);
+    __syncthreads();
+  }
   if (node) {
     contract<P, 0, false, false>(Dq, Sq, G, tid);
     contract<P, 1, false, false>(Dq, Sq, G + 5 * NB, tid);
     contract<P, 2, false, false>(Dq, Sq, G + 10 * NB, tid);
-    contract<P, 0, false, false>(B, Mu, V0, tid);
+    if constexpr (!GS) contract<P, 0, false, false>(B, Mu, V0, tid);
   }
   __syncthreads();
-  if (node) contract<P, 1, false, false>(B, V0, V1, tid);
-  __syncthreads();
-  if (node) contract<P, 2, false, false>(B, V1, V0, tid);  // V0: mu at quadrature points
-  __syncthreads();
+  if constexpr (!GS) {
+    if (node) contract<P, 1, false, false>(B, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 2, false, false>(B, V1, V0, tid);  // V0: mu at quadrature points
+    __syncthreads();
+  }
   if (node) {
-    contract<P, 0, false, false>(Dq, V0, N, tid);
-    contract<P, 1, false, false>(Dq, V0, N + 5 * NB, tid);
-    contract<P, 2, false, false>(Dq, V0, N + 10 * NB, tid);
+    const double* Mq = GS ? Mu : V0;  // mu at the quadrature points
+    contract<P, 0, false, false>(Dq, Mq, N, tid);
+    contract<P, 1, false, false>(Dq, Mq, N + 5 * NB, tid);
+    contract<P, 2, false, false>(Dq, Mq, N + 10 * NB, tid);
   }
   __syncthreads();
   if (node) {  // pointwise reverse at quadrature point tid
@@ -362,20 +484,31 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   }
   __syncthreads();
   double Ub[5] = {0., 0., 0., 0., 0.};
-  if (node) {  // S-bar + sum_i Dq_i^T g-bar_i, then B^T in three directions
-    contract<P, 0, true, false>(Dq, N, V0, tid);
-    contract<P, 1, true, true>(Dq, N + 5 * NB, V0, tid);
-    contract<P, 2, true, true>(Dq, N + 10 * NB, V0, tid);
+  if constexpr (GS) {  // S-bar + sum_i Dq_i^T g-bar_i at the Gauss point
+    if (node) {
+      contract<P, 0, true, false>(Dq, N, V0, tid);
+      contract<P, 1, true, true>(Dq, N + 5 * NB, V0, tid);
+      contract<P, 2, true, true>(Dq, N + 10 * NB, V0, tid);
 #pragma unroll
-    for (int r = 0; r < 5; ++r) V0[r * NB + tid] += Sq[r * NB + tid];
+      for (int r = 0; r < 5; ++r) Ub[r] = V0[r * NB + tid] + Sq[r * NB + tid];
+    }
+    __syncthreads();
+  } else {
+    if (node) {  // S-bar + sum_i Dq_i^T g-bar_i, then B^T in three directions
+      contract<P, 0, true, false>(Dq, N, V0, tid);
+      contract<P, 1, true, true>(Dq, N + 5 * NB, V0, tid);
+      contract<P, 2, true, true>(Dq, N + 10 * NB, V0, tid);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) V0[r * NB + tid] += Sq[r * NB + tid];
+    }
+    __syncthreads();
+    if (node) contract<P, 0, true, false>(B, V0, V1, tid);
+    __syncthreads();
+    if (node) contract<P, 1, true, false>(B, V1, V0, tid);
+    __syncthreads();
+    if (node) contract_reg<P, 2, true>(B, V0, tid, Ub);
+    __syncthreads();
   }
-  __syncthreads();
-  if (node) contract<P, 0, true, false>(B, V0, V1, tid);
-  __syncthreads();
-  if (node) contract<P, 1, true, false>(B, V1, V0, tid);
-  __syncthreads();
-  if (node) contract_reg<P, 2, true>(B, V0, tid, Ub);
-  __syncthreads();
 
   // ---- faces.  The lifting's transpose is pointwise like the lifting
   // (K = diag(1/w), see the stage kernel): zb = (K x K)^T (ef fw mu) = ef fJ mu.
@@ -385,7 +518,10 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     double Sm[5], gm[3][5];
-    face_value_grad<P>(half, Mu, sN, sY, so, Sm, gm);
+    if constexpr (GS)
+      gface_value_grad<P>(half, Mu, sN, so, Sm, gm);
+    else
+      face_value_grad<P>(half, Mu, sN, sY, so, Sm, gm);
     const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
     if (tid < NH) {
       const int nb = nbr[e * 6 + lf];
@@ -543,7 +679,8 @@ struct AdjBSmem {
   static constexpr int TOTAL = oX + 75 * NQF + 60 * NQF;
 };
 
-template <int P, bool CV, bool HT>
+// GS: the Gauss-point form (U and the result at the Gauss points), as adjA.
+template <int P, bool CV, bool HT, bool GS>
 __global__ void __launch_bounds__(Cfg<P>::NT, (AdjMinB<P, DGB_ADJB_MINB>::value))
 adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA, const double* __restrict__ opsg,
             const double* __restrict__ geo, const double* __restrict__ gf, const int* __restrict__ nbr,
@@ -578,7 +715,10 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     double S[5], g[3][5];
-    face_value_grad<P>(half, sU, sN, sY, so, S, g);
+    if constexpr (GS)
+      gface_value_grad<P>(half, sU, sN, so, S, g);
+    else
+      face_value_grad<P>(half, sU, sN, sY, so, S, g);
     if (tid < NH) {
       const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF;
       const int nb = nbr[e * 6 + lf];
@@ -636,7 +776,10 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
       }
     }
     __syncthreads();
-    face_test_transpose<P>(half, sv, sgr, su, sc, so, Racc);
+    if constexpr (GS)
+      gface_test_transpose<P>(half, sv, sgr, sc, so, Racc);
+    else
+      face_test_transpose<P>(half, sv, sgr, su, sc, so, Racc);
   }
   if (tid < NB) {
 #pragma unroll
@@ -649,79 +792,81 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
 }
 
 // ------------------------------------------------------------ host launchers
+// GS: the Gauss-point form (the reverse steps of recorded runs in that form)
 
-template <int P, bool CV, bool HT>
+template <int P, bool CV, bool HT, bool GS>
 cudaError_t prepare_pc()
 {
   static_assert(AdjASmem<P>::TOTAL * 8 <= 227 * 1024, "adjoint shared memory");
-  cudaError_t e = cudaFuncSetAttribute(adjA_kernel<P, CV, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(adjA_kernel<P, CV, HT, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(AdjASmem<P>::TOTAL * sizeof(double)));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(adjB_kernel<P, CV, HT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(adjB_kernel<P, CV, HT, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)(AdjBSmem<P>::TOTAL * sizeof(double)));
 }
 
-template <int P, bool HT>
+template <int P, bool HT, bool GS>
 cudaError_t prepare_adj_p()
 {
-  cudaError_t e = prepare_pc<P, false, HT>();
-  return e == cudaSuccess ? prepare_pc<P, true, HT>() : e;
+  cudaError_t e = prepare_pc<P, false, HT, GS>();
+  return e == cudaSuccess ? prepare_pc<P, true, HT, GS>() : e;
 }
 
-template <int P, bool CV, bool HT>
+template <int P, bool CV, bool HT, bool GS>
 cudaError_t vjp_pc(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, const double* Tr, cudaStream_t st)
 {
-  adjA_kernel<P, CV, HT><<<(unsigned)L.E, Cfg<P>::NT, AdjASmem<P>::TOTAL * sizeof(double), st>>>(
+  adjA_kernel<P, CV, HT, GS><<<(unsigned)L.E, Cfg<P>::NT, AdjASmem<P>::TOTAL * sizeof(double), st>>>(
       L.E, v.U, Tr, v, L.opsd, L.geo, L.gv, L.gf, L.nbr, L.prm, s.part, s.ta, s.flag);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  adjB_kernel<P, CV, HT><<<(unsigned)L.E, Cfg<P>::NT, AdjBSmem<P>::TOTAL * sizeof(double), st>>>(
+  adjB_kernel<P, CV, HT, GS><<<(unsigned)L.E, Cfg<P>::NT, AdjBSmem<P>::TOTAL * sizeof(double), st>>>(
       L.E, v.U, s.ta, L.opsd, L.geo, L.gf, L.nbr, L.prm, s.part, v);
   return cudaGetLastError();
 }
 
-template <int P, bool HT>
+template <int P, bool HT, bool GS>
 cudaError_t vjp_p(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st)
 {
   cudaError_t e;
   const double* Tr = v.Tr;
-  if (!Tr) {
+  if (!Tr) {  // FP64 face traces of v.U (a mixed-precision handle's stages have FP32 ones)
     KLaunch L64 = L;
     L64.precision = DGB_FP64;
     L64.ops = L.opsd;
-    if ((e = launch_trace(L64, v.U, s.trace, st)) != cudaSuccess) return e;
+    e = GS ? launch_vtrace(L64, v.U, s.trace, st) : launch_trace(L64, v.U, s.trace, st);
+    if (e != cudaSuccess) return e;
     Tr = s.trace;
   }
-  return L.gv ? vjp_pc<P, true, HT>(L, v, s, Tr, st) : vjp_pc<P, false, HT>(L, v, s, Tr, st);
+  return L.gv ? vjp_pc<P, true, HT, GS>(L, v, s, Tr, st) : vjp_pc<P, false, HT, GS>(L, v, s, Tr, st);
 }
 
-// the dispatch on the order, for one HT
-template <bool HT>
+// the dispatch on the order, for one (HT, GS)
+template <bool HT, bool GS>
 cudaError_t prepare_adj_t(int P)
 {
   switch (P) {
-    case 1: return prepare_adj_p<1, HT>();
-    case 2: return prepare_adj_p<2, HT>();
-    case 3: return prepare_adj_p<3, HT>();
-    case 4: return prepare_adj_p<4, HT>();
-    case 5: return prepare_adj_p<5, HT>();
-    case 6: return prepare_adj_p<6, HT>();
-    case 7: return prepare_adj_p<7, HT>();
+    case 1: return prepare_adj_p<1, HT, GS>();
+    case 2: return prepare_adj_p<2, HT, GS>();
+    case 3: return prepare_adj_p<3, HT, GS>();
+    case 4: return prepare_adj_p<4, HT, GS>();
+    case 5: return prepare_adj_p<5, HT, GS>();
+    case 6: return prepare_adj_p<6, HT, GS>();
+    case 7: return prepare_adj_p<7, HT, GS>();
   }
   return cudaErrorInvalidValue;
 }
 
-template <bool HT>
+template <bool HT, bool GS>
 cudaError_t launch_vjp_t(const KLaunch& L, const VjpArgs& v, const VjpScratch& s, cudaStream_t st)
 {
   switch (L.P) {
-    case 1: return vjp_p<1, HT>(L, v, s, st);
-    case 2: return vjp_p<2, HT>(L, v, s, st);
-    case 3: return vjp_p<3, HT>(L, v, s, st);
-    case 4: return vjp_p<4, HT>(L, v, s, st);
-    case 5: return vjp_p<5, HT>(L, v, s, st);
-    case 6: return vjp_p<6, HT>(L, v, s, st);
-    case 7: return vjp_p<7, HT>(L, v, s, st);
+    case 1: return vjp_p<1, HT, GS>(L, v, s, st);
+    case 2: return vjp_p<2, HT, GS>(L, v, s, st);
+    case 3: return vjp_p<3, HT, GS>(L, v, s, st);
+    case 4: return vjp_p<4, HT, GS>(L, v, s, st);
+    case 5: return vjp_p<5, HT, GS>(L, v, s, st);
+    case 6: return vjp_p<6, HT, GS>(L, v, s, st);
+    case 7: return vjp_p<7, HT, GS>(L, v, s, st);
   }
   return cudaErrorInvalidValue;
 }

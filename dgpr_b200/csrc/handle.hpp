@@ -90,6 +90,8 @@ struct dgb_handle {
   cudaGraphExec_t rev_graph = nullptr;  // one reverse step of d_U with the adjoint in ADJ_LAM
   int rev_scheme = -1;
   double rev_dt = 0.;
+  bool rev_gauss = false;  // the captured reverse step's form
+  bool rec_gauss = false;  // the recorded run steps the Gauss-point form (on d_V)
   long long rev_launches = 0;
   long long adj_forward_steps = 0;  // steps recomputed by the last dgb_backward
   long long adj_reverse_steps = 0;

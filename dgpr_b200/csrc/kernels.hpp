@@ -90,8 +90,15 @@ cudaError_t prepare_gauss(int P, int precision);
 cudaError_t launch_vtrace(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
 cudaError_t launch_vstage(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                           cudaStream_t st);
-// V = B3 U (to_gauss) or U = B3^-1 V, FP64, per element
-cudaError_t launch_gauss_basis(const KLaunch& L, const double* in, double* out, bool to_gauss, cudaStream_t st);
+// the basis changes of the Gauss-point form, FP64, per element (vspace.cuh)
+enum { GB_TO_GAUSS = 0, GB_TO_NODAL = 1, GB_ADJ_TO_GAUSS = 2, GB_ADJ_TO_NODAL = 3 };
+cudaError_t launch_gauss_basis_mode(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st);
+// V = B3 U (to_gauss) or U = B3^-1 V
+inline cudaError_t launch_gauss_basis(const KLaunch& L, const double* in, double* out, bool to_gauss,
+                                      cudaStream_t st)
+{
+  return launch_gauss_basis_mode(L, in, out, to_gauss ? GB_TO_GAUSS : GB_TO_NODAL, st);
+}
 // per compute type and heat flag (vspace_*.cu)
 cudaError_t vprepare_fp64(int P, bool heat);
 cudaError_t vlaunch_trace_fp64(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);

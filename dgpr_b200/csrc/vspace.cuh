@@ -410,31 +410,35 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   }
 }
 
-// V = (B x B x B) U (to_gauss) or U = (B^-1 x B^-1 x B^-1) V (from_gauss),
-// per element, FP64: the basis change at the edges of dgb_step.
-template <int P, bool TO>
+// The basis changes at the edges of the Gauss-point form, per element, FP64
+// (mode: GB_TO_GAUSS V = B3 U, GB_TO_NODAL U = B3^-1 V; for adjoint vectors,
+// J(U) = J(B3^-1 V): GB_ADJ_TO_GAUSS dJ/dV = B3^-T dJ/dU, GB_ADJ_TO_NODAL
+// dJ/dU = B3^T dJ/dV).
+template <int P, int MODE>
 __global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const double* __restrict__ in,
                                                                  double* __restrict__ out,
                                                                  const double* __restrict__ opsd)
 {
   using C = Cfg<P>;
   constexpr int NB = C::NB;
+  constexpr bool INV = MODE == GB_TO_NODAL || MODE == GB_ADJ_TO_GAUSS;  // B^-1 (else B)
+  constexpr bool TR = MODE == GB_ADJ_TO_GAUSS || MODE == GB_ADJ_TO_NODAL;
   __shared__ __align__(16) double sm[2 * P * P + 10 * NB];
-  double* M = sm;  // B or B^-1
+  double* M = sm;
   double* A = sm + 2 * P * P;
   double* Bf = A + 5 * NB;
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
-  for (int i = tid; i < P * P; i += blockDim.x) M[i] = opsd[(TO ? C::oB : C::oBi) + i];
+  for (int i = tid; i < P * P; i += blockDim.x) M[i] = opsd[(INV ? C::oBi : C::oB) + i];
   for (int i = tid; i < 5 * NB; i += blockDim.x) A[i] = in[e * 5 * NB + i];
   __syncthreads();
-  if (tid < NB) contract<P, 0, false, false>(M, A, Bf, tid);
+  if (tid < NB) contract<P, 0, TR, false>(M, A, Bf, tid);
   __syncthreads();
-  if (tid < NB) contract<P, 1, false, false>(M, Bf, A, tid);
+  if (tid < NB) contract<P, 1, TR, false>(M, Bf, A, tid);
   __syncthreads();
   if (tid < NB) {
     double v[5];
-    contract_reg<P, 2, false>(M, A, tid, v);
+    contract_reg<P, 2, TR>(M, A, tid, v);
 #pragma unroll
     for (int r = 0; r < 5; ++r) out[e * 5 * NB + r * NB + tid] = v[r];
   }

@@ -168,9 +168,11 @@ int dgb_state_device_ptr(dgb_handle* h, double** U_dev);
  * from the Gauss points drop out; it converts U -> V before its first step
  * and V -> U after its last (and continues from V across calls while the
  * state is not set otherwise, so a run split into calls is the same run).
- * DGB_STEP_NODAL steps the nodal coefficients, with the kernels the recorded
- * runs of the adjoint (dgb_forward_record) use.  Both are the reference's
- * discretisation; they agree to rounding. */
+ * DGB_STEP_NODAL steps the nodal coefficients.  Both are the reference's
+ * discretisation; they agree to rounding.  The recorded runs of the adjoint
+ * (dgb_forward_record*) step in the same form as dgb_step, and the backward
+ * sweep reverses that form; its adjoint vectors enter and leave in the nodal
+ * layout. */
 enum { DGB_STEP_GAUSS = 0, DGB_STEP_NODAL = 1 };
 int dgb_set_step_form(dgb_handle* h, int form);
 
@@ -237,9 +239,9 @@ int dgb_residual_vjp(dgb_handle* h, const double* U_host, const double* lam_host
  * stream, no host synchronisation. */
 int dgb_residual_vjp_device(dgb_handle* h, const double* U_dev, const double* lam_dev, double* Ubar_dev);
 
-/* Reverse of one RK step U -> U' of `scheme`: lam_dev holds the adjoint of U'
- * on entry and the adjoint of U on return (in place).  U_dev is unchanged.
- * Synchronises. */
+/* Reverse of one RK step U -> U' of `scheme`, as dgb_step takes it (in its
+ * form, dgb_set_step_form): lam_dev holds the adjoint of U' on entry and the
+ * adjoint of U on return (in place).  U_dev is unchanged.  Synchronises. */
 int dgb_step_vjp_device(dgb_handle* h, int scheme, double dt, const double* U_dev, double* lam_dev);
 
 /* Recorded forward run: advances the resident state by nsteps like dgb_step

@@ -123,12 +123,15 @@ STEP_CASES = [
 ]
 
 
+@pytest.mark.parametrize("form", [dg.STEP_GAUSS, dg.STEP_NODAL], ids=["gauss", "nodal"])
 @pytest.mark.parametrize("scheme", [dg.RK4, dg.TVDRK3], ids=["rk4", "tvdrk3"])
 @pytest.mark.parametrize("name,case_name,dt", STEP_CASES, ids=[c[0] for c in STEP_CASES])
-def test_step_vjp_matches_fd(scheme, name, case_name, dt):
+def test_step_vjp_matches_fd(scheme, name, case_name, dt, form):
+    """dgb_step_vjp_device is the VJP of dgb_step in its form."""
     case = next(c for c in C.residual_cases() if c.name == case_name)
     rng = np.random.default_rng(4)
     with solver(case) as s:
+        s.set_step_form(form)
         U = case.U
         w = rng.standard_normal(U.size)
         v = rng.standard_normal(U.size)
@@ -151,12 +154,16 @@ def _tgv_case(n=3, p=2, mu=2e-2):
     return C.Case("tgv", n, n, n, p, 1, nodes, [C.P_] * 6, prm, U)
 
 
+@pytest.mark.parametrize("form", [dg.STEP_GAUSS, dg.STEP_NODAL], ids=["gauss", "nodal"])
 @pytest.mark.parametrize("scheme", [dg.RK4, dg.TVDRK3], ids=["rk4", "tvdrk3"])
-def test_n_step_adjoint_fd_and_checkpoint_invariance(scheme):
+def test_n_step_adjoint_fd_and_checkpoint_invariance(scheme, form):
+    """The recorded run steps in dgb_step's form (Gauss-point or nodal) and
+    the backward sweep reverses that form."""
     case = _tgv_case()
     N, dt = 12, 5e-3
     rng = np.random.default_rng(5)
     with solver(case) as s:
+        s.set_step_form(form)
         U0 = case.U
         w = rng.standard_normal(U0.size)
         grads = {}
@@ -178,10 +185,7 @@ def test_n_step_adjoint_fd_and_checkpoint_invariance(scheme):
         fwd, rev, _ = s.adjoint_stats()
         assert fwd == 0 and rev == N
         ref = _step(s, U0, scheme, dt, N)
-        assert rel(UN, ref) < 1e-13, "recorded run (nodal form) equals dgb_step (Gauss-point form) to rounding"
-        s.set_step_form(dg.STEP_NODAL)
-        assert np.array_equal(UN, _step(s, U0, scheme, dt, N)), "recorded run equals the nodal dgb_step"
-        s.set_step_form(dg.STEP_GAUSS)
+        assert np.array_equal(UN, ref), "recorded run equals dgb_step"
         for slots, g in grads.items():
             assert np.array_equal(g, grads[N]), f"gradient depends on the checkpoint budget ({slots})"
         v = rng.standard_normal(U0.size)
@@ -189,6 +193,31 @@ def test_n_step_adjoint_fd_and_checkpoint_invariance(scheme):
         fd = w @ (_step(s, U0 + h * v, scheme, dt, N) - _step(s, U0 - h * v, scheme, dt, N)) / (2 * h)
         an = grads[N] @ v
     assert abs(fd - an) <= 1e-6 * abs(an), (fd, an)
+
+
+def test_adjoint_forms_agree():
+    """The Gauss-point and the nodal forms are one discretisation: their
+    recorded runs and gradients agree to rounding (affine TGV, RK4, and the
+    sinusoidally mapped mesh, TVD-RK3)."""
+    cases = [(_tgv_case(), dg.RK4)]
+    n, p, q = 2, 2, 3
+    L = 2 * math.pi
+    nodes = C.sine_nodes(n, n, n, q, L, L, L, 0.1)
+    prm = C.params(mu=2e-2, c=1.0 / 0.3, u=0.0, v=0.0, w=0.0)
+    U0 = C.taylor_green(C.node_coords(n, n, n, p, q, nodes), Ma=0.3).reshape(-1)
+    cases.append((C.Case("tgv_sine", n, n, n, p, q, nodes, [C.P_] * 6, prm, U0), dg.TVDRK3))
+    for case, scheme in cases:
+        w = np.random.default_rng(10).standard_normal(case.U.size)
+        out = {}
+        for form in (dg.STEP_GAUSS, dg.STEP_NODAL):
+            with solver(case) as s:
+                s.set_step_form(form)
+                s.set_state(case.U)
+                s.forward_record(scheme, 5e-3, 8, 3)
+                out[form] = (s.get_state(), s.backward(w))
+        assert rel(out[dg.STEP_GAUSS][0], out[dg.STEP_NODAL][0]) < 1e-13
+        assert rel(out[dg.STEP_GAUSS][1], out[dg.STEP_NODAL][1]) < 1e-12, rel(out[dg.STEP_GAUSS][1],
+                                                                             out[dg.STEP_NODAL][1])
 
 
 def test_curved_n_step_adjoint_fd():
