@@ -114,7 +114,7 @@ __device__ __forceinline__ int face_node(int a, int ia, int t1, int t2)
 template <int P, class T>
 __device__ __forceinline__ void load_line(const T* p, T* v)
 {
-  if constexpr (sizeof(T) == 8 && P % 2 == 0) {
+  if constexpr (std::is_same<T, double>::value && P % 2 == 0) {
 #pragma unroll
     for (int k = 0; k < P; k += 2) {
       const double2 q = *reinterpret_cast<const double2*>(p + k);
@@ -140,7 +140,7 @@ __device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in,
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
-  if constexpr (!TR && sizeof(T) == 8 && P % 2 == 0) {
+  if constexpr (!TR && std::is_same<T, double>::value && P % 2 == 0) {
     load_line<P>(Mat + a * P, m);
   } else {
 #pragma unroll
@@ -149,7 +149,7 @@ __device__ __forceinline__ void contract(const T* __restrict__ Mat, const T* in,
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
     T s = T(0);
-    if constexpr (AX == 0 && sizeof(T) == 8 && P % 2 == 0) {
+    if constexpr (AX == 0 && std::is_same<T, double>::value && P % 2 == 0) {
       T x[P];
       load_line<P>(in + r * NB + base, x);
 #pragma unroll
@@ -172,7 +172,7 @@ __device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T*
   const int a = (o / S) % P;
   const int base = o - a * S;
   T m[P];
-  if constexpr (!TR && sizeof(T) == 8 && P % 2 == 0) {
+  if constexpr (!TR && std::is_same<T, double>::value && P % 2 == 0) {
     load_line<P>(Mat + a * P, m);
   } else {
 #pragma unroll
@@ -181,7 +181,7 @@ __device__ __forceinline__ void contract_reg(const T* __restrict__ Mat, const T*
 #pragma unroll
   for (int r = 0; r < 5; ++r) {
     T s = T(0);
-    if constexpr (AX == 0 && sizeof(T) == 8 && P % 2 == 0) {
+    if constexpr (AX == 0 && std::is_same<T, double>::value && P % 2 == 0) {
       T x[P];
       load_line<P>(in + r * NB + base, x);
 #pragma unroll
@@ -403,17 +403,18 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
 
 // ------------------------------------------------------------- face fluxes
 
-// The face terms of one face point (lf, fq) of element e (solve.cpp:393-794):
-// fa[r * NQF] = the coefficient of the test function phi (Roe or boundary
+// The face terms of one face point (lf, fq) of an element (solve.cpp:393-794):
+// fa[r * OS] = the coefficient of the test function phi (Roe or boundary
 // flux, minus the viscous normal flux, plus the BR2 lifting), times fJ w;
-// fb[(i * 4 + r - 1) * NQF] = the dual-consistency coefficient of
-// d(phi)/d(xi_i) for variables 1..4.  The traces of the element (own) and of
-// its neighbours come from Tr.  Shared by the nodal and the Gauss-point
-// stage kernels, so their face arithmetic is the same.
-template <int P, class T, bool CV>
-__device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const T* __restrict__ Tr,
-                                                  const int* __restrict__ nbr, const T* so, const T* sg,
-                                                  const double* __restrict__ geo, const double* __restrict__ gf,
+// fb[(i * 4 + r - 1) * OS] = the dual-consistency coefficient of
+// d(phi)/d(xi_i) for variables 1..4.  Uo, Qo: the element's trace (values,
+// viscous normal flux) at the point; nb = nbr[e][lf]; for nb >= 0 also the
+// neighbour's (Un, Qn) and its lifting scale lift_n.  Shared by the nodal,
+// the Gauss-point and the paired Gauss-point stage kernels, so their face
+// arithmetic is the same; a pair (T = f2) takes interior faces only.
+template <int P, class T, bool CV, int OS = P * P>
+__device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const T* Uo, const T* Qo, const T* Un,
+                                                  const T* Qn, T lift_n, const T* so, const T* sg,
                                                   const double* __restrict__ gfe, const DevParams& prm, T gamma,
                                                   T mu, T kq, T detJ, const T* Ji, int* flag, T* fa, T* fb)
 {
@@ -433,19 +434,7 @@ __device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const 
   const T* n = CV ? nbuf : sg + kGeoN + 3 * lf;
   const T fJ = CV ? T(gp[kFaceFJ * NQF]) : sg[kGeoFJ + lf];
   const T fw = fJ * w1[q1] * w1[q2];
-  const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
-  T Uo[5], Qo[5];
-#pragma unroll
-  for (int r = 0; r < 5; ++r) {
-    Uo[r] = To[r * NQF + fq];
-    Qo[r] = To[(5 + r) * NQF + fq];
-  }
-  const int nb = nbr[e * 6 + lf];
   if (nb >= 0) {
-    const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
-    T Un[5];
-#pragma unroll
-    for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
     {
       // Roe flux in one orientation for both sides: the element that sees
       // the face on its high side is "left"; the other side negates it
@@ -459,7 +448,7 @@ __device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const 
       const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
       roe_flux(UL, UR, nn, gamma, F);
 #pragma unroll
-      for (int r = 0; r < 5; ++r) fa[r * NQF] = sgn * F[r] - T(0.5) * (Qo[r] - Tn[(5 + r) * NQF + fq]);
+      for (int r = 0; r < 5; ++r) fa[r * OS] = sgn * F[r] - T(0.5) * (Qo[r] - Qn[r]);
     }
     if (mu != T(0)) {
       T d[5];
@@ -471,25 +460,20 @@ __device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const 
 #pragma unroll
           for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
         }
-        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
+        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, OS, kq);
       }
 #pragma unroll
       for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Un[r];  // jump
       T ro[5], rn[5];
       visc_jump_n(Uo, d, n, mu, ro, kq);  // BR2 lifting sources of both sides
       visc_jump_n(Un, d, n, mu, rn, kq);
-      T lift_n;  // the neighbour's lifting scale at this face point
-      if constexpr (CV)
-        lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
-      else
-        lift_n = so[C::oC + (end ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
       const T lift = CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ;
       const T lo = T(0.5) * eta * T(0.5) * fJ * lift;
       const T ln = T(0.5) * eta * T(0.5) * fJ * lift_n;
 #pragma unroll
-      for (int r = 1; r < 5; ++r) fa[r * NQF] += lo * ro[r] + ln * rn[r];
+      for (int r = 1; r < 5; ++r) fa[r * OS] += lo * ro[r] + ln * rn[r];
     }
-  } else {
+  } else if constexpr (!is_pair<T>::value) {
     T Ub[5];
     const int bad = boundary_state(nb, Uo, n, prm, Ub);
     if (bad && flag) atomicOr(flag, 2);
@@ -497,7 +481,7 @@ __device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const 
       T F[5];
       euler_flux_n(Ub, gamma, n, F);
 #pragma unroll
-      for (int r = 0; r < 5; ++r) fa[r * NQF] = F[r] - Qo[r];
+      for (int r = 0; r < 5; ++r) fa[r * OS] = F[r] - Qo[r];
     }
     if (mu != T(0)) {
       T d[5], rb[5];
@@ -509,20 +493,53 @@ __device__ __forceinline__ void face_point_fluxes(long e, int lf, int fq, const 
 #pragma unroll
           for (int c = 0; c < 9; ++c) Jbuf[c] = T(gp[c * NQF]);
         }
-        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, NQF, kq);
+        dual_consistency_ref(Uo, d, n, mu, CV ? Jbuf : Ji, fw, fb, OS, kq);
       }
       visc_jump_n(Ub, d, n, mu, rb, kq);
       const T lb = eta * fJ * (CV ? T(gp[kFaceLift * NQF]) : so[C::oC + end] / detJ);
 #pragma unroll
-      for (int r = 1; r < 5; ++r) fa[r * NQF] += lb * rb[r];
+      for (int r = 1; r < 5; ++r) fa[r * OS] += lb * rb[r];
     }
   }
   if (mu == T(0)) {
 #pragma unroll
-    for (int i = 0; i < 12; ++i) fb[i * NQF] = T(0);
+    for (int i = 0; i < 12; ++i) fb[i * OS] = T(0);
   }
 #pragma unroll
-  for (int r = 0; r < 5; ++r) fa[r * NQF] *= fw;
+  for (int r = 0; r < 5; ++r) fa[r * OS] *= fw;
+}
+
+// The inputs of face_point_fluxes for face point (lf, fq) of element e from
+// the trace buffer Tr[E][6][10][NQF]; returns nb.
+template <int P, class T, bool CV>
+__device__ __forceinline__ int load_face_point(long e, int lf, int fq, const T* __restrict__ Tr,
+                                               const int* __restrict__ nbr, const T* so,
+                                               const double* __restrict__ geo, const double* __restrict__ gf,
+                                               T* Uo, T* Qo, T* Un, T* Qn, T& lift_n)
+{
+  using C = Cfg<P>;
+  constexpr int NQF = C::NQF;
+  const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    Uo[r] = To[r * NQF + fq];
+    Qo[r] = To[(5 + r) * NQF + fq];
+  }
+  const int nb = nbr[e * 6 + lf];
+  lift_n = T(0);
+  if (nb >= 0) {
+    const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      Un[r] = Tn[r * NQF + fq];
+      Qn[r] = Tn[(5 + r) * NQF + fq];
+    }
+    if constexpr (CV)  // the neighbour's lifting scale at this face point
+      lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
+    else
+      lift_n = so[C::oC + ((lf & 1) ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+  }
+  return nb;
 }
 
 // ------------------------------------------------------------- stage kernel
@@ -722,8 +739,10 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
   for (int half = 0; half < 6 / FPP; ++half) {
     if (tid < NH) {
       const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF;
-      face_point_fluxes<P, T, CV>(e, lf, fq, Tr, nbr, so, sg, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag,
-                                  Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
+      T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
+      const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
+      face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
+                                  sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
     __syncthreads();
     if (tid < NH) {  // test functions, first tangential direction: items (j, t1, q2)

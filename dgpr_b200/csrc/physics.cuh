@@ -1,5 +1,6 @@
 // Pointwise physics shared by the kernels, written for a generic real type T
-// (double in the FP64 path, float in the mixed path).  Formulas follow the
+// (double in the FP64 path, float in the mixed path, f2 for two elements of
+// the mixed path in lockstep, pair.cuh).  Formulas follow the
 // reference's flux.cpp and bound_states.cpp; the cited lines name the
 // equations restated here.
 #pragma once
@@ -7,6 +8,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+
+#include "pair.cuh"
 
 // host + device: the kernels use these, and the host-side check hooks run the
 // same code on the CPU
@@ -186,7 +189,14 @@ DGB_HD void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
   const T un = u * n[0] + v * n[1] + w * n[2];
   const T l1 = un + c, l2 = un - c, l3 = un, eps = T(0.05) * c;
   T a1 = fabs(l1), a2 = fabs(l2), a3 = fabs(l3);
-  if (a1 < eps || a2 < eps || a3 < eps) {  // entropy fix, rarely taken
+  if constexpr (is_pair<T>::value) {  // two elements in lockstep: the fix lane by lane
+    if (any_lt(a1, eps) || any_lt(a2, eps) || any_lt(a3, eps)) {
+      const T i2e = T(1) / (T(2) * eps);
+      a1 = select_lt(a1, eps, fabs((eps * eps + l1 * l1) * i2e), a1);
+      a2 = select_lt(a2, eps, fabs((eps * eps + l2 * l2) * i2e), a2);
+      a3 = select_lt(a3, eps, fabs((eps * eps + l3 * l3) * i2e), a3);
+    }
+  } else if (a1 < eps || a2 < eps || a3 < eps) {  // entropy fix, rarely taken
     const T i2e = T(1) / (T(2) * eps);
     if (a1 < eps) a1 = fabs((eps * eps + l1 * l1) * i2e);
     if (a2 < eps) a2 = fabs((eps * eps + l2 * l2) * i2e);
