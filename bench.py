@@ -389,6 +389,23 @@ def _channel_block(dg, torch, steps):
     5600, Ma 0.2), seeded perturbations of a parabolic profile, TVD-RK3 with
     dt from CFL 0.2.  Device time per step of both forms.  The isothermal wall
     and the heat flux are extensions (no reference counterpart)."""
+    mesh, prm, U0, dt = _channel_case(dg)
+    nx, ny, nz, p, q = mesh.nx, mesh.ny, mesh.nz, mesh.p, mesh.q
+    stream = torch.cuda.Stream()
+    out = {"workload": f"channel {nx}x{ny}x{nz} hexes, p = {p}, q = {q} sinusoidal map, isothermal walls, Pr 0.71, "
+                       f"body force, TVD-RK3 dt={dt:.3e} (CFL 0.2)"}
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_stream(stream.cuda_stream)
+            s.set_prandtl(0.71)
+            s.set_state(U0)
+            _warm(dg, torch, s, dt, 3, scheme=dg.TVDRK3)
+            ms = _timed_steps(dg, torch, s, stream, dt, steps, scheme=dg.TVDRK3) / steps
+        out[name] = {"ms_per_step": ms, "value": 5 * (p + 1) ** 3 * nx * ny * nz * 3 / (ms * 1e-3), "unit": UNIT}
+    return out
+
+
+def _channel_case(dg):
     from tests import cases as C
     nx, ny, nz, p, q = 64, 32, 32, P_ORD, 2
     lx, ly, lz = 4 * math.pi, 2.0, 2 * math.pi
@@ -406,17 +423,37 @@ def _channel_block(dg, torch, steps):
     dt = 0.2 * (ly / ny) / ((2 * p + 1) * (c + 1.5))
     iso = dg.ISOTHERMAL_WALL
     mesh = dg.Mesh(nx, ny, nz, p, q, nodes, [dg.PERIODIC, dg.PERIODIC, iso, iso, dg.PERIODIC, dg.PERIODIC])
-    stream = torch.cuda.Stream()
-    out = {"workload": f"channel {nx}x{ny}x{nz} hexes, p = {p}, q = {q} sinusoidal map, isothermal walls, Pr 0.71, "
-                       f"body force, TVD-RK3 dt={dt:.3e} (CFL 0.2)"}
-    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
-        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
-            s.set_stream(stream.cuda_stream)
-            s.set_prandtl(0.71)
-            s.set_state(U0)
-            _warm(dg, torch, s, dt, 3, scheme=dg.TVDRK3)
-            ms = _timed_steps(dg, torch, s, stream, dt, steps, scheme=dg.TVDRK3) / steps
-        out[name] = {"ms_per_step": ms, "value": 5 * (p + 1) ** 3 * nx * ny * nz * 3 / (ms * 1e-3), "unit": UNIT}
+    return mesh, prm, U0, dt
+
+
+def _geometry_block(dg, torch, reps=3):
+    """Set-up cost: wall time of dgb_create, whose element geometry is built
+    on the device (geometry.cu), beside the host builder on the same mesh
+    (dgb_geometry_host, all host threads up to 64; it excludes the
+    host-to-device copy of its output that a host-built handle also needs).
+    Curved: the channel mesh (per-point geometry); affine: the 48^3 p = 4
+    TGV box (one Jacobian per element plus the affinity check at every
+    volume point).  Median of `reps`."""
+    from tests import cases as C
+    mesh_c, prm_c, _, _ = _channel_case(dg)
+    n3 = 48
+    mesh_a = dg.Mesh(n3, n3, n3, 4, 1, C.box_nodes(n3, n3, n3, 1, L_BOX, L_BOX, L_BOX), [dg.PERIODIC] * 6)
+    out = {"host_threads": min(64, os.cpu_count() or 1)}
+    for name, mesh, prm in (("channel_curved", mesh_c, prm_c), ("tgv48_p4_affine", mesh_a, C.params())):
+        create, host = [], []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s = dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64)
+            torch.cuda.synchronize()
+            create.append(time.perf_counter() - t0)
+            s.close()
+            t0 = time.perf_counter()
+            dg.geometry_host(mesh, curved=mesh.q > 1)
+            host.append(time.perf_counter() - t0)
+        E = mesh.nx * mesh.ny * mesh.nz
+        out[name] = {"elements": E, "p": mesh.p, "q": mesh.q, "create_s": float(np.median(create)),
+                     "host_builder_s": float(np.median(host))}
     return out
 
 
@@ -537,6 +574,7 @@ def run_ours(args, rank, world, local_rank):
     curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
     heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
     channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
+    geometry = _geometry_block(dg, torch) if rank == 0 and not args.no_geometry else None
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
@@ -584,6 +622,7 @@ def run_ours(args, rank, world, local_rank):
             "curved": curved,
             "heat": heat,
             "channel": channel,
+            "geometry": geometry,
             "clocks": clocks,
         }
         if cpu:
@@ -601,6 +640,7 @@ def main():
     ap.add_argument("--no-curved", action="store_true", help="skip the curved-mesh block")
     ap.add_argument("--no-heat", action="store_true", help="skip the heat-conduction block")
     ap.add_argument("--no-channel", action="store_true", help="skip the channel (isothermal walls) block")
+    ap.add_argument("--no-geometry", action="store_true", help="skip the set-up (geometry build) timing")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")

@@ -22,6 +22,7 @@ ISOTHERMAL_WALL = -8  # an extension: no-slip wall at Solver.set_wall_temperatur
 RK4, TVDRK3 = 0, 1
 FP64, MIXED_FP32 = 0, 1
 STEP_GAUSS, STEP_NODAL = 0, 1  # dgb_set_step_form
+GEO_ELEMENT, GEO_VOLUME, GEO_FACE = 0, 1, 2  # dgb_get_geometry parts
 DPARAM_MU, DPARAM_SOURCE, DPARAM_TWALL, NDPARAMS = 0, 1, 6, 7  # dgb_backward_params: dJ/d[mu, source[0..4], Tw]
 
 BOUNDARY_TYPES = {  # the reference's boundary_types map (boundaries.cpp:37-44)
@@ -126,6 +127,10 @@ def lib():
             "dgb_lagrange1d": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
             "dgb_lagrange1d_deriv": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
             "dgb_bump_nodes": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.c_double] * 7 + [_dp]),
+            "dgb_get_geometry": (ctypes.c_int, [vp, ctypes.c_int, _dp, ctypes.c_size_t]),
+            "dgb_geometry_host": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(ctypes.c_int),
+                                                 _dp, ctypes.c_size_t, _dp, ctypes.c_size_t, _dp,
+                                                 ctypes.c_size_t]),
             "dgb_make_reference_state": (ctypes.c_int, [ctypes.c_double] * 9 + [_dp, ctypes.POINTER(Params)]),
             "dgb_write_state": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_ulonglong, ctypes.POINTER(MeshDesc),
                                                ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -202,6 +207,36 @@ def bump_nodes(nx, ny, nz, q, lx=2.0, ly=1.0, lz=1.0, a=0.0, bmp_height=0.1, bmp
     nodes = np.zeros(nx * ny * nz * (q + 1) ** 3 * 3)
     _check(lib().dgb_bump_nodes(nx, ny, nz, q, lx, ly, lz, a, bmp_height, bmp_center, bmp_variance, _p(nodes)))
     return nodes
+
+
+def _geometry_sizes(mesh):
+    E = mesh.nx * mesh.ny * mesh.nz
+    P = mesh.p + 1
+    return {GEO_ELEMENT: E * 36, GEO_VOLUME: E * 10 * P ** 3, GEO_FACE: E * 6 * 14 * P ** 2}
+
+
+def geometry_host(mesh, curved=None):
+    """Element geometry built on the host (dgb_geometry_host): (curved,
+    element records, per-point volume part or None, per-point face part or
+    None), flat arrays in dgb_get_geometry's layouts.  `curved` True
+    allocates the per-point parts up front (one build); None finds out with
+    a first build."""
+    n = _geometry_sizes(mesh)
+    d = mesh.desc()
+    cv = ctypes.c_int()
+    if curved:
+        cv.value = 1
+    else:
+        _check(lib().dgb_geometry_host(ctypes.byref(d), ctypes.byref(cv), None, 0, None, 0, None, 0))
+    geo = np.zeros(n[GEO_ELEMENT])
+    gv = np.zeros(n[GEO_VOLUME]) if cv.value else None
+    gf = np.zeros(n[GEO_FACE]) if cv.value else None
+    _check(lib().dgb_geometry_host(ctypes.byref(d), ctypes.byref(cv), _p(geo), geo.size,
+                                   _p(gv) if gv is not None else None, gv.size if gv is not None else 0,
+                                   _p(gf) if gf is not None else None, gf.size if gf is not None else 0))
+    if not cv.value:
+        gv = gf = None
+    return bool(cv.value), geo, gv, gf
 
 
 def box_nodes(nx, ny, nz, q, lx, ly, lz):
@@ -307,6 +342,12 @@ class Solver:
         U = np.zeros(self.n)
         _check(lib().dgb_get_state(self.h, _p(U)))
         return U
+
+    def geometry(self, part=GEO_ELEMENT):
+        """The device-built element geometry (dgb_get_geometry), flat."""
+        out = np.zeros(_geometry_sizes(self.mesh)[part])
+        _check(lib().dgb_get_geometry(self.h, part, _p(out), out.size))
+        return out
 
     def residual(self, U):
         """(R, f) for host state U, f = -Minv R."""

@@ -2,6 +2,7 @@
 // CUDA-graph RK stepping, and the host-only helpers.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -259,14 +260,14 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   h->NQF = h->P * h->P;
   h->E = (long)mesh->nx * mesh->ny * mesh->nz;
   h->n = (long long)h->E * 5 * h->NB;
-  std::vector<double> geo, gv, gf;
   std::vector<int32_t> nbr;
   std::string why;
-  rc = build_geometry(*mesh, h->ops, geo, nbr, why, h->curved, gv, gf);
+  rc = check_mesh(*mesh, why);
   if (rc) {
     delete h;
     return fail(rc, why);
   }
+  build_neighbours(*mesh, nbr);
   h->dprm = device_params(*params, 0., -1.);
   for (int s = 0; s < 6; ++s) h->isothermal = h->isothermal || mesh->bounds[s] == DGB_BT_ISOTHERMAL_WALL;
 
@@ -291,7 +292,7 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   pack_ops(h->ops, table.data());
   const size_t sb = sizeof(double) * (size_t)h->n;
   CKF(cudaMalloc(&h->d_ops, sizeof(double) * table.size()));
-  CKF(cudaMalloc(&h->d_geo, sizeof(double) * geo.size()));
+  CKF(cudaMalloc(&h->d_geo, sizeof(double) * (size_t)h->E * kGeoStride));
   CKF(cudaMalloc(&h->d_nbr, sizeof(int) * nbr.size()));
   CKF(cudaMalloc(&h->d_U, sb));
   CKF(cudaMalloc(&h->d_V, sb));
@@ -303,13 +304,14 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMalloc(&h->d_counter, sizeof(int)));
   CKF(cudaMalloc(&h->d_flag, sizeof(int)));
   CKF(cudaMemcpy(h->d_ops, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
-  CKF(cudaMemcpy(h->d_geo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice));
   CKF(cudaMemcpy(h->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
-  if (h->curved) {
-    CKF(cudaMalloc(&h->d_gv, sizeof(double) * gv.size()));
-    CKF(cudaMalloc(&h->d_gf, sizeof(double) * gf.size()));
-    CKF(cudaMemcpy(h->d_gv, gv.data(), sizeof(double) * gv.size(), cudaMemcpyHostToDevice));
-    CKF(cudaMemcpy(h->d_gf, gf.data(), sizeof(double) * gf.size(), cudaMemcpyHostToDevice));
+  // element geometry, built on the device (geometry.cu)
+  rc = build_geometry_device(*mesh, h->ops, nbr, h->d_nbr, h->stream, h->d_geo, &h->d_gv, &h->d_gf, h->curved, why);
+  if (rc) {
+    fail(rc, why);
+    free_all(h);
+    delete h;
+    return rc;
   }
   CKF(cudaMemset(h->d_U, 0, sb));
   CKF(cudaMemset(h->d_counter, 0, sizeof(int)));
@@ -323,6 +325,24 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(prepare_gauss(h->P, precision));
 #undef CKF
   *out = h;
+  return DGB_OK;
+}
+
+int dgb_get_geometry(dgb_handle* h, int part, double* out, size_t count)
+{
+  if (!h || !out) return fail(DGB_ERR_ARG, "null argument");
+  const double* src = part == DGB_GEO_ELEMENT ? h->d_geo : part == DGB_GEO_VOLUME ? h->d_gv
+                      : part == DGB_GEO_FACE  ? h->d_gf
+                                              : nullptr;
+  const size_t n = part == DGB_GEO_ELEMENT  ? (size_t)h->E * kGeoStride
+                   : part == DGB_GEO_VOLUME ? (size_t)h->E * kVolC * h->NB
+                                            : (size_t)h->E * 6 * kFaceC * h->NQF;
+  if (part < DGB_GEO_ELEMENT || part > DGB_GEO_FACE) return fail(DGB_ERR_ARG, "unknown geometry part");
+  if (!src) return fail(DGB_ERR_ARG, "per-point geometry exists only for curved meshes");
+  if (count != n) return fail(DGB_ERR_ARG, "count does not match the geometry part's size");
+  cudaSetDevice(h->device);
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return DGB_OK;
 }
 
@@ -593,6 +613,30 @@ int dgb_gauss_legendre(int n, double a, double b, double* x, double* w)
 {
   if (n < 1 || !x || !w) return fail(DGB_ERR_ARG, "n must be >= 1");
   gauss_legendre(n, a, b, x, w);
+  return DGB_OK;
+}
+
+int dgb_geometry_host(const dgb_mesh_desc* mesh, int* curved, double* geo, size_t ngeo, double* gv, size_t ngv,
+                      double* gf, size_t ngf)
+{
+  if (!mesh) return fail(DGB_ERR_ARG, "null mesh");
+  Ops1D ops;
+  if (build_ops(mesh->p, ops)) return fail(DGB_ERR_UNSUPPORTED, "solution order outside 0..6");
+  std::vector<double> g, v, f;
+  std::vector<int32_t> nbr;
+  std::string why;
+  bool cv = false;
+  const int rc = build_geometry(*mesh, ops, g, nbr, why, cv, v, f);
+  if (rc) return fail(rc, why);
+  const long E = (long)mesh->nx * mesh->ny * mesh->nz;
+  const size_t NB = (size_t)ops.P * ops.P * ops.P, NQF = (size_t)ops.P * ops.P;
+  if ((geo && ngeo != (size_t)E * kGeoStride) || (cv && gv && ngv != (size_t)E * kVolC * NB) ||
+      (cv && gf && ngf != (size_t)E * 6 * kFaceC * NQF))
+    return fail(DGB_ERR_ARG, "geometry output sizes do not match the mesh");
+  if (curved) *curved = cv ? 1 : 0;
+  if (geo) std::copy(g.begin(), g.end(), geo);
+  if (cv && gv) std::copy(v.begin(), v.end(), gv);
+  if (cv && gf) std::copy(f.begin(), f.end(), gf);
   return DGB_OK;
 }
 

@@ -315,16 +315,14 @@ int curved_element(const double* X, int q, const Ops1D& ops, double* gv, double*
 
 }  // namespace
 
-int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>& geo,
-                   std::vector<int32_t>& nbr, std::string& why, bool& curved, std::vector<double>& gv,
-                   std::vector<double>& gf)
+int check_mesh(const dgb_mesh_desc& m, std::string& why)
 {
-  curved = false;
-  gv.clear();
-  gf.clear();
-  const int nx = m.nx, ny = m.ny, nz = m.nz, q = m.q, P = ops.P;
-  if (nx <= 0 || ny <= 0 || nz <= 0 || q < 1 || q > 7 || !m.nodes) {
+  if (m.nx <= 0 || m.ny <= 0 || m.nz <= 0 || m.q < 1 || m.q > 7 || !m.nodes) {
     why = "mesh sizes must be positive and 1 <= q <= 7";
+    return DGB_ERR_ARG;
+  }
+  if ((long)m.nx * m.ny * m.nz * 6 > 0x7fffffffL) {
+    why = "more elements than a 32-bit neighbour table holds";
     return DGB_ERR_ARG;
   }
   for (int s = 0; s < 6; ++s)
@@ -337,10 +335,64 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
       why = "periodic boundaries are not matching";  // geometry_shared.cpp:123-131
       return DGB_ERR_GEOMETRY;
     }
-  const long E = (long)nx * ny * nz;
+  return DGB_OK;
+}
+
+// neighbours (geometry_common.cpp:397-414 adjacency, periodic wrap as
+// geometry_shared.cpp:205-209)
+void build_neighbours(const dgb_mesh_desc& m, std::vector<int32_t>& nbr)
+{
+  const int nx = m.nx, ny = m.ny, nz = m.nz;
+  nbr.assign((size_t)nx * ny * nz * 6, 0);
+  const int di[6] = {-1, 1, 0, 0, 0, 0}, dj[6] = {0, 0, -1, 1, 0, 0}, dk[6] = {0, 0, 0, 0, -1, 1};
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const long e = i + (long)nx * (j + (long)ny * k);
+        for (int lf = 0; lf < 6; ++lf) {
+          const int ia = i + di[lf], ja = j + dj[lf], ka = k + dk[lf];
+          int side = ia < 0 ? 0 : ia >= nx ? 1 : ja < 0 ? 2 : ja >= ny ? 3 : ka < 0 ? 4 : ka >= nz ? 5 : -1;
+          if (side < 0 || m.bounds[side] == DGB_BT_PERIODIC) {
+            const long en = ((ia + nx) % nx) + (long)nx * (((ja + ny) % ny) + (long)ny * ((ka + nz) % nz));
+            nbr[6 * e + lf] = (int32_t)en;
+          } else {
+            nbr[6 * e + lf] = (int32_t)m.bounds[side];
+          }
+        }
+      }
+}
+
+void build_geo_tables(const Ops1D& ops, int q, GeoTables& t)
+{
+  std::memset(&t, 0, sizeof t);
+  const int P = ops.P;
+  for (int m = 0; m < P + 3; ++m) {
+    const double r = m < P ? ops.x[m] : m == P ? 0. : m == P + 1 ? 1. : 0.5;
+    for (int i = 0; i <= q; ++i) {
+      t.l[m][i] = lagrange1d(i, q, r);
+      t.d[m][i] = lagrange1d_deriv(i, q, r);
+    }
+  }
+  for (int a = 0; a < P; ++a) {
+    t.EL[0][a] = ops.EL[0][a];
+    t.EL[1][a] = ops.EL[1][a];
+    t.w[a] = ops.w[a];
+  }
+}
+
+int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>& geo,
+                   std::vector<int32_t>& nbr, std::string& why, bool& curved, std::vector<double>& gv,
+                   std::vector<double>& gf)
+{
+  curved = false;
+  gv.clear();
+  gf.clear();
+  int rc = check_mesh(m, why);
+  if (rc) return rc;
+  const int q = m.q, P = ops.P;
+  const long E = (long)m.nx * m.ny * m.nz;
   const int Q = q + 1, nq = Q * Q * Q;
   geo.assign((size_t)E * kGeoStride, 0.);
-  nbr.assign((size_t)E * 6, 0);
 
   // sample points for the affinity check: all volume quadrature points and the
   // eight element corners
@@ -392,40 +444,29 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
     gf.assign((size_t)E * 6 * kFaceC * NQF, 0.);
     const int nth = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
     std::vector<int> rcs(nth, DGB_OK);
+    std::vector<long> fails(nth, E);
     std::vector<std::string> whys(nth);
     std::vector<std::thread> pool;
     for (int t = 0; t < nth; ++t)
       pool.emplace_back([&, t]() {
-        for (long e = t; e < E && rcs[t] == DGB_OK; e += nth)
+        for (long e = t; e < E && rcs[t] == DGB_OK; e += nth) {
           rcs[t] = curved_element(m.nodes + (size_t)e * nq * 3, q, ops, &gv[(size_t)e * kVolC * NB],
                                   &gf[(size_t)e * 6 * kFaceC * NQF], e, whys[t]);
+          if (rcs[t]) fails[t] = e;
+        }
       });
     for (auto& th : pool) th.join();
+    // the first failing element in element order, whatever the thread split
+    int tf = -1;
     for (int t = 0; t < nth; ++t)
-      if (rcs[t]) {
-        why = whys[t];
-        return rcs[t];
-      }
+      if (rcs[t] && (tf < 0 || fails[t] < fails[tf])) tf = t;
+    if (tf >= 0) {
+      why = whys[tf];
+      return rcs[tf];
+    }
   }
 
-  // neighbours (geometry_common.cpp:397-414 adjacency, periodic wrap as
-  // geometry_shared.cpp:205-209)
-  const int di[6] = {-1, 1, 0, 0, 0, 0}, dj[6] = {0, 0, -1, 1, 0, 0}, dk[6] = {0, 0, 0, 0, -1, 1};
-  for (int k = 0; k < nz; ++k)
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
-        const long e = i + (long)nx * (j + (long)ny * k);
-        for (int lf = 0; lf < 6; ++lf) {
-          const int ia = i + di[lf], ja = j + dj[lf], ka = k + dk[lf];
-          int side = ia < 0 ? 0 : ia >= nx ? 1 : ja < 0 ? 2 : ja >= ny ? 3 : ka < 0 ? 4 : ka >= nz ? 5 : -1;
-          if (side < 0 || m.bounds[side] == DGB_BT_PERIODIC) {
-            const long en = ((ia + nx) % nx) + (long)nx * (((ja + ny) % ny) + (long)ny * ((ka + nz) % nz));
-            nbr[6 * e + lf] = (int32_t)en;
-          } else {
-            nbr[6 * e + lf] = (int32_t)m.bounds[side];
-          }
-        }
-      }
+  build_neighbours(m, nbr);
 
   // the two sides of every interior face must see the same face
   for (long e = 0; e < E; ++e)

@@ -73,6 +73,32 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
                    std::vector<int32_t>& nbr, std::string& why, bool& curved, std::vector<double>& gv,
                    std::vector<double>& gf);
 
+// The parts of build_geometry that stay on the host in the device build:
+// argument checks, and the neighbour table.
+int check_mesh(const dgb_mesh_desc& m, std::string& why);
+void build_neighbours(const dgb_mesh_desc& m, std::vector<int32_t>& nbr);
+
+// Lagrange values l[m][i] and derivatives d[m][i] (i <= q) of the order-q
+// geometry basis at the reference coordinates the geometry is sampled at:
+// rows m < P the Gauss points, then 0, 1 and 1/2; with the face-lifting
+// weights EL and the Gauss weights.  Built by the host's lagrange1d, so the
+// device builder starts from the host builder's numbers.
+struct GeoTables {
+  double l[kMaxP + 3][8], d[kMaxP + 3][8];
+  double EL[2][kMaxP], w[kMaxP];
+};
+void build_geo_tables(const Ops1D& ops, int q, GeoTables& t);
+
+// build_geometry on the device (geometry.cu), bit-identical to the host
+// builder: d_geo (E * kGeoStride doubles, allocated by the caller) receives
+// the affine records; when an element is curved, *d_gv and *d_gf are
+// allocated and filled with the per-point geometry.  nbr is the host
+// neighbour table and d_nbr its device copy.  The same checks in the same
+// order, with the same messages; CUDA failures return DGB_ERR_CUDA.
+int build_geometry_device(const dgb_mesh_desc& m, const Ops1D& ops, const std::vector<int32_t>& nbr,
+                          const int32_t* d_nbr, void* stream, double* d_geo, double** d_gv, double** d_gf,
+                          bool& curved, std::string& why);
+
 // Total conditions used by the subsonic inflow state (solve.cpp:167-175).
 void total_conditions(const dgb_params& prm, double* Tt, double* Pt);
 

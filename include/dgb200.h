@@ -18,6 +18,8 @@
 #ifndef DGB200_H
 #define DGB200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -100,6 +102,27 @@ const char* dgb_last_error_message(void);
  * current CUDA device. */
 int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precision,
                dgb_handle** out);
+
+/* Element geometry as dgb_create built it on the device, copied to out
+ * (count doubles, which must equal the part's size):
+ *   DGB_GEO_ELEMENT  [E][36]          per element: inverse Jacobian [9]
+ *                                     (row-major d xi_i / d x_c), detJ, the
+ *                                     six outward unit normals [6][3], the
+ *                                     six surface Jacobians, 2 zeros; taken
+ *                                     at the element centre
+ *   DGB_GEO_VOLUME   [E][10][P^3]     curved meshes: inverse Jacobian [9] and
+ *                                     detJ at each volume Gauss point
+ *   DGB_GEO_FACE     [E][6][14][P^2]  curved meshes: inverse Jacobian [9],
+ *                                     outward unit normal [3], surface
+ *                                     Jacobian and BR2 lifting scale at each
+ *                                     face Gauss point
+ * (P = p + 1; Gauss points x-fastest, face points in the face's axis order:
+ * x faces (y,z), y faces (x,z), z faces (x,y)).  The per-point parts of an
+ * affine mesh return DGB_ERR_ARG.  The reference keeps the same quantities
+ * in core_geometry (geometry_common.cpp:292-454) and shared_geometry
+ * (geometry_shared.cpp:156-267). */
+enum { DGB_GEO_ELEMENT = 0, DGB_GEO_VOLUME = 1, DGB_GEO_FACE = 2 };
+int dgb_get_geometry(dgb_handle* h, int part, double* out, size_t count);
 
 /* Frees everything dgb_create allocated.  Replaces free_cuda_device_geometry
  * (solve_cuda.cu:267) and free_cuda_residual_workspace (solve_cuda.cu:323). */
@@ -310,6 +333,17 @@ int dgb_gauss_legendre(int n, double a, double b, double* x, double* w);
 /* Equispaced Lagrange basis on [0,1] and its derivative (basis.cpp:91-148). */
 double dgb_lagrange1d(int i, int p, double x);
 double dgb_lagrange1d_deriv(int i, int p, double x);
+
+/* The element geometry of dgb_get_geometry computed on the host's threads
+ * instead (the builder dgb_residual_noalloc uses), with the same checks and
+ * messages as dgb_create; dgb_create's device builder gives the same bits.
+ * *curved (may be NULL) is set when some element is not affine.  geo gets
+ * the DGB_GEO_ELEMENT part (ngeo doubles); gv and gf the DGB_GEO_VOLUME and
+ * DGB_GEO_FACE parts of a curved mesh (ngv, ngf doubles; untouched for an
+ * affine mesh).  Any of the three may be NULL; a non-NULL one of the wrong
+ * size is DGB_ERR_ARG. */
+int dgb_geometry_host(const dgb_mesh_desc* mesh, int* curved, double* geo, size_t ngeo, double* gv, size_t ngv,
+                      double* gf, size_t ngf);
 
 /* Geometry nodes of the reference's bump / stretched channel generator
  * (generate_bump_nodes, geometry_common.cpp:494-576, as called by

@@ -113,13 +113,8 @@ def test_invalid_meshes_are_rejected_before_device_work():
     assert _try_create(2, 2, 2, 2, 1, box, [dg.PERIODIC, dg.FREESTREAM] + [dg.PERIODIC] * 4) == dg.ERR_GEOMETRY
     assert _try_create(2, 2, 2, 7, 1, box, [dg.PERIODIC] * 6) == dg.ERR_UNSUPPORTED
     assert _try_create(2, 2, 2, 2, 1, box, [dg.INTERIOR] + [dg.PERIODIC] * 5) == dg.ERR_ARG
-    flat = box.copy().reshape(-1, 3)
-    flat[:, 0] = 0.0  # zero-volume elements
-    assert _try_create(2, 2, 2, 2, 1, flat.ravel(), [dg.PERIODIC] * 6) == dg.ERR_GEOMETRY
-    # curved elements are accepted, but periodic sides of a curved mesh must match
-    # point by point: a bump off the channel centre differs at x = 0 and x = lx
-    bump = dg.bump_nodes(2, 2, 2, 2, 2.0, 1.0, 1.0, 0.0, 0.2, 0.7, 0.05)
-    assert _try_create(2, 2, 2, 2, 2, bump, [dg.PERIODIC, dg.PERIODIC] + [dg.FREESTREAM] * 4) == dg.ERR_GEOMETRY
+    # singular and mismatched element geometry is found by the device builder
+    # (tests/test_geometry.py checks it against the host builder's messages)
 
 
 def test_noalloc_residual_rejects_oversized_meshes_before_device_work():
