@@ -273,6 +273,11 @@ def _adjoint_config(dg, torch, nsteps, budgets):
         U0 = modes.state(a0).detach()
         s.set_state(U0.cpu().numpy())
         s.step(dg.RK4, dt, 5, norms=False)  # warm-up
+        # untimed backward of a short record: the reverse-step graph and the
+        # adjoint buffers are made on first use, outside the timed budgets
+        s.set_state(U0.cpu().numpy())
+        s.forward_record(dg.RK4, dt, 2, 2, norms=False)
+        s.backward(np.zeros(U0.numel()))
         grad = None
         for slots in budgets:
             # untimed recorded run first: allocates (or frees) the checkpoint buffers

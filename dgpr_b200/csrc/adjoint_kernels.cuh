@@ -201,8 +201,33 @@ __device__ __forceinline__ void face_test_transpose(int half, const double* sv, 
 // Gauss-point form of face_value_grad: the field sVx[5][NB] holds values at
 // the Gauss points (vspace.cuh); the face value and normal derivative come
 // from the normal line through EL / DL, the tangential derivatives from Dq
-// on the face.  Scratch sN[3][10][NQF]; contains one barrier.
+// on the face.  Scratch sN[3][10][NQF]; contains one barrier.  With WG
+// false only S is returned; gface_grad_point reads g from sN afterwards.
 template <int P>
+__device__ __forceinline__ void gface_grad_point(int half, const double* sN, const double* so, double g[3][5])
+{
+  using C = Cfg<P>;
+  constexpr int NQF = C::NQF;
+  const int tid = threadIdx.x;
+  const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+  const double* in = sN + j * 10 * NQF;
+  const double* Dq = so + C::oDq;
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    double d1 = 0., d2 = 0.;
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      d1 = fma(Dq[q1 * P + k], in[r * NQF + k + P * q2], d1);
+      d2 = fma(Dq[q2 * P + k], in[r * NQF + q1 + P * k], d2);
+    }
+    const double dn = in[(5 + r) * NQF + fq];
+    g[0][r] = a == 0 ? dn : d1;
+    g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
+    g[2][r] = a == 2 ? dn : d2;
+  }
+}
+
+template <int P, bool WG = true>
 __device__ __forceinline__ void gface_value_grad(int half, const double* sVx, double* sN, const double* so,
                                                  double S[5], double g[3][5])
 {
@@ -230,23 +255,11 @@ __device__ __forceinline__ void gface_value_grad(int half, const double* sVx, do
   }
   __syncthreads();
   if (tid < NH) {
-    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+    const int j = tid / NQF, fq = tid % NQF;
     const double* in = sN + j * 10 * NQF;
-    const double* Dq = so + C::oDq;
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      double d1 = 0., d2 = 0.;
-#pragma unroll
-      for (int k = 0; k < P; ++k) {
-        d1 = fma(Dq[q1 * P + k], in[r * NQF + k + P * q2], d1);
-        d2 = fma(Dq[q2 * P + k], in[r * NQF + q1 + P * k], d2);
-      }
-      const double dn = in[(5 + r) * NQF + fq];
-      S[r] = in[r * NQF + fq];
-      g[0][r] = a == 0 ? dn : d1;
-      g[1][r] = a == 0 ? d1 : (a == 1 ? dn : d2);
-      g[2][r] = a == 2 ? dn : d2;
-    }
+    for (int r = 0; r < 5; ++r) S[r] = in[r * NQF + fq];
+    if (WG) gface_grad_point<P>(half, sN, so, g);
   }
 }
 
@@ -448,32 +461,33 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     }
     const double* Ji = CV ? Jbuf : sg + kGeoJinv;  // inverse Jacobian at this point
     const double wJ = w[qx] * w[qy] * w[qz] * (CV ? gve[kVolDetJ * NB + tid] : detJ);
-    double S[5], Gp[3][5], Hb[3][5];
+    double S[5], Hb[3][5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       S[r] = Sq[r * NB + tid];
-      const double g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
       const double n0 = N[r * NB + tid], n1 = N[5 * NB + r * NB + tid], n2 = N[10 * NB + r * NB + tid];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Gp[c][r] = Ji[c] * g0 + Ji[3 + c] * g1 + Ji[6 + c] * g2;
-        Hb[c][r] = wJ * (n0 * Ji[c] + n1 * Ji[3 + c] + n2 * Ji[6 + c]);  // adjoint of H = Q - F
-      }
+      for (int c = 0; c < 3; ++c) Hb[c][r] = wJ * (n0 * Ji[c] + n1 * Ji[3 + c] + n2 * Ji[6 + c]);  // adjoint of H = Q - F
     }
     double Sb[5] = {0., 0., 0., 0., 0.}, Gb[3][5];
+    // F enters H with a minus sign; the Euler VJP is linear in its cotangent
+    euler_flux_vjp(S, gamma, Hb, Sb);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Sb[r] = -Sb[r];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int r = 0; r < 5; ++r) Gb[c][r] = 0.;
-    {
-      double Fb[3][5];
+    if (mu != 0.) {  // the physical gradients only now: they are dead outside the viscous VJP
+      double Gp[3][5];
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 5; ++r) {
+        const double g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) Fb[c][r] = -Hb[c][r];
-      euler_flux_vjp(S, gamma, Fb, Sb);
+        for (int c = 0; c < 3; ++c) Gp[c][r] = Ji[c] * g0 + Ji[3 + c] * g1 + Ji[6 + c] * g2;
+      }
+      visc_flux_vjp(S, Gp, mu, Hb, Sb, Gb, kq);
     }
-    if (mu != 0.) visc_flux_vjp(S, Gp, mu, Hb, Sb, Gb, kq);
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       Sq[r * NB + tid] = Sb[r];
@@ -510,6 +524,11 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     __syncthreads();
   }
 
+  if (node) {  // the volume part is final: out now, so it holds no registers through the faces
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Ubar_part[e * 5 * NB + r * NB + tid] = Ub[r];
+  }
+
   // ---- faces.  The lifting's transpose is pointwise like the lifting
   // (K = diag(1/w), see the stage kernel): zb = (K x K)^T (ef fw mu) = ef fJ mu.
   double* sN = sX;
@@ -518,8 +537,8 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     double Sm[5], gm[3][5];
-    if constexpr (GS)
-      gface_value_grad<P>(half, Mu, sN, so, Sm, gm);
+    if constexpr (GS)  // the gradient of mu is read from sN where the viscous terms need it
+      gface_value_grad<P, false>(half, Mu, sN, so, Sm, gm);
     else
       face_value_grad<P>(half, Mu, sN, sY, so, Sm, gm);
     const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
@@ -546,14 +565,18 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
       double ab[5];
 #pragma unroll
       for (int r = 0; r < 5; ++r) ab[r] = Sm[r];
-      // adjoint of the dual-consistency tensor: dc_bar[c] = -fw sum_i Jinv[i][c] grad_i(mu)
-      double dcb[3][5];
+      // adjoint of the dual-consistency tensor: dc_bar[c] = -fw sum_i Jinv[i][c] grad_i(mu),
+      // made where the viscous terms use it
+      auto dual_bar = [&](double dcb[3][5]) {
+        if constexpr (GS) gface_grad_point<P>(half, sN, so, gm);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        dcb[c][0] = 0.;
+        for (int c = 0; c < 3; ++c) {
+          dcb[c][0] = 0.;
 #pragma unroll
-        for (int r = 1; r < 5; ++r) dcb[c][r] = -fw * (Ji[c] * gm[0][r] + Ji[3 + c] * gm[1][r] + Ji[6 + c] * gm[2][r]);
-      }
+          for (int r = 1; r < 5; ++r)
+            dcb[c][r] = -fw * (Ji[c] * gm[0][r] + Ji[3 + c] * gm[1][r] + Ji[6 + c] * gm[2][r]);
+        }
+      };
       const double* To = Tr + ((e * 6 + lf) * 10) * NQF;
       double Uo[5], Uob[5] = {0., 0., 0., 0., 0.}, Qob[5];
 #pragma unroll
@@ -564,22 +587,15 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
         double Un[5], Unb[5] = {0., 0., 0., 0., 0.};
 #pragma unroll
         for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
-        {  // Roe flux, one orientation for both sides
-          const double sgn = end ? 1. : -1.;
-          double UL[5], UR[5], fb[5], ULb[5] = {0., 0., 0., 0., 0.}, URb[5] = {0., 0., 0., 0., 0.};
+        {  // Roe flux.  The forward orients it (the high side is left) so that
+           // both elements compute the same bits; as a function it is
+           // f(Uo, Un, n_out) either way (antisymmetric under swapping the
+           // sides and flipping n), so its VJP is taken in this element's
+           // orientation, without the side copies
+          double fb[5];
 #pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            UL[r] = end ? Uo[r] : Un[r];
-            UR[r] = end ? Un[r] : Uo[r];
-            fb[r] = sgn * fw * ab[r];
-          }
-          const double nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
-          roe_flux_vjp(UL, UR, nn, gamma, fb, ULb, URb);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            Uob[r] += end ? ULb[r] : URb[r];
-            Unb[r] += end ? URb[r] : ULb[r];
-          }
+          for (int r = 0; r < 5; ++r) fb[r] = fw * ab[r];
+          roe_flux_vjp(Uo, Un, n, gamma, fb, Uob, Unb);
         }
 #pragma unroll
         for (int r = 0; r < 5; ++r) Qob[r] = -0.5 * fw * ab[r];
@@ -587,7 +603,11 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
           double d[5], dbar[5] = {0., 0., 0., 0., 0.};
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - 0.5 * (Uo[r] + Un[r]);
-          visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
+          {
+            double dcb[3][5];
+            dual_bar(dcb);
+            visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
+          }
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
             Uob[r] += 0.5 * dbar[r];
@@ -634,7 +654,11 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
           double d[5], dbar[5] = {0., 0., 0., 0., 0.};
 #pragma unroll
           for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ubd[r];
-          visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
+          {
+            double dcb[3][5];
+            dual_bar(dcb);
+            visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
+          }
           const double co = fw * lift;
           double rbb[5];
 #pragma unroll
@@ -660,10 +684,6 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
       }
     }
     __syncthreads();
-  }
-  if (node) {
-#pragma unroll
-    for (int r = 0; r < 5; ++r) Ubar_part[e * 5 * NB + r * NB + tid] = Ub[r];
   }
 }
 

@@ -436,6 +436,10 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
   const T fw = fJ * w1[q1] * w1[q2];
   if (nb >= 0) {
     {
+      // the gradient-flux jump first: Qo and Qn are dead after it
+      T qd[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) qd[r] = T(0.5) * (Qo[r] - Qn[r]);
       // Roe flux in one orientation for both sides: the element that sees
       // the face on its high side is "left"; the other side negates it
       T UL[5], UR[5], F[5];
@@ -448,7 +452,7 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
       const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
       roe_flux(UL, UR, nn, gamma, F);
 #pragma unroll
-      for (int r = 0; r < 5; ++r) fa[r * OS] = sgn * F[r] - T(0.5) * (Qo[r] - Qn[r]);
+      for (int r = 0; r < 5; ++r) fa[r * OS] = sgn * F[r] - qd[r];
     }
     if (mu != T(0)) {
       T d[5];

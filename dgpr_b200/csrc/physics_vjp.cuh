@@ -240,24 +240,64 @@ DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Q
   rank1_tail_vjp(S, d, v, ir, abar, vbar, T(0), Sbar, dbar);
 }
 
-// Roe flux with entropy fix (roe_flux): fbar[5] -> Ulbar, Urbar
+// Normal Euler flux F(U).n of one side: Fnbar[5] -> Ubar (accumulated),
+// written out directly (no 3x5 intermediate).  With u = m / r, un = u.n,
+// q = |u|^2, p = (g - 1)(E - r q / 2), H = (E + p) / r:
+//   F = (r un, m un + p n, (E + p) un).
+template <class T>
+DGB_HD void euler_normal_flux_vjp(const T* U, T g, const T* n, const T* fb, T* Ubar)
+{
+  const T gm1 = g - T(1);
+  const T ir = T(1) / U[0];
+  const T u[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+  const T un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+  const T q = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const T p = gm1 * (U[4] - T(0.5) * U[0] * q);
+  const T H = (U[4] + p) * ir;
+  const T fbn = fb[1] * n[0] + fb[2] * n[1] + fb[3] * n[2];
+  const T fbu = fb[1] * u[0] + fb[2] * u[1] + fb[3] * u[2];
+  Ubar[0] += -un * fbu + T(0.5) * gm1 * q * fbn + fb[4] * un * (T(0.5) * gm1 * q - H);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    Ubar[1 + j] += (fb[0] + fbu + fb[4] * H) * n[j] + fb[1 + j] * un - gm1 * u[j] * (fbn + fb[4] * un);
+  Ubar[4] += gm1 * fbn + g * un * fb[4];
+}
+
+// Roe flux with entropy fix (roe_flux, flux.cpp:56-154): fbar[5] -> Ulbar,
+// Urbar (accumulated).  The central part 1/2 (F(Ul) + F(Ur)).n goes side by side through
+// euler_normal_flux_vjp; the dissipation -1/2 |A_roe| (Ur - Ul) reverses
+// through the Roe average, and each side's share of the average is taken
+// from its own sqrt(rho), velocity and enthalpy.  Few values are live at a
+// time, which keeps the adjoint face kernel's registers down.
 template <class T>
 DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fbar, T* Ulbar, T* Urbar)
 {
-  // ---- forward, as roe_flux
-  const T gm1 = g - T(1);
-  const T rl = Ul[0], irl = T(1) / rl, ul = Ul[1] * irl, vl = Ul[2] * irl, wl = Ul[3] * irl;
-  const T ql2 = ul * ul + vl * vl + wl * wl;
-  const T pl = gm1 * (Ul[4] - T(0.5) * rl * ql2);
-  const T Hl = (Ul[4] + pl) * irl;
-  const T rr = Ur[0], irr = T(1) / rr, ur = Ur[1] * irr, vr = Ur[2] * irr, wr = Ur[3] * irr;
-  const T qr2 = ur * ur + vr * vr + wr * wr;
-  const T pr = gm1 * (Ur[4] - T(0.5) * rr * qr2);
-  const T Hr = (Ur[4] + pr) * irr;
-  const T sl = sqrt(rl), sr = sqrt(rr), iden = T(1) / (sl + sr);
-  const T uk[3] = {(sl * ul + sr * ur) * iden, (sl * vl + sr * vr) * iden, (sl * wl + sr * wr) * iden};
-  const T H = (sl * Hl + sr * Hr) * iden;
-  const T dr = rr - rl;
+  const T gm1 = g - T(1), h = T(0.5);
+  {
+    T hb[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) hb[k] = h * fbar[k];
+    euler_normal_flux_vjp(Ul, g, n, hb, Ulbar);
+    euler_normal_flux_vjp(Ur, g, n, hb, Urbar);
+  }
+  // ---- forward of the dissipation
+  T sq[2], us[2][3], Hs[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const T* U = s ? Ur : Ul;
+    const T ir = T(1) / U[0];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) us[s][k] = U[1 + k] * ir;
+    const T p = gm1 * (U[4] - T(0.5) * U[0] * (us[s][0] * us[s][0] + us[s][1] * us[s][1] + us[s][2] * us[s][2]));
+    Hs[s] = (U[4] + p) * ir;
+    sq[s] = sqrt(U[0]);
+  }
+  const T iden = T(1) / (sq[0] + sq[1]);
+  T uk[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) uk[k] = (sq[0] * us[0][k] + sq[1] * us[1][k]) * iden;
+  const T H = (sq[0] * Hs[0] + sq[1] * Hs[1]) * iden;
+  const T dr = Ur[0] - Ul[0];
   const T dm[3] = {Ur[1] - Ul[1], Ur[2] - Ul[2], Ur[3] - Ul[3]};
   const T dE = Ur[4] - Ul[4];
   const T q2 = uk[0] * uk[0] + uk[1] * uk[1] + uk[2] * uk[2];
@@ -279,59 +319,27 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   const T G2 = -un * dr + (dm[0] * n[0] + dm[1] * n[1] + dm[2] * n[2]);
   const T C1 = (G1 * ic * ic) * (s1 - a[2]) + (G2 * ic) * s2;
   const T C2 = (G1 * ic) * s2 + (s1 - a[2]) * G2;
-  const T ulk[3] = {ul, vl, wl}, urk[3] = {ur, vr, wr};
-  const T unl = ul * n[0] + vl * n[1] + wl * n[2];
-  const T unr = ur * n[0] + vr * n[1] + wr * n[2];
 
-  // ---- reverse
-  T rlb = T(0), rrb = T(0), unlb = T(0), unrb = T(0), plb = T(0), prb = T(0), Hlb = T(0), Hrb = T(0);
-  T ulkb[3] = {T(0), T(0), T(0)}, urkb[3] = {T(0), T(0), T(0)}, ukb[3] = {T(0), T(0), T(0)};
-  T a3b = T(0), drb = T(0), dmb[3] = {T(0), T(0), T(0)}, dEb = T(0), Hb = T(0), unb = T(0);
-  const T h = T(0.5);
-  // central parts
-  rlb += h * fbar[0] * unl + h * fbar[4] * Hl * unl;
-  rrb += h * fbar[0] * unr + h * fbar[4] * Hr * unr;
-  unlb += h * fbar[0] * rl + h * fbar[4] * rl * Hl;
-  unrb += h * fbar[0] * rr + h * fbar[4] * rr * Hr;
-  Hlb += h * fbar[4] * rl * unl;
-  Hrb += h * fbar[4] * rr * unr;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const T fb = fbar[1 + k];
-    rlb += h * fb * ulk[k] * unl;
-    rrb += h * fb * urk[k] * unr;
-    unlb += h * fb * rl * ulk[k];
-    unrb += h * fb * rr * urk[k];
-    ulkb[k] += h * fb * rl * unl;
-    urkb[k] += h * fb * rr * unr;
-    plb += h * fb * n[k];
-    prb += h * fb * n[k];
-  }
-  // dissipation: -1/2 (a3 dr + C1), -1/2 (a3 dm_k + C1 u_k + C2 n_k), -1/2 (a3 dE + C1 H + C2 un)
-  a3b += -h * (fbar[0] * dr + fbar[1] * dm[0] + fbar[2] * dm[1] + fbar[3] * dm[2] + fbar[4] * dE);
-  drb += -h * fbar[0] * a[2];
-  dEb += -h * fbar[4] * a[2];
+  // ---- reverse: -1/2 (a3 dr + C1), -1/2 (a3 dm_k + C1 u_k + C2 n_k), -1/2 (a3 dE + C1 H + C2 un)
+  T ukb[3], Hb, unb, drb, dmb[3], dEb;
+  T a3b = -h * (fbar[0] * dr + fbar[1] * dm[0] + fbar[2] * dm[1] + fbar[3] * dm[2] + fbar[4] * dE);
+  drb = -h * fbar[0] * a[2];
+  dEb = -h * fbar[4] * a[2];
   T C1b = -h * (fbar[0] + fbar[4] * H);
   T C2b = -h * fbar[4] * un;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    dmb[k] += -h * fbar[1 + k] * a[2];
+    dmb[k] = -h * fbar[1 + k] * a[2];
     C1b += -h * fbar[1 + k] * uk[k];
     C2b += -h * fbar[1 + k] * n[k];
-    ukb[k] += -h * fbar[1 + k] * C1;
+    ukb[k] = -h * fbar[1 + k] * C1;
   }
-  Hb += -h * fbar[4] * C1;
-  unb += -h * fbar[4] * C2;
-  // unl = ulk . n, unr = urk . n
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    ulkb[k] += unlb * n[k];
-    urkb[k] += unrb * n[k];
-  }
+  Hb = -h * fbar[4] * C1;
+  unb = -h * fbar[4] * C2;
   // C1 = G1 ic^2 (s1 - a3) + G2 ic s2 ; C2 = G1 ic s2 + (s1 - a3) G2
-  T G1b = C1b * ic * ic * (s1 - a[2]) + C2b * ic * s2;
-  T G2b = C1b * ic * s2 + C2b * (s1 - a[2]);
-  T icb = C1b * (T(2) * G1 * ic * (s1 - a[2]) + G2 * s2) + C2b * G1 * s2;
+  const T G1b = C1b * ic * ic * (s1 - a[2]) + C2b * ic * s2;
+  const T G2b = C1b * ic * s2 + C2b * (s1 - a[2]);
+  const T icb = C1b * (T(2) * G1 * ic * (s1 - a[2]) + G2 * s2) + C2b * G1 * s2;
   const T s1b = C1b * G1 * ic * ic + C2b * G2;
   const T s2b = C1b * G2 * ic + C2b * G1 * ic;
   a3b += -C1b * G1 * ic * ic - C2b * G2;
@@ -349,9 +357,8 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
     ukb[k] += -G1b * gm1 * dm[k];
     dmb[k] += -G1b * gm1 * uk[k];
   }
-  // s1, s2
-  T ab[3] = {h * (s1b + s2b), h * (s1b - s2b), a3b};
-  // a_i from l_i (with the entropy fix where it was taken)
+  // s1, s2, then a_i from l_i (with the entropy fix where it was taken)
+  const T ab[3] = {h * (s1b + s2b), h * (s1b - s2b), a3b};
   T lb[3], epsb = T(0);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -364,19 +371,16 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   }
   unb += lb[0] + lb[1] + lb[2];
   T cb = lb[0] - lb[1] + T(0.05) * epsb;
-  // un = uk . n
-#pragma unroll
-  for (int k = 0; k < 3; ++k) ukb[k] += unb * n[k];
-  // ic = 1/c ; c = sqrt(gm1 (H - q2/2))
+  // un = uk . n ; ic = 1/c ; c = sqrt(gm1 (H - q2/2)) ; q2 = |uk|^2
   cb += -icb * ic * ic;
   const T c2b = cb / (T(2) * c);
   Hb += gm1 * c2b;
   q2b += -h * gm1 * c2b;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) ukb[k] += T(2) * uk[k] * q2b;
-  // differences
-  rrb += drb;
-  rlb -= drb;
+  for (int k = 0; k < 3; ++k) ukb[k] += unb * n[k] + T(2) * uk[k] * q2b;
+  // the jumps
+  Urbar[0] += drb;
+  Ulbar[0] -= drb;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     Urbar[1 + k] += dmb[k];
@@ -384,46 +388,30 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   }
   Urbar[4] += dEb;
   Ulbar[4] -= dEb;
-  // Roe averages: uk = (sl ulk + sr urk) iden, H = (sl Hl + sr Hr) iden
-  T slb = Hb * Hl * iden, srb = Hb * Hr * iden;
-  T idenb = Hb * (sl * Hl + sr * Hr);
-  Hlb += Hb * sl * iden;
-  Hrb += Hb * sr * iden;
+  // the Roe average, side by side: uk = (sl ul + sr ur) iden, H likewise;
+  // d/d s_side = (side value - average) iden, d/d side value = s_side iden;
+  // then u = m / r, H = g E / r - (g - 1) |u|^2 / 2, s = sqrt(r)
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    slb += ukb[k] * ulk[k] * iden;
-    srb += ukb[k] * urk[k] * iden;
-    ulkb[k] += ukb[k] * sl * iden;
-    urkb[k] += ukb[k] * sr * iden;
-    idenb += ukb[k] * (sl * ulk[k] + sr * urk[k]);
-  }
-  const T sumb = -idenb * iden * iden;
-  slb += sumb;
-  srb += sumb;
-  rlb += slb / (T(2) * sl);
-  rrb += srb / (T(2) * sr);
-  // H_side = (U4 + p) ir ; p = gm1 (U4 - r q2/2) ; u = U_{1..3} ir
-  T irlb = Hlb * (Ul[4] + pl), irrb = Hrb * (Ur[4] + pr);
-  plb += Hlb * irl;
-  prb += Hrb * irr;
-  Ulbar[4] += Hlb * irl + gm1 * plb;
-  Urbar[4] += Hrb * irr + gm1 * prb;
-  rlb += -h * gm1 * ql2 * plb;
-  rrb += -h * gm1 * qr2 * prb;
+  for (int s = 0; s < 2; ++s) {
+    const T* U = s ? Ur : Ul;
+    T* Ub = s ? Urbar : Ulbar;
+    const T ir = T(1) / U[0], w = sq[s] * iden;
+    T sqb = Hb * (Hs[s] - H), ub[3], qs = T(0), uub = T(0);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    ulkb[k] += -gm1 * rl * ulk[k] * plb;
-    urkb[k] += -gm1 * rr * urk[k] * prb;
-    Ulbar[1 + k] += ulkb[k] * irl;
-    Urbar[1 + k] += urkb[k] * irr;
-    irlb += ulkb[k] * Ul[1 + k];
-    irrb += urkb[k] * Ur[1 + k];
+    for (int k = 0; k < 3; ++k) {
+      sqb += ukb[k] * (us[s][k] - uk[k]);
+      ub[k] = ukb[k] * w;
+      qs += us[s][k] * us[s][k];
+      uub += ub[k] * us[s][k];
+    }
+    const T Hsb = Hb * w;
+    Ub[4] += Hsb * g * ir;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Ub[1 + k] += (ub[k] - Hsb * gm1 * us[s][k]) * ir;
+    Ub[0] += sqb * iden / (T(2) * sq[s]) + (-uub + Hsb * (gm1 * qs - g * U[4] * ir)) * ir;
   }
-  rlb += -irlb * irl * irl;
-  rrb += -irrb * irr * irr;
-  Ulbar[0] += rlb;
-  Urbar[0] += rrb;
 }
+
 
 // Boundary ghost state (boundary_state): Ubbar -> ULbar for every boundary
 // type.  Subsonic inflow depends on UL only through the outgoing Riemann
