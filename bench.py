@@ -432,8 +432,9 @@ def _channel_case(dg):
 
 
 def _geometry_block(dg, torch, reps=3):
-    """Set-up cost: wall time of dgb_create, whose element geometry is built
-    on the device (geometry.cu), beside the host builder on the same mesh
+    """Set-up cost: wall time of dgb_create (allocations included), and of
+    the element geometry it builds on the device (geometry.cu;
+    dgb_geometry_stats), beside the host builder on the same mesh
     (dgb_geometry_host, all host threads up to 64; it excludes the
     host-to-device copy of its output that a host-built handle also needs).
     Curved: the channel mesh (per-point geometry); affine: the 48^3 p = 4
@@ -445,20 +446,21 @@ def _geometry_block(dg, torch, reps=3):
     mesh_a = dg.Mesh(n3, n3, n3, 4, 1, C.box_nodes(n3, n3, n3, 1, L_BOX, L_BOX, L_BOX), [dg.PERIODIC] * 6)
     out = {"host_threads": min(64, os.cpu_count() or 1)}
     for name, mesh, prm in (("channel_curved", mesh_c, prm_c), ("tgv48_p4_affine", mesh_a, C.params())):
-        create, host = [], []
+        create, build, host = [], [], []
         for _ in range(reps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             s = dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64)
             torch.cuda.synchronize()
             create.append(time.perf_counter() - t0)
+            build.append(s.geometry_stats()[1])
             s.close()
             t0 = time.perf_counter()
             dg.geometry_host(mesh, curved=mesh.q > 1)
             host.append(time.perf_counter() - t0)
         E = mesh.nx * mesh.ny * mesh.nz
         out[name] = {"elements": E, "p": mesh.p, "q": mesh.q, "create_s": float(np.median(create)),
-                     "host_builder_s": float(np.median(host))}
+                     "device_geometry_build_s": float(np.median(build)), "host_builder_s": float(np.median(host))}
     return out
 
 

@@ -128,6 +128,7 @@ def lib():
             "dgb_lagrange1d_deriv": (ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_double]),
             "dgb_bump_nodes": (ctypes.c_int, [ctypes.c_int] * 4 + [ctypes.c_double] * 7 + [_dp]),
             "dgb_get_geometry": (ctypes.c_int, [vp, ctypes.c_int, _dp, ctypes.c_size_t]),
+            "dgb_geometry_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
             "dgb_geometry_host": (ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(ctypes.c_int),
                                                  _dp, ctypes.c_size_t, _dp, ctypes.c_size_t, _dp,
                                                  ctypes.c_size_t]),
@@ -342,6 +343,12 @@ class Solver:
         U = np.zeros(self.n)
         _check(lib().dgb_get_state(self.h, _p(U)))
         return U
+
+    def geometry_stats(self):
+        """(curved, seconds dgb_create spent building the geometry on the device)."""
+        cv, t = ctypes.c_int(), ctypes.c_double()
+        _check(lib().dgb_geometry_stats(self.h, ctypes.byref(cv), ctypes.byref(t)))
+        return bool(cv.value), t.value
 
     def geometry(self, part=GEO_ELEMENT):
         """The device-built element geometry (dgb_get_geometry), flat."""

@@ -312,6 +312,59 @@ __device__ __forceinline__ void gface_test_transpose(int half, const double* sv,
   __syncthreads();
 }
 
+// Inputs of one boundary face point of adjA (passed by value to a function
+// that is not inlined).
+struct AdjWallIn {
+  double Uo[5], n[3], ab[5], zb[5], dcb[3][5], fw, lift;
+};
+
+// The adjoint of a boundary face point's fluxes (ghost state, its Euler flux,
+// dual consistency, BR2 lifting, the ghost state's own VJP), written to the
+// point's slots of TA: T[c * NQF] for c < 20.  Not inlined: boundary points
+// are rare, and inlined their registers would count on every path.
+static __device__ __noinline__ void adj_boundary_face_point(const AdjWallIn in, int nb, const DevParams prm, double gamma,
+                                                     double mu, double kq, int* flag, double* T, int NQF)
+{
+  double Uob[5] = {0., 0., 0., 0., 0.}, Qob[5];
+  double Ubd[5], Ubb[5] = {0., 0., 0., 0., 0.};
+  boundary_state(nb, in.Uo, in.n, prm, Ubd);
+  {
+    double fb[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) fb[r] = in.fw * in.ab[r];
+    euler_flux_n_vjp(Ubd, gamma, in.n, fb, Ubb);
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r) Qob[r] = -in.fw * in.ab[r];
+  if (mu != 0.) {
+    double d[5], dbar[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+    for (int r = 0; r < 5; ++r) d[r] = in.Uo[r] - Ubd[r];
+    visc_rank1_vjp(in.Uo, d, in.n, mu, in.dcb, Uob, dbar, kq);
+    const double co = in.fw * in.lift;
+    double rbb[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) rbb[r] = co * in.zb[r];
+    visc_jump_n_vjp(Ubd, d, in.n, mu, rbb, Ubb, dbar, kq);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      Uob[r] += dbar[r];
+      Ubb[r] -= dbar[r];
+    }
+  }
+  // an isothermal wall point leaves its dJ/dTw term (Ub[4] = r R Tw / (gamma - 1)) in the
+  // first slot of the neighbour half of TA, which no element reads for a boundary face
+  const double wall_term = nb == -8 ? Ubb[4] * in.Uo[0] * (prm.R / (prm.gamma - 1.)) : 0.;
+  if (boundary_state_vjp(nb, in.Uo, in.n, prm, Ubb, Uob) && flag) atomicOr(flag, 8);
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    T[r * NQF] = Uob[r];
+    T[(5 + r) * NQF] = Qob[r];
+    T[(10 + r) * NQF] = r == 0 ? wall_term : 0.;
+    T[(15 + r) * NQF] = 0.;
+  }
+}
+
 template <int P>
 struct AdjASmem {
   using C = Cfg<P>;
@@ -639,48 +692,27 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
           TAe[(10 + r) * NQF + fq] = Unb[r];
           TAe[(15 + r) * NQF + fq] = -Qob[r];
         }
-      } else {
-        double Ubd[5], Ubb[5] = {0., 0., 0., 0., 0.};
-        boundary_state(nb, Uo, n, prm, Ubd);
-        {
-          double fb[5];
-#pragma unroll
-          for (int r = 0; r < 5; ++r) fb[r] = fw * ab[r];
-          euler_flux_n_vjp(Ubd, gamma, n, fb, Ubb);
-        }
-#pragma unroll
-        for (int r = 0; r < 5; ++r) Qob[r] = -fw * ab[r];
-        if (mu != 0.) {
-          double d[5], dbar[5] = {0., 0., 0., 0., 0.};
-#pragma unroll
-          for (int r = 0; r < 5; ++r) d[r] = Uo[r] - Ubd[r];
-          {
-            double dcb[3][5];
-            dual_bar(dcb);
-            visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
-          }
-          const double co = fw * lift;
-          double rbb[5];
-#pragma unroll
-          for (int r = 0; r < 5; ++r) rbb[r] = co * zb[r];
-          visc_jump_n_vjp(Ubd, d, n, mu, rbb, Ubb, dbar, kq);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            Uob[r] += dbar[r];
-            Ubb[r] -= dbar[r];
-          }
-        }
-        // an isothermal wall point leaves its dJ/dTw term (Ub[4] = r R Tw / (gamma - 1)) in the
-        // first slot of the neighbour half of TA, which no element reads for a boundary face
-        const double wall_term = nb == -8 ? Ubb[4] * Uo[0] * (prm.R / (prm.gamma - 1.)) : 0.;
-        if (boundary_state_vjp(nb, Uo, n, prm, Ubb, Uob) && flag) atomicOr(flag, 8);
+      } else {  // boundary face point: a call, so its registers stay out of the interior path
+        AdjWallIn in;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
-          TAe[r * NQF + fq] = Uob[r];
-          TAe[(5 + r) * NQF + fq] = Qob[r];
-          TAe[(10 + r) * NQF + fq] = r == 0 ? wall_term : 0.;
-          TAe[(15 + r) * NQF + fq] = 0.;
+          in.Uo[r] = Uo[r];
+          in.ab[r] = ab[r];
+          in.zb[r] = zb[r];
         }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) in.n[c] = n[c];
+        if (mu != 0.) {
+          dual_bar(in.dcb);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < 5; ++r) in.dcb[c][r] = 0.;
+        }
+        in.fw = fw;
+        in.lift = lift;
+        adj_boundary_face_point(in, nb, prm, gamma, mu, kq, flag, TAe + fq, NQF);
       }
     }
     __syncthreads();

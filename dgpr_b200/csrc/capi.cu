@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -306,7 +307,9 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMemcpy(h->d_ops, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
   CKF(cudaMemcpy(h->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
   // element geometry, built on the device (geometry.cu)
+  const auto g0 = std::chrono::steady_clock::now();
   rc = build_geometry_device(*mesh, h->ops, nbr, h->d_nbr, h->stream, h->d_geo, &h->d_gv, &h->d_gf, h->curved, why);
+  h->geometry_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - g0).count();
   if (rc) {
     fail(rc, why);
     free_all(h);
@@ -343,6 +346,14 @@ int dgb_get_geometry(dgb_handle* h, int part, double* out, size_t count)
   cudaSetDevice(h->device);
   CK(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return DGB_OK;
+}
+
+int dgb_geometry_stats(const dgb_handle* h, int* curved, double* build_seconds)
+{
+  if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (curved) *curved = h->curved ? 1 : 0;
+  if (build_seconds) *build_seconds = h->geometry_s;
   return DGB_OK;
 }
 

@@ -32,6 +32,7 @@ struct dgb_handle {
   float* d_opsf = nullptr;    // operator table for the mixed form
   double* d_geo = nullptr;
   bool curved = false;         // per-point geometry (non-affine elements)
+  double geometry_s = 0.;      // host wall time of the device geometry build in dgb_create
   double* d_gv = nullptr;      // [E][kVolC][P^3]
   double* d_gf = nullptr;      // [E][6][kFaceC][P^2]
   int* d_nbr = nullptr;

@@ -462,9 +462,11 @@ __global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const d
 // with an even element count.  Face traces are kept pair-interleaved,
 // Tr2[k][lf][10][NQF] of (e0, e1) values; interior faces run paired, and a
 // face point where either element meets a boundary runs each element's
-// lane through the scalar FP32 face routine.
+// lane through the scalar FP32 face routine (a call, pair_face_lane).  96
+// registers (10 CTAs per SM) measured faster than 128 (8 CTAs) once the
+// boundary lanes were out of the inlined path.
 #ifndef DGB_STAGE_REGS_F2
-#define DGB_STAGE_REGS_F2 128
+#define DGB_STAGE_REGS_F2 96
 #endif
 
 template <int P>
@@ -521,6 +523,41 @@ vtrace2_kernel(long E, const double* __restrict__ V, const float* __restrict__ o
     if (half) __syncthreads();
     vtrace_half<P, f2, false>(half, sV, sN, so, sg, f2(prm.mu), HT ? f2(prm.kq) : f2(0.f), Te, nullptr);
   }
+}
+
+// One lane of a paired face point where either element meets a boundary,
+// through the scalar FP32 face routine.  Not inlined: a call keeps the
+// boundary code's registers out of the paired kernel's allocation (taken
+// only at boundary faces).
+template <int P, bool HT>
+__device__ __noinline__ void pair_face_lane(int l, int nb, int lf, int fq, const f2* To, const f2* __restrict__ Tr2,
+                                            const float* sof, const float* sgl, const double* __restrict__ geo,
+                                            const DevParams prm, int* flag, f2* fa, f2* fb)
+{
+  using C = Cfg<P>;
+  constexpr int NQF = C::NQF;
+  float Uo[5], Qo[5], Un[5], Qn[5], lift_n = 0.f, fal[5], fbl[12];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    Uo[r] = To[r * NQF + fq].lane(l);
+    Qo[r] = To[(5 + r) * NQF + fq].lane(l);
+  }
+  if (nb >= 0) {
+    const long in = ((long)(nb / 2) * 6 + (lf ^ 1)) * 10 * NQF + fq;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      Un[r] = pair_lane(Tr2, in + r * NQF, nb);
+      Qn[r] = pair_lane(Tr2, in + (5 + r) * NQF, nb);
+    }
+    lift_n = sof[C::oC + ((lf & 1) ^ 1)] / (float)geo[(long)nb * kGeoStride + kGeoDetJ];
+  }
+  face_point_fluxes<P, float, false, 1>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, sof, sgl, nullptr, prm,
+                                        (float)prm.gamma, (float)prm.mu, HT ? (float)prm.kq : 0.f,
+                                        sgl[kGeoDetJ], sgl + kGeoJinv, flag, fal, fbl);
+#pragma unroll
+  for (int r = 0; r < 5; ++r) reinterpret_cast<float*>(fa + r * NQF)[l] = fal[r];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) reinterpret_cast<float*>(fb + i * NQF)[l] = fbl[i];
 }
 
 template <int P, bool HT>
@@ -665,32 +702,9 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
                                        Ji, sa.flag, fa, fb);
       } else {  // a boundary in either lane: each lane through the scalar routine
 #pragma unroll 1
-        for (int l = 0; l < 2; ++l) {
-          const int nb = l ? nb1 : nb0;
-          const float* sgl = sgf + l * kGeoStride;
-          float Uo[5], Qo[5], Un[5], Qn[5], lift_n = 0.f, fal[5], fbl[12];
-#pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            Uo[r] = To[r * NQF + fq].lane(l);
-            Qo[r] = To[(5 + r) * NQF + fq].lane(l);
-          }
-          if (nb >= 0) {
-            const long in = ((long)(nb / 2) * 6 + (lf ^ 1)) * 10 * NQF + fq;
-#pragma unroll
-            for (int r = 0; r < 5; ++r) {
-              Un[r] = pair_lane(Tr2, in + r * NQF, nb);
-              Qn[r] = pair_lane(Tr2, in + (5 + r) * NQF, nb);
-            }
-            lift_n = sof[C::oC + ((lf & 1) ^ 1)] / (float)geo[(long)nb * kGeoStride + kGeoDetJ];
-          }
-          face_point_fluxes<P, float, false, 1>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, sof, sgl, nullptr, prm,
-                                                (float)prm.gamma, (float)prm.mu, HT ? (float)prm.kq : 0.f,
-                                                sgl[kGeoDetJ], sgl + kGeoJinv, sa.flag, fal, fbl);
-#pragma unroll
-          for (int r = 0; r < 5; ++r) reinterpret_cast<float*>(fa + r * NQF)[l] = fal[r];
-#pragma unroll
-          for (int i = 0; i < 12; ++i) reinterpret_cast<float*>(fb + i * NQF)[l] = fbl[i];
-        }
+        for (int l = 0; l < 2; ++l)
+          pair_face_lane<P, HT>(l, l ? nb1 : nb0, lf, fq, To, Tr2, sof, sgf + l * kGeoStride, geo, prm, sa.flag,
+                                fa, fb);
       }
     }
     __syncthreads();

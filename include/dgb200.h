@@ -124,6 +124,12 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
 enum { DGB_GEO_ELEMENT = 0, DGB_GEO_VOLUME = 1, DGB_GEO_FACE = 2 };
 int dgb_get_geometry(dgb_handle* h, int part, double* out, size_t count);
 
+/* Whether the mesh got per-point geometry, and the host wall time dgb_create
+ * spent building the element geometry on the device (node upload, kernels
+ * and checks; the handle's other allocations excluded).  Either output may
+ * be NULL. */
+int dgb_geometry_stats(const dgb_handle* h, int* curved, double* build_seconds);
+
 /* Frees everything dgb_create allocated.  Replaces free_cuda_device_geometry
  * (solve_cuda.cu:267) and free_cuda_residual_workspace (solve_cuda.cu:323). */
 int dgb_destroy(dgb_handle* h);

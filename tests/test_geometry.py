@@ -148,6 +148,8 @@ def test_device_geometry_is_bit_identical_to_the_host_builder():
     for c in _device_cases():
         curved, geo, gv, gf = dg.geometry_host(_mesh(c))
         with dg.Solver(_mesh(c), C.params()) as s:
+            cv, build_s = s.geometry_stats()
+            assert cv == curved and build_s > 0.0, c.name
             assert np.array_equal(s.geometry(dg.GEO_ELEMENT), geo), c.name
             if curved:
                 assert np.array_equal(s.geometry(dg.GEO_VOLUME), gv), c.name
