@@ -442,15 +442,20 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
       for (int r = 0; r < 5; ++r) qd[r] = T(0.5) * (Qo[r] - Qn[r]);
       // Roe flux in one orientation for both sides: the element that sees
       // the face on its high side is "left"; the other side negates it
-      T UL[5], UR[5], F[5];
+      T F[5];
       const T sgn = end ? T(1) : T(-1);
+      if constexpr (!std::is_same<T, double>::value) {  // FP32 and pairs measured better with the copies
+        T UL[5], UR[5];
 #pragma unroll
-      for (int r = 0; r < 5; ++r) {
-        UL[r] = end ? Uo[r] : Un[r];
-        UR[r] = end ? Un[r] : Uo[r];
+        for (int r = 0; r < 5; ++r) {
+          UL[r] = end ? Uo[r] : Un[r];
+          UR[r] = end ? Un[r] : Uo[r];
+        }
+        const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
+        roe_flux(UL, UR, nn, gamma, F);
+      } else {
+        roe_flux_oriented(Uo, Un, end, n, gamma, F);
       }
-      const T nn[3] = {sgn * n[0], sgn * n[1], sgn * n[2]};
-      roe_flux(UL, UR, nn, gamma, F);
 #pragma unroll
       for (int r = 0; r < 5; ++r) fa[r * OS] = sgn * F[r] - qd[r];
     }
