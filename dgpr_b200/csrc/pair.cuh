@@ -13,6 +13,15 @@
 #include <cmath>
 #include <type_traits>
 
+// Products are kept unrounded (f2mul) until they meet an addition, which
+// then becomes one __ffma2_rn: `a * b + c` contracts into a fused
+// multiply-add as the scalar compiler does for float.  Anywhere else an
+// f2mul rounds to f2 (one __fmul2_rn).  DGB_PAIR_CONTRACT 0 keeps every
+// product rounded.
+#ifndef DGB_PAIR_CONTRACT
+#define DGB_PAIR_CONTRACT 1
+#endif
+
 namespace dgb {
 
 // the scalar overloads stay visible beside the f2 ones declared below
@@ -44,6 +53,10 @@ __host__ __device__ inline f2 operator+(f2 a, f2 b)
   return f2(a.v.x + b.v.x, a.v.y + b.v.y);
 #endif
 }
+#if DGB_PAIR_CONTRACT
+struct f2mul;
+__host__ __device__ inline f2mul operator*(f2 a, f2 b);
+#else
 __host__ __device__ inline f2 operator*(f2 a, f2 b)
 {
 #ifdef __CUDA_ARCH__
@@ -53,12 +66,21 @@ __host__ __device__ inline f2 operator*(f2 a, f2 b)
   return f2(a.v.x * b.v.x, a.v.y * b.v.y);
 #endif
 }
+#endif
 __host__ __device__ inline f2 operator-(f2 a) { return f2(-a.v.x, -a.v.y); }
 __host__ __device__ inline f2 operator-(f2 a, f2 b) { return a + (-b); }
 __host__ __device__ inline f2 operator/(f2 a, f2 b) { return f2(a.v.x / b.v.x, a.v.y / b.v.y); }
 __host__ __device__ inline f2& operator+=(f2& a, f2 b) { return a = a + b; }
 __host__ __device__ inline f2& operator-=(f2& a, f2 b) { return a = a - b; }
-__host__ __device__ inline f2& operator*=(f2& a, f2 b) { return a = a * b; }
+__host__ __device__ inline f2& operator*=(f2& a, f2 b)
+{
+#ifdef __CUDA_ARCH__
+  const float2 r = __fmul2_rn(a.v, b.v);
+  return a = f2(r.x, r.y);
+#else
+  return a = f2(a.v.x * b.v.x, a.v.y * b.v.y);
+#endif
+}
 // branch conditions on values both lanes share
 __host__ __device__ inline bool operator!=(f2 a, f2 b) { return a.v.x != b.v.x || a.v.y != b.v.y; }
 __host__ __device__ inline bool operator==(f2 a, f2 b) { return !(a != b); }
@@ -74,6 +96,40 @@ __host__ __device__ inline f2 fma(f2 a, f2 b, f2 c)
 }
 __host__ __device__ inline f2 sqrt(f2 a) { return f2(sqrtf(a.v.x), sqrtf(a.v.y)); }
 __host__ __device__ inline f2 fabs(f2 a) { return f2(fabsf(a.v.x), fabsf(a.v.y)); }
+
+#if DGB_PAIR_CONTRACT
+struct f2mul {
+  f2 a, b;
+  __host__ __device__ operator f2() const
+  {
+#ifdef __CUDA_ARCH__
+    const float2 r = __fmul2_rn(a.v, b.v);
+    return f2(r.x, r.y);
+#else
+    return f2(a.v.x * b.v.x, a.v.y * b.v.y);
+#endif
+  }
+};
+__host__ __device__ inline f2mul operator*(f2 a, f2 b) { return f2mul{a, b}; }
+__host__ __device__ inline f2 operator+(f2mul p, f2 c) { return fma(p.a, p.b, c); }
+__host__ __device__ inline f2 operator+(f2 c, f2mul p) { return fma(p.a, p.b, c); }
+__host__ __device__ inline f2 operator+(f2mul p, f2mul q) { return fma(p.a, p.b, f2(q)); }
+__host__ __device__ inline f2 operator-(f2mul p, f2 c) { return fma(p.a, p.b, -c); }
+__host__ __device__ inline f2 operator-(f2 c, f2mul p) { return fma(-p.a, p.b, c); }
+__host__ __device__ inline f2 operator-(f2mul p, f2mul q) { return fma(p.a, p.b, -f2(q)); }
+__host__ __device__ inline f2mul operator-(f2mul p) { return f2mul{-p.a, p.b}; }
+__host__ __device__ inline f2mul operator*(f2mul p, f2 c) { return f2mul{f2(p), c}; }
+__host__ __device__ inline f2mul operator*(f2 c, f2mul p) { return f2mul{c, f2(p)}; }
+__host__ __device__ inline f2mul operator*(f2mul p, f2mul q) { return f2mul{f2(p), f2(q)}; }
+__host__ __device__ inline f2 operator/(f2mul p, f2 c) { return f2(p) / c; }
+__host__ __device__ inline f2 operator/(f2 c, f2mul p) { return c / f2(p); }
+__host__ __device__ inline f2 operator/(f2mul p, f2mul q) { return f2(p) / f2(q); }
+__host__ __device__ inline f2& operator+=(f2& a, f2mul p) { return a = fma(p.a, p.b, a); }
+__host__ __device__ inline f2& operator-=(f2& a, f2mul p) { return a = fma(-p.a, p.b, a); }
+__host__ __device__ inline f2& operator*=(f2& a, f2mul p) { return a *= f2(p); }
+__host__ __device__ inline f2 sqrt(f2mul a) { return sqrt(f2(a)); }
+__host__ __device__ inline f2 fabs(f2mul a) { return fabs(f2(a)); }
+#endif
 
 // lane-wise: a < b ? x : y
 __host__ __device__ inline f2 select_lt(f2 a, f2 b, f2 x, f2 y)

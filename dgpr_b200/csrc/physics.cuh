@@ -212,7 +212,7 @@ DGB_HD void roe_dissipation(const T* Ul, const T* Ur, const T* n, T gm1, T u, T 
   T jump[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) jump[k] = Ur[k] - Ul[k];
-  roe_dissipation_jump(jump, n, gm1, u, v, w, H, d);
+  roe_dissipation_jump<T>(jump, n, gm1, u, v, w, H, d);
 }
 
 // f = 1/2 (F(Ul) + F(Ur)).n - 1/2 |A_roe| (Ur - Ul), the two sides taken in
@@ -245,7 +245,7 @@ DGB_HD void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
     }
     const T iden = T(1) / (sq[0] + sq[1]);
     T d[5];
-    roe_dissipation(Ul, Ur, n, gm1, (sa[0][0] + sa[1][0]) * iden, (sa[0][1] + sa[1][1]) * iden,
+    roe_dissipation<T>(Ul, Ur, n, gm1, (sa[0][0] + sa[1][0]) * iden, (sa[0][1] + sa[1][1]) * iden,
                     (sa[0][2] + sa[1][2]) * iden, (sa[0][3] + sa[1][3]) * iden, d);
 #pragma unroll
     for (int k = 0; k < 5; ++k) f[k] = T(0.5) * f[k] - T(0.5) * d[k];
@@ -258,7 +258,7 @@ DGB_HD void roe_flux(const T* Ul, const T* Ur, const T* n, T g, T* f)
     const T Hr = (Ur[4] + pr) * irr;
     const T sl = sqrt(rl), sr = sqrt(rr), iden = T(1) / (sl + sr);
     T d[5];
-    roe_dissipation(Ul, Ur, n, gm1, (sl * ul + sr * ur) * iden, (sl * vl + sr * vr) * iden,
+    roe_dissipation<T>(Ul, Ur, n, gm1, (sl * ul + sr * ur) * iden, (sl * vl + sr * vr) * iden,
                     (sl * wl + sr * wr) * iden, (sl * Hl + sr * Hr) * iden, d);
     const T unl = ul * n[0] + vl * n[1] + wl * n[2];
     const T unr = ur * n[0] + vr * n[1] + wr * n[2];
@@ -305,7 +305,7 @@ DGB_HD void roe_flux_oriented(const T* Uo, const T* Un, int end, const T* n, T g
 #pragma unroll
   for (int k = 0; k < 5; ++k) jump[k] = sgn * (Un[k] - Uo[k]);
   T d[5];
-  roe_dissipation_jump(jump, nn, gm1, (sa[0][0] + sa[1][0]) * iden, (sa[0][1] + sa[1][1]) * iden,
+  roe_dissipation_jump<T>(jump, nn, gm1, (sa[0][0] + sa[1][0]) * iden, (sa[0][1] + sa[1][1]) * iden,
                        (sa[0][2] + sa[1][2]) * iden, (sa[0][3] + sa[1][3]) * iden, d);
 #pragma unroll
   for (int k = 0; k < 5; ++k) f[k] = T(0.5) * f[k] - T(0.5) * d[k];
