@@ -13,7 +13,7 @@ on the handle's stream, max over ranks) of K graph-launched steps; `e2e` is the
 same metric through the C ABI with host buffers (pinned H2D of the state, the
 step, D2H of the state and the residual norm, every step).  Multi-GPU runs
 are independent replicas (weak scaling): the reference's multi-rank mode is a
-domain decomposition this build does not implement.
+domain decomposition this library does not implement.
 
 --impl reference: the reference's own FP64 CPU solver (compiled in place into
 oracle/_ref/) on the host cores, one process per core, each step a bounded

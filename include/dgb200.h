@@ -28,7 +28,7 @@ extern "C" {
 enum {
   DGB_OK = 0,
   DGB_ERR_ARG = 1,          /* bad argument, size or layout */
-  DGB_ERR_UNSUPPORTED = 2,  /* valid input outside what this build implements */
+  DGB_ERR_UNSUPPORTED = 2,  /* valid input outside what this library implements */
   DGB_ERR_CUDA = 3,         /* a CUDA runtime call failed */
   DGB_ERR_GEOMETRY = 4,     /* singular Jacobian / mass matrix, mismatched periodic bounds */
   DGB_ERR_NONFINITE = 5,    /* a residual or state value became NaN/Inf */

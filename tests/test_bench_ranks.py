@@ -68,7 +68,7 @@ def test_reference_arm_line_or_unavailable_on_rank_zero():
     """Rank 0 prints one JSON line: the reference's numbers, or `unavailable`."""
     import oracle
     if oracle.reference() is not None:
-        pytest.skip("the reference is built here: the full arm runs for minutes (exercised by the driver)")
+        pytest.skip("the reference is built here: the full arm runs for minutes")
 
     class A:
         steps, warmup = 1, 3

@@ -7,7 +7,7 @@ Tolerances:
       the flux divergence of the large background pressure cancels, so f is
       relatively less accurate than the state)
   state after 1000 RK4 steps of a Taylor-Green vortex,
-      relative L2 vs the FP64 form                    1e-6  (the north-star bound)
+      relative L2 vs the FP64 form                    1e-6  (the required bound)
 """
 import numpy as np
 import pytest

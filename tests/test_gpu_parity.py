@@ -7,7 +7,7 @@ Tolerances (relative L2 over the whole array):
                                         its exact tensor-product inverse; the two
                                         differ by rounding amplified by the mass
                                         matrix condition number)
-  state after N RK steps       1e-12   (the north-star bound on conserved variables)
+  state after N RK steps       1e-12   (the required bound on the conserved variables)
   per-step residual norms      1e-10
 """
 import numpy as np
