@@ -431,6 +431,71 @@ def _channel_case(dg):
     return mesh, prm, U0, dt
 
 
+def _channel_adjoint_block(dg, torch, nsteps, slots=50):
+    """The adjoint-at-scale configuration on config 5's channel: mixed-form
+    forward record (FP32 contractions and fluxes) of `nsteps` TVD-RK3 steps
+    with `slots` checkpoint buffers, then the FP64 adjoint sweep giving
+    dJ/dT_w for J = the mean wall shear stress of the y = 0 wall at the end
+    (functionals.wall_shear, with the box metric of the unmapped mesh; the
+    sinusoidal map leaves the walls flat).  dJ/dT_w is checked against central
+    differences of two FP64 forward runs with T_w moved by 1e-4 T_w.  The
+    isothermal wall, the heat flux and this gradient have no reference
+    counterpart."""
+    from dgpr_b200 import functionals as F
+    mesh, prm, U0, dt = _channel_case(dg)
+    lx, ly, lz = 4 * math.pi, 2.0, 2 * math.pi
+    quad = F.BoxQuadrature(mesh.nx, mesh.ny, mesh.nz, mesh.p, lx, ly, lz, device="cuda")
+    mu, Tw = prm[2], prm[4]
+
+    def J_of(U):
+        return F.wall_shear(U, quad, mu, wall="-y")
+
+    out = {"workload": f"channel {mesh.nx}x{mesh.ny}x{mesh.nz} p = {mesh.p} q = {mesh.q}, isothermal walls at "
+                       f"T_w = {Tw:.4g}, Pr 0.71, {nsteps} TVD-RK3 steps dt={dt:.3e}; J = mean wall shear of "
+                       f"the y = 0 wall; mixed forward, FP64 adjoint, {slots} checkpoint slots"}
+    with dg.Solver(mesh, dg.Params.from_array(prm), dg.MIXED_FP32) as s:
+        s.set_prandtl(0.71)
+        s.set_state(U0)
+        s.step(dg.TVDRK3, dt, 3, norms=False)  # warm-up
+        s.set_state(U0)
+        s.forward_record(dg.TVDRK3, dt, 2, 2, norms=False)
+        s.backward(np.zeros(U0.size))  # warm-up of the sweep
+        s.set_state(U0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.step(dg.TVDRK3, dt, nsteps, norms=False)
+        torch.cuda.synchronize()
+        plain = time.perf_counter() - t0
+        s.set_state(U0)
+        t0 = time.perf_counter()
+        s.forward_record(dg.TVDRK3, dt, nsteps, slots, norms=False)
+        torch.cuda.synchronize()
+        rec = time.perf_counter() - t0
+        UN = torch.tensor(s.get_state(), device="cuda", requires_grad=True)
+        J = J_of(UN)
+        J.backward()
+        lamN = UN.grad.cpu().numpy()
+        t0 = time.perf_counter()
+        _, dp = s.backward_params(lamN)
+        back = time.perf_counter() - t0
+        fwd, rev, _ = s.adjoint_stats()
+    with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
+        s.set_prandtl(0.71)
+        h = 1e-4 * Tw
+        Js = []
+        for t in (Tw + h, Tw - h):
+            s.set_wall_temperature(t)
+            s.set_state(U0)
+            s.step(dg.TVDRK3, dt, nsteps, norms=False)
+            Js.append(float(J_of(torch.tensor(s.get_state(), device="cuda"))))
+        fd = (Js[0] - Js[1]) / (2 * h)
+    an = float(dp[dg.DPARAM_TWALL])
+    out.update({"J": float(J), "dJ_dTw": an, "dJ_dTw_fd_fp64": fd, "rel_err": abs(an - fd) / abs(fd),
+                "plain_forward_s": plain, "recorded_forward_s": rec, "backward_s": back,
+                "backward_over_plain_forward": back / plain, "recomputed_steps": fwd, "reversed_steps": rev})
+    return out
+
+
 def _geometry_block(dg, torch, reps=3):
     """Set-up cost: wall time of dgb_create (allocations included), and of
     the element geometry it builds on the device (geometry.cu;
@@ -582,6 +647,8 @@ def run_ours(args, rank, world, local_rank):
     heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
     channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
     geometry = _geometry_block(dg, torch) if rank == 0 and not args.no_geometry else None
+    chadj = (_channel_adjoint_block(dg, torch, args.channel_adjoint_steps)
+             if rank == 0 and not args.no_channel and args.channel_adjoint_steps > 0 else None)
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
     peaks = {}
@@ -630,6 +697,7 @@ def run_ours(args, rank, world, local_rank):
             "heat": heat,
             "channel": channel,
             "geometry": geometry,
+            "channel_adjoint": chadj,
             "clocks": clocks,
         }
         if cpu:
@@ -648,6 +716,8 @@ def main():
     ap.add_argument("--no-heat", action="store_true", help="skip the heat-conduction block")
     ap.add_argument("--no-channel", action="store_true", help="skip the channel (isothermal walls) block")
     ap.add_argument("--no-geometry", action="store_true", help="skip the set-up (geometry build) timing")
+    ap.add_argument("--channel-adjoint-steps", type=int, default=500,
+                    help="TVD-RK3 steps of the channel adjoint block (0 or --no-channel skips it)")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")
