@@ -92,16 +92,17 @@ __global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __rest
 }
 
 // dpar[0] += the isothermal-wall points' dJ/dTw terms, which adjA leaves in
-// ta[e][lf][10][NQF] of every face with nbr == -8; fixed order
-__global__ void wall_terms_kernel(long E, int nqf, const int* __restrict__ nbr, const double* __restrict__ ta,
+// ta[e][lf][10][NQF] of every face with nbr == -8 (the nf faces 6 e + lf of
+// wallf); fixed order
+__global__ void wall_terms_kernel(long nf, int nqf, const int* __restrict__ wallf, const double* __restrict__ ta,
                                   double* dpar)
 {
   __shared__ double red[256];
   const int tid = threadIdx.x;
   double acc = 0.;
-  for (long i = tid; i < E * 6 * nqf; i += blockDim.x) {
-    const long ef = i / nqf;
-    if (nbr[ef] == -8) acc += ta[(ef * 20 + 10) * nqf + i % nqf];
+  for (long i = tid; i < nf * nqf; i += blockDim.x) {
+    const long ef = wallf[i / nqf];
+    acc += ta[(ef * 20 + 10) * nqf + i % nqf];
   }
   red[tid] = acc;
   __syncthreads();
@@ -267,8 +268,8 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     const int r = enqueue_param_terms(h, w, dpar, gauss);
     if (r) return r;
     CK(vjp_launch(w));
-    if (h->isothermal) {  // the VJP left the isothermal walls' dJ/dTw terms in its trace adjoints
-      wall_terms_kernel<<<1, 256, 0, h->stream>>>(h->E, h->NQF, h->d_nbr, sc.ta, dpar + DGB_DPARAM_TWALL);
+    if (h->n_wallf) {  // the VJP left the isothermal walls' dJ/dTw terms in its trace adjoints
+      wall_terms_kernel<<<1, 256, 0, h->stream>>>(h->n_wallf, h->NQF, h->d_wallf, sc.ta, dpar + DGB_DPARAM_TWALL);
       CK(cudaGetLastError());
     }
     return DGB_OK;

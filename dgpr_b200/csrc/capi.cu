@@ -112,7 +112,7 @@ long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == D
 void free_all(dgb_handle* h)
 {
   drop_step_graphs(h);
-  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_mean, h->d_U, h->d_V, h->d_Us, h->d_acc, h->d_trace[0],
+  void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_wallf, h->d_mean, h->d_U, h->d_V, h->d_Us, h->d_acc, h->d_trace[0],
                   h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
                   h->d_counter, h->d_flag};
   for (void* p : ptrs)
@@ -306,6 +306,16 @@ int dgb_create(const dgb_mesh_desc* mesh, const dgb_params* params, int precisio
   CKF(cudaMalloc(&h->d_flag, sizeof(int)));
   CKF(cudaMemcpy(h->d_ops, table.data(), sizeof(double) * table.size(), cudaMemcpyHostToDevice));
   CKF(cudaMemcpy(h->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
+  {  // the isothermal-wall faces, for the dJ/dTw sum of the adjoint
+    std::vector<int> wf;
+    for (size_t i = 0; i < nbr.size(); ++i)
+      if (nbr[i] == DGB_BT_ISOTHERMAL_WALL) wf.push_back((int)i);
+    h->n_wallf = (long)wf.size();
+    if (!wf.empty()) {
+      CKF(cudaMalloc(&h->d_wallf, sizeof(int) * wf.size()));
+      CKF(cudaMemcpy(h->d_wallf, wf.data(), sizeof(int) * wf.size(), cudaMemcpyHostToDevice));
+    }
+  }
   // element geometry, built on the device (geometry.cu)
   const auto g0 = std::chrono::steady_clock::now();
   rc = build_geometry_device(*mesh, h->ops, nbr, h->d_nbr, h->stream, h->d_geo, &h->d_gv, &h->d_gf, h->curved, why);

@@ -36,6 +36,8 @@ struct dgb_handle {
   double* d_gv = nullptr;      // [E][kVolC][P^3]
   double* d_gf = nullptr;      // [E][6][kFaceC][P^2]
   int* d_nbr = nullptr;
+  int* d_wallf = nullptr;  // faces 6 e + lf on isothermal walls (btype -8), in element order
+  long n_wallf = 0;
   double* d_U = nullptr;      // resident state
   double* d_Us = nullptr;     // stage state
   double* d_acc = nullptr;    // RK4 accumulator
