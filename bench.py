@@ -35,6 +35,10 @@ import numpy as np  # noqa: E402
 
 METRIC = "RK-stage DOF-updates/s (FP64, TGV 32^3 p=3 RK4)"
 UNIT = "DOF-updates/s"
+# B200 FP64 arithmetic peak: 148 SMs x 64 FP64 FMA lanes x 2 flop x 1.965 GHz
+# (nominal; the FP64 rate is not among the measured peaks)
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+FP64_PEAK_SOURCE = "nominal: 148 SMs x 64 FP64 FMA/clk x 2 x 1965 MHz"
 N_EL = 32
 P_ORD = 3
 L_BOX = 2 * math.pi
@@ -49,19 +53,20 @@ def tgv_case(n, p):
     return nodes, prm, U, dt
 
 
-def config(extra=None):
-    c = {"workload": "Taylor-Green vortex Re=1600 Ma=0.1, periodic [0,2pi]^3, 32^3 hexes, p=3, BR2, RK4, FP64",
-         "nelem": N_EL ** 3, "p": P_ORD, "dof_per_stage": 5 * (P_ORD + 1) ** 3 * N_EL ** 3,
-         "scheme": "RK4", "l2_between_steps": "inputs larger than L2 (trace buffer 252 MB + 3 state arrays 84 MB each)"}
-    if extra:
-        c.update(extra)
-    return c
+def config():
+    """The workload both arms report (the same dict in both lines)."""
+    return {"workload": f"Taylor-Green vortex Re=1600 Ma=0.1, periodic [0,2pi]^3, {N_EL}^3 hexes, p={P_ORD}, BR2, "
+                        f"RK4, FP64",
+            "nelem": N_EL ** 3, "p": P_ORD, "dof_per_stage": 5 * (P_ORD + 1) ** 3 * N_EL ** 3,
+            "scheme": "RK4", "l2_between_steps": "inputs larger than L2 (trace buffer 252 MB + 3 state arrays "
+                                                 "84 MB each)"}
 
 
 # ------------------------------------------------------------- reference arm
 
 def _ref_worker(args):
-    """One process: the reference solver on a small block of the TGV mesh."""
+    """One process: the reference solver on a small block of the TGV mesh.
+    Returns the stage time (s) of its RK4 step, geometry set-up excluded."""
     nsteps, n = args
     import oracle
     ref = oracle.reference()
@@ -81,7 +86,7 @@ REF_BLOCK = 6  # elements per direction of one reference process's sample block
 
 def cpu_rate(nsteps, n, procs, pool=None):
     """DOF-updates/s of `procs` concurrent reference processes (a spawn pool
-    is made for the call unless one is passed in)."""
+    is made for the call unless one is passed in), and their stage times."""
     import multiprocessing as mp
     if pool is None:
         with mp.get_context("spawn").Pool(procs) as p:
@@ -91,7 +96,26 @@ def cpu_rate(nsteps, n, procs, pool=None):
     return sum(dof / s for s in stage_s), stage_s
 
 
+def host_cores():
+    """(logical, physical) host core counts."""
+    logical = os.cpu_count() or 1
+    physical = None
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False)
+    except ImportError:
+        pass
+    return logical, physical
+
+
 def run_reference(args, rank, world):
+    """The reference's own FP64 CPU solver on every host thread.  A step is
+    one sample: every process runs one RK4 step of a 6^3 block of the TGV
+    mesh (periodic, same p, so the same work per element), all processes at
+    once.  `value` is the summed DOF-updates/s of the processes (median over
+    steps); `ms_per_step` is the measured time of a sample step (the mean
+    over processes of their RK4 step), not the cost of a full 32^3 step,
+    which is reported beside it as an extrapolation."""
     if rank != 0:
         return
     import oracle
@@ -100,26 +124,36 @@ def run_reference(args, rank, world):
                           "(the reference tree is needed to compile it)"}))
         return
     import multiprocessing as mp
-    procs = os.cpu_count() or 1
+    procs, physical = host_cores()
     n = REF_BLOCK
-    rates = []
+    rates, step_s = [], []
     with mp.get_context("spawn").Pool(procs) as pool:  # one pool for the run
         for i in range(args.warmup + args.steps):
-            r, _ = cpu_rate(1, n, procs, pool)
+            r, st = cpu_rate(1, n, procs, pool)
             if i >= args.warmup:
                 rates.append(r)
+                step_s.append(4 * float(np.mean(st)))
+    with mp.get_context("spawn").Pool(1) as pool:  # one process alone: the per-core rate
+        single, _ = cpu_rate(1, n, 1, pool)
     value = float(np.median(rates))
-    stage_ms = 5 * (P_ORD + 1) ** 3 * N_EL ** 3 / value * 1e3
-    sample = (f"{procs} concurrent single-rank reference processes, each 1 RK4 step of an {n}^3 block "
-              f"(periodic, same p, same per-element work) of the 32^3 TGV; stage time = (wall with the step "
-              f"- wall of geometry setup alone) / 4")
+    dof32 = 5 * (P_ORD + 1) ** 3 * N_EL ** 3
+    sample = (f"{procs} concurrent single-rank reference processes ({physical} physical cores), each one RK4 "
+              f"step of a {n}^3 block (periodic, same p, same per-element work) of the {N_EL}^3 TGV per bench step; "
+              f"stage time = (wall with the step - wall of geometry set-up alone) / 4")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 4 * stage_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config({"sample_block": f"{n}^3"}),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(step_s)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "physical_cores": physical,
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ms_per_step_is": f"the measured RK4 step of one {n}^3 sample block per process (all processes at once)",
+        "samples_run": {"bench_steps": args.steps, "warmup_steps": args.warmup,
+                        "rk4_steps_per_process_per_bench_step": 1, "processes": procs},
+        "full_step_ms_extrapolated": 4 * dof32 / value * 1e3,
+        "single_process_rate": {"value": single, "unit": UNIT, "cores": 1,
+                                "sample": f"one process alone, one RK4 step of a {n}^3 block"},
     }))
 
 
@@ -432,15 +466,19 @@ def _channel_case(dg):
 
 
 def _channel_adjoint_block(dg, torch, nsteps, slots=50):
-    """The adjoint-at-scale configuration on config 5's channel: mixed-form
-    forward record (FP32 contractions and fluxes) of `nsteps` TVD-RK3 steps
-    with `slots` checkpoint buffers, then the FP64 adjoint sweep giving
-    dJ/dT_w for J = the mean wall shear stress of the y = 0 wall at the end
-    (functionals.wall_shear, with the box metric of the unmapped mesh; the
-    sinusoidal map leaves the walls flat).  dJ/dT_w is checked against central
-    differences of two FP64 forward runs with T_w moved by 1e-4 T_w.  The
-    isothermal wall, the heat flux and this gradient have no reference
-    counterpart."""
+    """The adjoint-at-scale configuration on config 5's channel: `nsteps`
+    TVD-RK3 steps recorded with `slots` checkpoint buffers, then the FP64
+    adjoint sweep giving dJ/dT_w for J = the mean wall shear stress of the
+    y = 0 wall at the end (functionals.wall_shear, with the box metric of the
+    unmapped mesh; the sinusoidal map leaves the walls flat).  Two gradients:
+    the configuration's (mixed-form forward record: FP32 contractions and
+    fluxes, FP64 adjoint) and the all-FP64 one.  The reference value is
+    central differences of FP64 forward runs at two steps, h = 1e-4 T_w and
+    h/2, Richardson-extrapolated, so the differencing error is not charged to
+    either gradient: the FP64 gradient's error against it is the adjoint's,
+    and the mixed gradient's distance from the FP64 gradient is the cost of
+    the mixed forward.  The isothermal wall, the heat flux and this gradient
+    have no reference counterpart."""
     from dgpr_b200 import functionals as F
     mesh, prm, U0, dt = _channel_case(dg)
     lx, ly, lz = 4 * math.pi, 2.0, 2 * math.pi
@@ -452,47 +490,136 @@ def _channel_adjoint_block(dg, torch, nsteps, slots=50):
 
     out = {"workload": f"channel {mesh.nx}x{mesh.ny}x{mesh.nz} p = {mesh.p} q = {mesh.q}, isothermal walls at "
                        f"T_w = {Tw:.4g}, Pr 0.71, {nsteps} TVD-RK3 steps dt={dt:.3e}; J = mean wall shear of "
-                       f"the y = 0 wall; mixed forward, FP64 adjoint, {slots} checkpoint slots"}
-    with dg.Solver(mesh, dg.Params.from_array(prm), dg.MIXED_FP32) as s:
-        s.set_prandtl(0.71)
-        s.set_state(U0)
-        s.step(dg.TVDRK3, dt, 3, norms=False)  # warm-up
-        s.set_state(U0)
-        s.forward_record(dg.TVDRK3, dt, 2, 2, norms=False)
-        s.backward(np.zeros(U0.size))  # warm-up of the sweep
-        s.set_state(U0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s.step(dg.TVDRK3, dt, nsteps, norms=False)
-        torch.cuda.synchronize()
-        plain = time.perf_counter() - t0
-        s.set_state(U0)
-        t0 = time.perf_counter()
-        s.forward_record(dg.TVDRK3, dt, nsteps, slots, norms=False)
-        torch.cuda.synchronize()
-        rec = time.perf_counter() - t0
-        UN = torch.tensor(s.get_state(), device="cuda", requires_grad=True)
-        J = J_of(UN)
-        J.backward()
-        lamN = UN.grad.cpu().numpy()
-        t0 = time.perf_counter()
-        _, dp = s.backward_params(lamN)
-        back = time.perf_counter() - t0
-        fwd, rev, _ = s.adjoint_stats()
+                       f"the y = 0 wall; FP64 adjoint, {slots} checkpoint slots; forward record mixed (the "
+                       f"configuration) and FP64"}
+    grads = {}
+    for prec, name in ((dg.MIXED_FP32, "mixed_forward"), (dg.FP64, "fp64_forward")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_prandtl(0.71)
+            s.set_state(U0)
+            s.step(dg.TVDRK3, dt, 3, norms=False)  # warm-up
+            s.set_state(U0)
+            s.forward_record(dg.TVDRK3, dt, 2, 2, norms=False)
+            s.backward(np.zeros(U0.size))  # warm-up of the sweep
+            s.set_state(U0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.step(dg.TVDRK3, dt, nsteps, norms=False)
+            torch.cuda.synchronize()
+            plain = time.perf_counter() - t0
+            s.set_state(U0)
+            t0 = time.perf_counter()
+            s.forward_record(dg.TVDRK3, dt, nsteps, slots, norms=False)
+            torch.cuda.synchronize()
+            rec = time.perf_counter() - t0
+            UN = torch.tensor(s.get_state(), device="cuda", requires_grad=True)
+            J = J_of(UN)
+            J.backward()
+            lamN = UN.grad.cpu().numpy()
+            t0 = time.perf_counter()
+            _, dp = s.backward_params(lamN)
+            back = time.perf_counter() - t0
+            fwd, rev, _ = s.adjoint_stats()
+        grads[name] = float(dp[dg.DPARAM_TWALL])
+        out[name] = {"J": float(J.detach()), "dJ_dTw": grads[name], "plain_forward_s": plain,
+                     "recorded_forward_s": rec, "backward_s": back, "backward_over_plain_forward": back / plain,
+                     "recomputed_steps": fwd, "reversed_steps": rev}
+    fd = {}
     with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
         s.set_prandtl(0.71)
-        h = 1e-4 * Tw
-        Js = []
-        for t in (Tw + h, Tw - h):
-            s.set_wall_temperature(t)
+        for k, h in (("h", 1e-4 * Tw), ("h/2", 0.5e-4 * Tw)):
+            Js = []
+            for t in (Tw + h, Tw - h):
+                s.set_wall_temperature(t)
+                s.set_state(U0)
+                s.step(dg.TVDRK3, dt, nsteps, norms=False)
+                Js.append(float(J_of(_device_state(s, torch))))
+            fd[k] = (Js[0] - Js[1]) / (2 * h)
+    rich = (4 * fd["h/2"] - fd["h"]) / 3
+    out["fd_fp64"] = {"h": 1e-4 * Tw, "central_h": fd["h"], "central_h2": fd["h/2"], "richardson": rich,
+                      "h_vs_h2_rel": abs(fd["h"] - fd["h/2"]) / abs(rich)}
+    out["rel_err_fp64_adjoint_vs_fd"] = abs(grads["fp64_forward"] - rich) / abs(rich)
+    out["rel_err_mixed_forward_vs_fd"] = abs(grads["mixed_forward"] - rich) / abs(rich)
+    out["rel_gap_mixed_vs_fp64_adjoint"] = abs(grads["mixed_forward"] - grads["fp64_forward"]) / abs(
+        grads["fp64_forward"])
+    return out
+
+
+def _hbm_peak():
+    """(peak GB/s, its source): the measured copy bandwidth when present."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6650 GB/s"
+
+
+def _device_state(s, torch):
+    """The handle's nodal state as a CUDA float64 tensor (device-to-device)."""
+    U = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    s.get_state_device(U.data_ptr())
+    torch.cuda.synchronize()
+    return U
+
+
+def _config3_block(dg, torch, steps, acc_steps, ke_every=100):
+    """The mixed-precision configuration's size: TGV Re 1600 Ma 0.1 on 48^3
+    hexes, p = 4 (125 DOF per element and variable), RK4, dt from CFL 0.2.
+    Device time per step of both forms, each form's stage-kernel roofline
+    fraction (algorithmic bytes 200 nb + 80 per element and launch), and, over
+    `acc_steps` steps, the relative L2 distance of the mixed state from the
+    FP64 form's, with both kinetic-energy histories (every `ke_every` steps)
+    and the dissipation rates -dKE/dt between them."""
+    from dgpr_b200 import functionals as F
+    n, p = 48, 4
+    nodes, prm, U0, dt = tgv_case(n, p)
+    mesh = dg.Mesh(n, n, n, p, 1, nodes, [dg.PERIODIC] * 6)
+    nb = (p + 1) ** 3
+    dof_stage = 5 * nb * n ** 3
+    alg = (200 * nb + 80) * n ** 3
+    peak, peak_src = _hbm_peak()
+    stream = torch.cuda.Stream()
+    out = {"workload": f"TGV Re 1600 Ma 0.1, periodic [0,2pi]^3, {n}^3 hexes, p = {p}, RK4 dt={dt:.4e}",
+           "dof_per_stage": dof_stage, "algorithmic_bytes_per_stage_launch": alg, "peak_gbs": peak,
+           "peak_source": peak_src}
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+        with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+            s.set_stream(stream.cuda_stream)
             s.set_state(U0)
-            s.step(dg.TVDRK3, dt, nsteps, norms=False)
-            Js.append(float(J_of(torch.tensor(s.get_state(), device="cuda"))))
-        fd = (Js[0] - Js[1]) / (2 * h)
-    an = float(dp[dg.DPARAM_TWALL])
-    out.update({"J": float(J), "dJ_dTw": an, "dJ_dTw_fd_fp64": fd, "rel_err": abs(an - fd) / abs(fd),
-                "plain_forward_s": plain, "recorded_forward_s": rec, "backward_s": back,
-                "backward_over_plain_forward": back / plain, "recomputed_steps": fwd, "reversed_steps": rev})
+            _warm(dg, torch, s, dt, 3)
+            ms = _timed_steps(dg, torch, s, stream, dt, steps) / steps
+            kms, tms = _stage_kernel_ms(dg, s, U0, dt, 5)
+        out[name] = {"ms_per_step": ms, "value": dof_stage * 4 / (ms * 1e-3), "unit": UNIT,
+                     "stage_kernel_ms": kms, "trace_kernel_ms": tms,
+                     "stage_roofline_frac": alg / (kms * 1e-3) / 1e9 / peak}
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if acc_steps > 0:
+        L = 2 * math.pi
+        quad = F.BoxQuadrature(n, n, n, p, L, L, L, device="cuda")
+        fin, ke = {}, {}
+        for prec in (dg.FP64, dg.MIXED_FP32):
+            with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
+                s.set_state(U0)
+                hist = [float(F.kinetic_energy(_device_state(s, torch), quad))]
+                done = 0
+                while done < acc_steps:
+                    k = min(ke_every, acc_steps - done)
+                    s.step(dg.RK4, dt, k, norms=False)
+                    done += k
+                    hist.append(float(F.kinetic_energy(_device_state(s, torch), quad)))
+                fin[prec] = _device_state(s, torch)
+                ke[prec] = np.array(hist)
+        err = float(torch.linalg.norm(fin[dg.MIXED_FP32] - fin[dg.FP64]) / torch.linalg.norm(fin[dg.FP64]))
+        t = dt * np.minimum(np.arange(len(ke[dg.FP64])) * ke_every, acc_steps)
+        eps = {k: -np.diff(v) / np.diff(t) for k, v in ke.items()}
+        out["accuracy"] = {
+            "steps": acc_steps, "rel_l2_mixed_vs_fp64": err, "bound": 1e-6, "within_bound": err <= 1e-6,
+            "ke_every_steps": ke_every, "t": t.tolist(), "ke_fp64": ke[dg.FP64].tolist(),
+            "ke_mixed": ke[dg.MIXED_FP32].tolist(),
+            "dissipation_fp64": eps[dg.FP64].tolist(), "dissipation_mixed": eps[dg.MIXED_FP32].tolist(),
+            "max_rel_ke_diff": float(np.max(np.abs(ke[dg.MIXED_FP32] - ke[dg.FP64]) / np.abs(ke[dg.FP64]))),
+            "max_rel_dissipation_diff": float(np.max(np.abs(eps[dg.MIXED_FP32] - eps[dg.FP64])) /
+                                              np.max(np.abs(eps[dg.FP64])))}
     return out
 
 
@@ -542,7 +669,7 @@ def run_reverse_steps(args):
         s.set_state(U0)
         fwd = _timed_steps(dg, torch, s, stream, dt, args.steps) / args.steps
         rev, launches = _reverse_step_ms(dg, torch, s, stream, U0, dt, args.steps)
-    print(json.dumps({"workload": config()["workload"].replace("32^3", f"{N_EL}^3"), "forward_step_ms": fwd,
+    print(json.dumps({"workload": config()["workload"], "forward_step_ms": fwd,
                       "reverse_step_ms": rev, "reverse_over_forward": rev / fwd, "launches": launches}))
 
 
@@ -571,7 +698,7 @@ def run_ours(args, rank, world, local_rank):
     s.set_state(U0)
     clk = Clocks(local_rank)
     clk.start()
-    args.warmup = _warm(dg, torch, s, dt, args.warmup)
+    warm_run = _warm(dg, torch, s, dt, args.warmup)
     barrier()
     torch.cuda.synchronize()
     ms = max_over_ranks(_timed_steps(dg, torch, s, stream, dt, args.steps))
@@ -643,6 +770,8 @@ def run_ours(args, rank, world, local_rank):
                "reverse_over_nodal_forward": rev_ms / nodal_ms, "reverse_step_launches": rev_launches,
                "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
+    config3 = (_config3_block(dg, torch, min(args.steps, 20), args.config3_accuracy_steps)
+               if rank == 0 and not args.no_config3 else None)
     curved = _curved_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_curved else None
     heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
     channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
@@ -651,13 +780,9 @@ def run_ours(args, rank, world, local_rank):
              if rank == 0 and not args.no_channel and args.channel_adjoint_steps > 0 else None)
 
     alg_bytes = (200 * nb + 80) * N_EL ** 3  # fused RK4 stage minimum, per element 200 nb + 80 B
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peak, peak_src = _hbm_peak()
     achieved = alg_bytes / (stage_ms * 1e-3) / 1e9
+    achieved_mixed = alg_bytes / (stage_ms_mixed * 1e-3) / 1e9
     barrier()
 
     if rank == 0:
@@ -665,34 +790,46 @@ def run_ours(args, rank, world, local_rank):
         if not args.no_cpu_baseline and world == 1:
             import oracle
             if oracle.reference() is not None:
-                procs = os.cpu_count() or 1
+                procs, physical = host_cores()
                 rate, _ = cpu_rate(1, REF_BLOCK, procs)
-                cpu = {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
+                cpu = {"value": rate, "unit": UNIT, "cores": procs, "physical_cores": physical, "kind": "reference",
                        "sample": f"{procs} concurrent reference processes, each 1 RK4 step on a {REF_BLOCK}^3 "
                                  f"block of the TGV mesh (same per-element work)"}
-        traffic = None
+        prof = {}
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get("stage_kernel_bytes_per_launch")
+            prof = json.load(open(tpath))
+        traffic = prof.get("stage_kernel_bytes_per_launch")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "vstage_kernel<4,double>", "kernel_ms": stage_ms,
+                "trace_kernel_ms": trace_ms, "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_src}
+        fp64_flop = prof.get("stage_kernel_fp64_flop_per_launch")
+        if fp64_flop:  # executed FP64 arithmetic (ncu instruction counts, scaled to the launch)
+            rate = fp64_flop / (stage_ms * 1e-3) / 1e12
+            roof["fp64_executed_tflops"] = rate
+            roof["fp64_peak_tflops"] = FP64_PEAK_TFLOPS
+            roof["fp64_frac"] = rate / FP64_PEAK_TFLOPS
+            roof["fp64_peak_source"] = FP64_PEAK_SOURCE
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU"}),
+            "config": config(),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "warmup_steps_run": warm_run,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": U0.size * 8,
                     "d2h_bytes_per_step": U0.size * 8 + 8},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "vstage_kernel<4,double>", "kernel_ms": stage_ms, "trace_kernel_ms": trace_ms,
-                         "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"
-                         if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+            "roofline": roof,
             "mixed": {"value": value_mixed, "unit": UNIT, "ms_per_step": ms_mixed / args.steps,
                       "speedup_vs_fp64": value_mixed / value, "stage_kernel_ms": stage_ms_mixed,
                       "trace_kernel_ms": trace_ms_mixed,
+                      "roofline": {"bound": "hbm", "achieved": achieved_mixed, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved_mixed / peak, "algorithmic_bytes_per_launch": alg_bytes},
                       "dtype": "f32 contractions/fluxes, f64 geometry/inverse mass/RK state",
                       "accuracy": acc},
             "adjoint": adj,
+            "config3": config3,
             "curved": curved,
             "heat": heat,
             "channel": channel,
@@ -702,6 +839,21 @@ def run_ours(args, rank, world, local_rank):
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        # the headline figures again, short, at the end of the line
+        head = {"fp64_value": value, "fp64_stage_frac": achieved / peak,
+                "mixed_speedup_32_p3": value_mixed / value,
+                "mixed_rel_l2_1000_32_p3": acc["rel_l2_mixed_vs_fp64"] if acc else None}
+        if config3:
+            head["mixed_speedup_48_p4"] = config3["speedup_mixed_vs_fp64"]
+            head["mixed_rel_l2_48_p4"] = config3.get("accuracy", {}).get("rel_l2_mixed_vs_fp64")
+        if adj:
+            head["adjoint_reverse_over_forward"] = adj["reverse_over_forward"]
+            head["adjoint_config_backward_over_forward"] = {
+                str(b["slots"]): round(b["backward_over_plain_forward"], 3) for b in adj["config"]["budgets"]}
+        if chadj:
+            head["channel_grad_rel_err_fp64"] = chadj["rel_err_fp64_adjoint_vs_fd"]
+            head["channel_grad_rel_err_mixed"] = chadj["rel_err_mixed_forward_vs_fd"]
+        out["headline"] = head
         print(json.dumps(out))
 
 
@@ -725,6 +877,9 @@ def main():
                     help="RK4 steps of the adjoint configuration (0 skips the adjoint block)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (0 skips it)")
+    ap.add_argument("--no-config3", action="store_true", help="skip the 48^3 p = 4 block")
+    ap.add_argument("--config3-accuracy-steps", type=int, default=1000,
+                    help="steps of the 48^3 p = 4 mixed-vs-FP64 accuracy and kinetic-energy check (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     globals()["N_EL"] = args.nel

@@ -5,6 +5,7 @@
 
 #include "../../include/dgb200.h"
 #include "../../include/dgb200_check.h"
+#include "host.hpp"
 #include "physics_vjp.cuh"
 
 using namespace dgb;
@@ -99,6 +100,9 @@ extern "C" int dgb_check_pointwise(int which, const double* x, const double* yba
       }
       return DGB_OK;
     }
+    case DGB_CHECK_FACE_MATCH:  // x = {n_own[3], n_nbr[3], fJ_own, fJ_nbr}
+      y[0] = face_mismatch(x, x + 3, 1, x[6], x[7]) ? 1. : 0.;
+      return DGB_OK;
   }
   return DGB_ERR_ARG;
 }

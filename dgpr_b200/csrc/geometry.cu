@@ -236,19 +236,18 @@ __global__ void geo_match_kernel(const int32_t* __restrict__ nbr, long E, int NQ
   if (en < 0) return;
   const long e = ef / 6;
   const int lf = (int)(ef - 6 * e), lo = lf ^ 1;
-  double dn = 0., df;
+  bool bad;
   if (gf) {
     const double* g = gf + (size_t)ef * kFaceC * NQF;
     const double* h = gf + ((size_t)en * 6 + lo) * kFaceC * NQF;
-    for (int r = 0; r < 3; ++r) dn = fmax(dn, fabs(g[(kFaceN + r) * NQF + fq] + h[(kFaceN + r) * NQF + fq]));
-    df = fabs(g[kFaceFJ * NQF + fq] - h[kFaceFJ * NQF + fq]) / g[kFaceFJ * NQF + fq];
+    bad = face_mismatch(g + kFaceN * NQF + fq, h + kFaceN * NQF + fq, NQF, g[kFaceFJ * NQF + fq],
+                        h[kFaceFJ * NQF + fq]);
   } else {
     const double* g = geo + (size_t)e * kGeoStride;
     const double* h = geo + (size_t)en * kGeoStride;
-    for (int r = 0; r < 3; ++r) dn = fmax(dn, fabs(g[kGeoN + 3 * lf + r] + h[kGeoN + 3 * lo + r]));
-    df = fabs(g[kGeoFJ + lf] - h[kGeoFJ + lo]) / g[kGeoFJ + lf];
+    bad = face_mismatch(g + kGeoN + 3 * lf, h + kGeoN + 3 * lo, 1, g[kGeoFJ + lf], h[kGeoFJ + lo]);
   }
-  if (dn > 1e-10 || df > 1e-10) atomicMin(&st->face, (int)ef);
+  if (bad) atomicMin(&st->face, (int)ef);
 }
 
 unsigned blocks(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }

@@ -478,11 +478,8 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
         const double* g = &gf[((size_t)e * 6 + lf) * kFaceC * NQF];
         const double* h = &gf[((size_t)en * 6 + (lf ^ 1)) * kFaceC * NQF];
         for (int fq = 0; fq < NQF; ++fq) {
-          double dn = 0.;
-          for (int r = 0; r < 3; ++r)
-            dn = std::fmax(dn, std::fabs(g[(kFaceN + r) * NQF + fq] + h[(kFaceN + r) * NQF + fq]));
-          const double df = std::fabs(g[kFaceFJ * NQF + fq] - h[kFaceFJ * NQF + fq]) / g[kFaceFJ * NQF + fq];
-          if (dn > 1e-10 || df > 1e-10) {
+          if (face_mismatch(g + kFaceN * NQF + fq, h + kFaceN * NQF + fq, NQF, g[kFaceFJ * NQF + fq],
+                            h[kFaceFJ * NQF + fq])) {
             char buf[160];
             snprintf(buf, sizeof buf, "face %d of element %ld does not match its neighbour %d", lf, e, en);
             why = buf;
@@ -494,10 +491,7 @@ int build_geometry(const dgb_mesh_desc& m, const Ops1D& ops, std::vector<double>
       const double* g = &geo[(size_t)e * kGeoStride];
       const double* h = &geo[(size_t)en * kGeoStride];
       const int lo = lf ^ 1;
-      double dn = 0.;
-      for (int r = 0; r < 3; ++r) dn = std::fmax(dn, std::fabs(g[kGeoN + 3 * lf + r] + h[kGeoN + 3 * lo + r]));
-      const double df = std::fabs(g[kGeoFJ + lf] - h[kGeoFJ + lo]) / g[kGeoFJ + lf];
-      if (dn > 1e-10 || df > 1e-10) {
+      if (face_mismatch(g + kGeoN + 3 * lf, h + kGeoN + 3 * lo, 1, g[kGeoFJ + lf], h[kGeoFJ + lo])) {
         char buf[160];
         snprintf(buf, sizeof buf, "face %d of element %ld does not match its neighbour %d", lf, e, en);
         why = buf;

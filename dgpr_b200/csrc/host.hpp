@@ -2,6 +2,7 @@
 // the tensor-product basis, per-element affine geometry, neighbour table.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -51,6 +52,18 @@ struct Ops1D {
 //   sum_a EL[end][a]^2 / (w_a detJ(a, t1, t2))   (= cend / detJ when affine).
 constexpr int kVolC = 10, kVolDetJ = 9;
 constexpr int kFaceC = 14, kFaceN = 9, kFaceFJ = 12, kFaceLift = 13;
+
+// True unless the two sides of an interior face agree: opposite unit normals
+// (ng = -nh) and equal surface Jacobians, to 1e-10.  Written as the negation
+// of "both within tolerance" so that a NaN normal or surface Jacobian (a
+// degenerate face) counts as a mismatch.  sn: stride between the normal's
+// components.
+__host__ __device__ inline bool face_mismatch(const double* ng, const double* nh, int sn, double fJg, double fJh)
+{
+  bool ok = true;
+  for (int r = 0; r < 3; ++r) ok = ok && (fabs(ng[r * sn] + nh[r * sn]) <= 1e-10);
+  return !(ok && fabs(fJg - fJh) / fJg <= 1e-10);
+}
 
 int build_ops(int p, Ops1D& ops);
 

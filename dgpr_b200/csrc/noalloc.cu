@@ -17,11 +17,12 @@
 //    (different streams, or different host threads) race and give wrong
 //    results: callers must order them (same stream, or synchronise between);
 //  * the array keeps the previous call's contents; everything the kernels read
-//    is rewritten at the start of each call, and the status word is cleared.
+//    is rewritten at the start of each call, and the status word is cleared;
+//  * a call cannot be captured into a CUDA graph: it copies from pageable host
+//    memory and synchronises the stream before it returns.
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -38,10 +39,6 @@ constexpr size_t kNoallocScratchBytes = 32u << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
-
 size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 
 }  // namespace
@@ -54,6 +51,16 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
   Ops1D ops;
   int rc = build_ops(mesh->p, ops);
   if (rc) return set_last_error(rc, "solution order outside 0..6");
+  if (mesh->nx <= 0 || mesh->ny <= 0 || mesh->nz <= 0) return set_last_error(DGB_ERR_ARG, "empty mesh");
+  {  // the affine layout is a lower bound on the scratch any mesh of this size
+     // needs: reject far-too-large meshes before building their geometry
+    const double E = (double)mesh->nx * mesh->ny * mesh->nz, NQF = (double)ops.P * ops.P;
+    const double lower = E * (60. * NQF * sizeof(double) + kGeoStride * sizeof(double) + 6. * sizeof(int32_t));
+    if (lower > (double)kNoallocScratchBytes)
+      return set_last_error(DGB_ERR_ARG, "mesh needs at least " + std::to_string((long long)lower) +
+                                             " bytes of scratch; the static array holds " +
+                                             std::to_string(kNoallocScratchBytes) + " bytes (32 MiB)");
+  }
   std::vector<double> geo, gv, gf;
   std::vector<int32_t> nbr;
   std::string why;
@@ -79,29 +86,33 @@ extern "C" int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params*
                                            " bytes of scratch; the static array holds " +
                                            std::to_string(kNoallocScratchBytes) + " bytes (32 MiB)");
 
-  // set-up once per device, with that device current: the array's device
-  // address (the host-side symbol is not a device pointer)
+  // the array's device address on the current device, looked up on every
+  // call (a lookup, no allocation): the host-side symbol is not a device
+  // pointer, and an address kept from an earlier call would be stale after
+  // the context was torn down and made again
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_last_error(DGB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return set_last_error(DGB_ERR_UNSUPPORTED, "device index above 63");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int sdev = dev;
+  e = cudaStreamGetDevice(st, &sdev);
+  if (e != cudaSuccess)
+    return set_last_error(DGB_ERR_CUDA, std::string("cudaStreamGetDevice: ") + cudaGetErrorString(e));
+  if (sdev != dev)
+    return set_last_error(DGB_ERR_ARG, "stream belongs to device " + std::to_string(sdev) +
+                                           ", but the current device is " + std::to_string(dev));
   unsigned char* base = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-      void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return set_last_error(DGB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_scratch_addr[dev] = p;
-    }
-    base = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_last_error(DGB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    base = static_cast<unsigned char*>(p);
   }
   // shared-memory attributes of the kernel instances for this order (no allocation)
   e = prepare_kernels(P, DGB_FP64);
   if (e != cudaSuccess) return set_last_error(DGB_ERR_CUDA, std::string("kernel set-up: ") + cudaGetErrorString(e));
 
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   int* flag = reinterpret_cast<int*>(base + oFlag);
 #define NA_CK(call)                                                                                \
   do {                                                                                             \

@@ -244,11 +244,13 @@ int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_
  * that loads the library holds until the process exits.  Meshes needing more
  * scratch than that (about 4,000 affine or 1,500 curved elements at p = 3) are rejected with
  * DGB_ERR_ARG and a message giving the size needed.
- * The first call on each device looks up the array's device address (set-up);
- * make that first call before any stream capture.  All calls share the array
- * and it keeps the last call's contents: calls whose GPU work could overlap
- * (different streams or host threads) race -- order them.  Synchronises
- * `stream` (cudaStream_t as void*, NULL = legacy default) before returning.
+ * Each call looks up the array's device address on the current device (no
+ * allocation); `stream` (cudaStream_t as void*, NULL = legacy default) must
+ * belong to the current device.  All calls share the array and it keeps the
+ * last call's contents: calls whose GPU work could overlap (different
+ * streams or host threads) race -- order them.  The call copies from
+ * pageable host memory and synchronises `stream` before returning, so it
+ * cannot be made while `stream` is being captured.
  * This entry point has no counterpart in the reference. */
 int dgb_residual_noalloc(const dgb_mesh_desc* mesh, const dgb_params* params, const double* U_dev,
                          double* f_dev, void* stream);

@@ -23,7 +23,12 @@ enum {
    * in the energy row (an extension: the reference conducts no heat). */
   DGB_CHECK_VISC_FLUX_HEAT = 7,    /* x as 2; aux = {mu, kq} */
   DGB_CHECK_VISC_RANK1_HEAT = 8,   /* x as 3; aux = {mu, n[3], kq} */
-  DGB_CHECK_VISC_JUMP_N_HEAT = 9   /* x as 4; aux = {mu, n[3], kq} */
+  DGB_CHECK_VISC_JUMP_N_HEAT = 9,  /* x as 4; aux = {mu, n[3], kq} */
+  /* The face-match test of the geometry builders (host and device): the two
+   * sides of an interior face must have opposite unit normals and equal
+   * surface Jacobians.  x = {n_own[3], n_nbr[3], fJ_own, fJ_nbr}; aux unused;
+   * y[0] = 1 on a mismatch (NaN counts as one), else 0.  No reverse mode. */
+  DGB_CHECK_FACE_MATCH = 10
 };
 
 /* Evaluates function `which` at x into y; when ybar and xbar are non-NULL

@@ -175,3 +175,31 @@ def test_device_geometry_errors_match_the_host_builder():
             dg.Solver(m, C.params())
         assert dev.value.code == host.value.code == dg.ERR_GEOMETRY
         assert str(dev.value) == str(host.value)
+
+
+def test_face_match_predicate_flags_degenerate_faces():
+    """The face-match test both builders run (host.cpp, geometry.cu) through
+    the check hook: matching sides pass; a normal or surface Jacobian that is
+    off by more than 1e-10, a NaN normal, and a zero or NaN surface
+    Jacobian (a collapsed face, 0/0) are mismatches."""
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+    f = dg.lib().dgb_check_pointwise
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, dp, dp, dp, dp, dp]
+
+    def mismatch(ng, nh, fg, fh):
+        x = np.array([*ng, *nh, fg, fh], dtype=np.float64)
+        aux, y = np.zeros(1), np.zeros(1)
+        assert f(10, x.ctypes.data_as(dp), None, aux.ctypes.data_as(dp), y.ctypes.data_as(dp), None) == 0
+        return bool(y[0])
+
+    n = np.array([0.6, 0.8, 0.0])
+    assert not mismatch(n, -n, 2.0, 2.0)
+    assert not mismatch(n, -n + 1e-12, 2.0, 2.0 * (1 + 1e-12))
+    assert mismatch(n, -n + 1e-8, 2.0, 2.0)
+    assert mismatch(n, -n, 2.0, 2.0 * (1 + 1e-8))
+    assert mismatch(np.array([np.nan, 0.8, 0.0]), -n, 2.0, 2.0)
+    assert mismatch(n, np.array([-0.6, np.nan, 0.0]), 2.0, 2.0)
+    assert mismatch(n, -n, 0.0, 0.0)
+    assert mismatch(n, -n, np.nan, 2.0)

@@ -7,8 +7,8 @@ Checked through the C ABI against the ordinary entry point (dgb_residual),
 within the parity tolerance of the FP64 tests (1e-11 relative L2; in practice
 the two run the same kernels and agree exactly), on two calls in a row with
 different meshes, so stale contents of the shared array would show.  This
-file is collected last; it also passes alone in a fresh process, where its
-first call performs the per-device set-up."""
+file is collected last; it also passes alone in a fresh process.  Each call
+looks up the static array's device address itself (no cached set-up)."""
 import ctypes
 
 import numpy as np
