@@ -545,6 +545,82 @@ def _channel_adjoint_block(dg, torch, nsteps, slots=50):
     return out
 
 
+def _checkpoint_block(dg, steps=200, chkint=20):
+    """Checkpoint cadence of the dgb driver (C++ host code over the C ABI,
+    the drop-in for the reference's cudg): wall time of `steps` RK4 steps of
+    the TGV workload read from a .dg file, writing a .dg checkpoint every
+    `chkint` steps, against the same run with no checkpoint.  The driver
+    writes each checkpoint from a snapshot on a host thread while the steps
+    go on.  Process start, set-up and the final file are in both times."""
+    import tempfile
+    exe = os.path.join(ROOT, "dgpr_b200", "_lib", "dgb")
+    if not os.path.exists(exe):
+        return {"unavailable": "dgpr_b200/_lib/dgb was not built"}
+    nodes, prm, U0, dt = tgv_case(N_EL, P_ORD)
+    mesh = dg.Mesh(N_EL, N_EL, N_EL, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
+    out = {"workload": f"dgb -ifile (TGV {N_EL}^3 p={P_ORD}) -scheme RK4 -niter {steps}, FP64",
+           "checkpoint_bytes": int(U0.size * 8)}
+    with tempfile.TemporaryDirectory() as d:
+        dg.write_state(os.path.join(d, "tgv.dg"), 0, mesh, {"state": U0})
+        args = [exe, "-ifile", os.path.join(d, "tgv"), "-niter", str(steps), "-scheme", "RK4", "-dt", repr(dt),
+                "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0",
+                "-ofile", os.path.join(d, "out")]
+        for name, ci in (("no_checkpoints_s", 10 * steps), ("checkpoint_every_%d_s" % chkint, chkint),
+                         ("no_checkpoints_again_s", 10 * steps)):
+            t0 = time.perf_counter()
+            subprocess.run(args + ["-chkint", str(ci)], stdout=subprocess.DEVNULL, check=True, timeout=600)
+            out[name] = time.perf_counter() - t0
+    base = min(out["no_checkpoints_s"], out["no_checkpoints_again_s"])
+    out["overhead_frac"] = out["checkpoint_every_%d_s" % chkint] / base - 1.0
+    out["checkpoints_written"] = steps // chkint
+    return out
+
+
+def _reference_cuda_block(dg, n, k1=20, k2=120):
+    """The reference's own GPU path (solver/cudg.cu built unmodified for
+    sm_100a into oracle/_ref/cudg: FP32, thread-per-quadrature-point kernels
+    with a device synchronisation after each) on the TGV at n^3, p = 3, RK4,
+    read from a .dg file.  Information only, not a parity target: it
+    approximates BR2 by a local penalty and uses dt/2 in stage 3 of RK4.
+    Its rate comes from wall times, (k2 - k1) steps / (t(k2) - t(k1)), the
+    two runs started at the same time so that their host set-up (the
+    reference's CPU geometry precompute) overlaps; its final state is compared
+    with this library's FP64 state after k2 steps."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "cudg")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/cudg was not built (the reference tree is needed to compile it)"}
+    nodes, prm, U0, dt = tgv_case(n, P_ORD)
+    mesh = dg.Mesh(n, n, n, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
+    dof_step = 4 * 5 * (P_ORD + 1) ** 3 * n ** 3
+    out = {"workload": f"reference cudg (FP32) -ifile TGV {n}^3 p={P_ORD} -scheme RK4", "steps": [k1, k2]}
+    with tempfile.TemporaryDirectory() as d:
+        dg.write_state(os.path.join(d, "tgv.dg"), 0, mesh, {"state": U0})
+        procs, t0 = [], time.perf_counter()
+        for k in (k1, k2):
+            args = [exe, "-ifile", os.path.join(d, "tgv"), "-niter", str(k), "-chkint", str(10 * k2), "-scheme",
+                    "RK4", "-dt", repr(dt), "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0",
+                    "-ofile", os.path.join(d, f"out{k}")]
+            procs.append(subprocess.Popen(args, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE))
+        walls = []
+        for p in procs:
+            _, err = p.communicate(timeout=900)
+            walls.append(time.perf_counter() - t0)
+            if p.returncode != 0:
+                return {"unavailable": f"cudg exited {p.returncode}: {err.decode()[-300:]}"}
+        _, _, Uref = dg.read_state(os.path.join(d, f"out{k2}.dg"))
+    with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
+        s.set_state(U0)
+        s.step(dg.RK4, dt, k2, norms=False)
+        Uours = s.get_state()
+    rate = dof_step * (k2 - k1) / max(walls[1] - walls[0], 1e-9)
+    out.update({"wall_s": walls, "ms_per_step": 1e3 * (walls[1] - walls[0]) / (k2 - k1),
+                "value": rate, "unit": UNIT,
+                "rel_l2_vs_fp64_after_k2": float(np.linalg.norm(Uref - Uours) / np.linalg.norm(Uours)),
+                "finite": bool(np.all(np.isfinite(Uref)))})
+    return out
+
+
 def _hbm_peak():
     """(peak GB/s, its source): the measured copy bandwidth when present."""
     try:
@@ -776,6 +852,7 @@ def run_ours(args, rank, world, local_rank):
     heat = _heat_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_heat else None
     channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
     geometry = _geometry_block(dg, torch) if rank == 0 and not args.no_geometry else None
+    ckpt = _checkpoint_block(dg) if rank == 0 and not args.no_checkpoint else None
     chadj = (_channel_adjoint_block(dg, torch, args.channel_adjoint_steps)
              if rank == 0 and not args.no_channel and args.channel_adjoint_steps > 0 else None)
 
@@ -835,6 +912,7 @@ def run_ours(args, rank, world, local_rank):
             "channel": channel,
             "geometry": geometry,
             "channel_adjoint": chadj,
+            "checkpoint_cadence": ckpt,
             "clocks": clocks,
         }
         if cpu:
@@ -878,6 +956,7 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 accuracy check (0 skips it)")
     ap.add_argument("--no-config3", action="store_true", help="skip the 48^3 p = 4 block")
+    ap.add_argument("--no-checkpoint", action="store_true", help="skip the driver's checkpoint-cadence timing")
     ap.add_argument("--config3-accuracy-steps", type=int, default=1000,
                     help="steps of the 48^3 p = 4 mixed-vs-FP64 accuracy and kinetic-energy check (0 skips it)")
     args = ap.parse_args()

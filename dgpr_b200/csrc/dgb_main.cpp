@@ -13,12 +13,15 @@
 // running mean (-mean_start) follows the reference's CPU driver dg.cpp, which
 // has it (cudg.cu does not).  -prandtl adds the optional heat flux (an
 // extension; 0, the default, is the reference's physics).
+#include <cuda_runtime.h>
+
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dgb200.h"
@@ -303,6 +306,47 @@ int main(int argc, char** argv)
   if (in.twall > 0. && (rc = dgb_set_wall_temperature(h, in.twall))) die("dgb_set_wall_temperature", rc);
   if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
 
+  // checkpoints are written while the steps go on: the state is copied to
+  // a device snapshot (a device-to-device copy on the handle's stream), the
+  // snapshot goes to pinned host memory on a copy stream, and a host thread
+  // writes the .dg file once that copy is done.  The next checkpoint waits
+  // for the previous file before it reuses the buffers.
+  struct Writer {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t done = nullptr;
+    double* d_snap = nullptr;
+    double* h_state = nullptr;
+    std::thread th;
+    int rc = DGB_OK;
+    std::string file;
+    void wait()
+    {
+      if (th.joinable()) th.join();
+      if (rc) die(file.c_str(), rc);
+    }
+    ~Writer()
+    {
+      if (th.joinable()) th.join();
+      if (d_snap) cudaFree(d_snap);
+      if (h_state) cudaFreeHost(h_state);
+      if (done) cudaEventDestroy(done);
+      if (copy) cudaStreamDestroy(copy);
+    }
+  } writer;
+  auto cuda_ok = [](cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+      fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
+      exit(1);
+    }
+  };
+  if (in.chkint && in.chkint <= in.niter) {
+    const size_t bytes = sizeof(double) * U.size();
+    cuda_ok(cudaStreamCreateWithFlags(&writer.copy, cudaStreamNonBlocking), "checkpoint stream");
+    cuda_ok(cudaEventCreateWithFlags(&writer.done, cudaEventDisableTiming), "checkpoint event");
+    cuda_ok(cudaMalloc(&writer.d_snap, bytes), "checkpoint snapshot");
+    cuda_ok(cudaMallocHost(&writer.h_state, bytes), "checkpoint host buffer");
+  }
+
   // running mean (dg.cpp:123-131): an input file may carry one to continue
   std::vector<double> M(U.size());
   bool have_mean = false;
@@ -335,10 +379,29 @@ int main(int argc, char** argv)
     if (in.chkint && (tstep + 1) % in.chkint == 0) {
       char f[1100];
       snprintf(f, sizeof f, "%s%" PRIu64 ".dg", in.ofile.c_str(), (uint64_t)tstep);
-      write(f, tstep);
+      writer.wait();  // the previous checkpoint's file is written: its buffers are free
+      if ((rc = dgb_get_state_device(h, writer.d_snap))) die("dgb_get_state_device", rc);
       // continue from the state as written, as a restart from this file
       // would (dgb_step otherwise continues from its Gauss-point copy)
-      if ((rc = dgb_set_state(h, U.data()))) die("dgb_set_state", rc);
+      if ((rc = dgb_set_state_device(h, writer.d_snap))) die("dgb_set_state_device", rc);
+      const bool with_mean = have_mean;
+      if (with_mean && (rc = dgb_get_mean(h, M.data()))) die("dgb_get_mean", rc);
+      cuda_ok(cudaMemcpyAsync(writer.h_state, writer.d_snap, sizeof(double) * U.size(), cudaMemcpyDeviceToHost,
+                              writer.copy),
+              "checkpoint copy");
+      cuda_ok(cudaEventRecord(writer.done, writer.copy), "checkpoint event");
+      writer.file = f;
+      writer.rc = DGB_OK;
+      writer.th = std::thread([&writer, &mesh, &M, with_mean, ts = tstep, file = std::string(f)]() {
+        if (cudaEventSynchronize(writer.done) != cudaSuccess) {
+          writer.rc = DGB_ERR_CUDA;
+          return;
+        }
+        const char* k[2] = {"state", "mean"};
+        const double* d[2] = {writer.h_state, M.data()};
+        writer.rc = dgb_write_state(file.c_str(), ts, &mesh, with_mean ? 2 : 1, k, d);
+      });
+      if (with_mean) writer.wait();  // the mean's host copy is reused by the next update
     }
     unsigned long long n = tfinal - tstep;
     if (in.chkint) {  // up to, not including, the next checkpointing step
@@ -365,6 +428,7 @@ int main(int argc, char** argv)
       have_mean = true;
     }
   }
+  writer.wait();
   write(in.ofile + ".dg", tstep - 1);  // the index of the last step taken, as cudg.cu:140-141 writes
   dgb_destroy(h);
   return 0;
