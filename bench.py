@@ -949,6 +949,7 @@ def main():
     ap.add_argument("--channel-adjoint-steps", type=int, default=500,
                     help="TVD-RK3 steps of the channel adjoint block (0 or --no-channel skips it)")
     ap.add_argument("--nel", type=int, default=N_EL, help="elements per direction (profiling runs use fewer)")
+    ap.add_argument("--p", type=int, default=P_ORD, help="solution order of the workload (profiling runs)")
     ap.add_argument("--reverse-steps-only", action="store_true",
                     help="only time reverse RK4 steps at the --nel workload (profiling the adjoint kernels)")
     ap.add_argument("--adjoint-steps", type=int, default=400,
@@ -962,6 +963,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     globals()["N_EL"] = args.nel
+    globals()["P_ORD"] = args.p
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
