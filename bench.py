@@ -545,13 +545,15 @@ def _channel_adjoint_block(dg, torch, nsteps, slots=50):
     return out
 
 
-def _checkpoint_block(dg, steps=200, chkint=20):
+def _checkpoint_block(dg, steps=600, chkints=(30, 150)):
     """Checkpoint cadence of the dgb driver (C++ host code over the C ABI,
     the drop-in for the reference's cudg): wall time of `steps` RK4 steps of
     the TGV workload read from a .dg file, writing a .dg checkpoint every
-    `chkint` steps, against the same run with no checkpoint.  The driver
-    writes each checkpoint from a snapshot on a host thread while the steps
-    go on.  Process start, set-up and the final file are in both times."""
+    `chkint` steps, against the same run with none.  The driver writes each
+    checkpoint from a device snapshot on a host thread while the steps go on,
+    so a checkpoint costs only what its file write exceeds the steps until
+    the next one.  Process start, set-up and the final file are in every
+    time."""
     import tempfile
     exe = os.path.join(ROOT, "dgpr_b200", "_lib", "dgb")
     if not os.path.exists(exe):
@@ -565,60 +567,149 @@ def _checkpoint_block(dg, steps=200, chkint=20):
         args = [exe, "-ifile", os.path.join(d, "tgv"), "-niter", str(steps), "-scheme", "RK4", "-dt", repr(dt),
                 "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0",
                 "-ofile", os.path.join(d, "out")]
-        for name, ci in (("no_checkpoints_s", 10 * steps), ("checkpoint_every_%d_s" % chkint, chkint),
-                         ("no_checkpoints_again_s", 10 * steps)):
+        runs = [("no_checkpoints_s", 10 * steps)] + [(f"checkpoint_every_{c}_s", c) for c in chkints] + \
+               [("no_checkpoints_again_s", 10 * steps)]
+        for name, ci in runs:
             t0 = time.perf_counter()
             subprocess.run(args + ["-chkint", str(ci)], stdout=subprocess.DEVNULL, check=True, timeout=600)
             out[name] = time.perf_counter() - t0
     base = min(out["no_checkpoints_s"], out["no_checkpoints_again_s"])
-    out["overhead_frac"] = out["checkpoint_every_%d_s" % chkint] / base - 1.0
-    out["checkpoints_written"] = steps // chkint
+    for c in chkints:
+        out[f"overhead_frac_every_{c}"] = out[f"checkpoint_every_{c}_s"] / base - 1.0
+        out[f"checkpoints_written_every_{c}"] = steps // c
     return out
 
 
-def _reference_cuda_block(dg, n, k1=20, k2=120):
-    """The reference's own GPU path (solver/cudg.cu built unmodified for
-    sm_100a into oracle/_ref/cudg: FP32, thread-per-quadrature-point kernels
-    with a device synchronisation after each) on the TGV at n^3, p = 3, RK4,
-    read from a .dg file.  Information only, not a parity target: it
-    approximates BR2 by a local penalty and uses dt/2 in stage 3 of RK4.
-    Its rate comes from wall times, (k2 - k1) steps / (t(k2) - t(k1)), the
-    two runs started at the same time so that their host set-up (the
-    reference's CPU geometry precompute) overlaps; its final state is compared
-    with this library's FP64 state after k2 steps."""
+def _reference_cuda_block(nx=16, ny=16, nz=16, k1=10, k2=2010, ours_steps=2000):
+    """The reference's own GPU path, solver/cudg.cu built unmodified for
+    sm_100a into oracle/_ref/cudg (FP32, thread-per-quadrature-point kernels
+    with a device synchronisation after each), beside this library on the
+    same workload: the reference's bump channel, nx x ny x nz hexes, p = 3,
+    q = 2, turbulent initial state, subsonic inflow/outflow, inviscid walls,
+    RK4 dt 1e-4.  (On an all-periodic mesh the reference's driver stops in
+    its norm reduction, so the TGV box is not used here.)  Information only,
+    not a parity target: the reference's CUDA path approximates BR2 by a
+    local penalty and uses dt/2 in stage 3 of RK4.
+
+    The reference is timed by the wall times of two whole driver runs,
+    (k2 - k1) steps / (t(k2) - t(k1)), which removes process start and its
+    set-up (its geometry precompute runs on one host core); k2 - k1 is sized
+    so the difference is many seconds (process start alone varies by a
+    second or two).  This library is timed in process on the same initial
+    state (written by dgb -niter 0) through the C ABI call the dgb driver
+    makes, `ours_steps` steps with the printed norm of every step: wall time
+    (host overheads included, as in the reference's figure) and CUDA
+    events."""
     import tempfile
-    exe = os.path.join(ROOT, "oracle", "_ref", "cudg")
-    if not os.path.exists(exe):
-        return {"unavailable": "oracle/_ref/cudg was not built (the reference tree is needed to compile it)"}
-    nodes, prm, U0, dt = tgv_case(n, P_ORD)
-    mesh = dg.Mesh(n, n, n, P_ORD, 1, nodes, [dg.PERIODIC] * 6)
-    dof_step = 4 * 5 * (P_ORD + 1) ** 3 * n ** 3
-    out = {"workload": f"reference cudg (FP32) -ifile TGV {n}^3 p={P_ORD} -scheme RK4", "steps": [k1, k2]}
+    ref = os.path.join(ROOT, "oracle", "_ref", "cudg")
+    ours = os.path.join(ROOT, "dgpr_b200", "_lib", "dgb")
+    out = {"workload": f"bump channel {nx}x{ny}x{nz}, p = 3, q = 2, -turb, subsonic inflow/outflow, inviscid "
+                       f"walls, RK4 dt 1e-4"}
+    dof_step = 4 * 5 * 64 * nx * ny * nz
+    args = ["-p", "3", "-nx", str(nx), "-ny", str(ny), "-nz", str(nz), "-turb", "-scheme", "RK4", "-dt", "1e-4",
+            "-chkint", "100000000"]
     with tempfile.TemporaryDirectory() as d:
-        dg.write_state(os.path.join(d, "tgv.dg"), 0, mesh, {"state": U0})
-        procs, t0 = [], time.perf_counter()
-        for k in (k1, k2):
-            args = [exe, "-ifile", os.path.join(d, "tgv"), "-niter", str(k), "-chkint", str(10 * k2), "-scheme",
-                    "RK4", "-dt", repr(dt), "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0",
-                    "-ofile", os.path.join(d, f"out{k}")]
-            procs.append(subprocess.Popen(args, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE))
-        walls = []
-        for p in procs:
-            _, err = p.communicate(timeout=900)
-            walls.append(time.perf_counter() - t0)
-            if p.returncode != 0:
-                return {"unavailable": f"cudg exited {p.returncode}: {err.decode()[-300:]}"}
-        _, _, Uref = dg.read_state(os.path.join(d, f"out{k2}.dg"))
-    with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as s:
-        s.set_state(U0)
-        s.step(dg.RK4, dt, k2, norms=False)
-        Uours = s.get_state()
-    rate = dof_step * (k2 - k1) / max(walls[1] - walls[0], 1e-9)
-    out.update({"wall_s": walls, "ms_per_step": 1e3 * (walls[1] - walls[0]) / (k2 - k1),
-                "value": rate, "unit": UNIT,
-                "rel_l2_vs_fp64_after_k2": float(np.linalg.norm(Uref - Uours) / np.linalg.norm(Uours)),
-                "finite": bool(np.all(np.isfinite(Uref)))})
+        if os.path.exists(ref):
+            walls, rc = [], 0
+            for k in (k1, k2):
+                t0 = time.perf_counter()
+                r = subprocess.run([ref] + args + ["-niter", str(k), "-ofile", os.path.join(d, f"ref{k}")],
+                                   stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, timeout=1200)
+                walls.append(time.perf_counter() - t0)
+                rc = rc or r.returncode
+            if rc == 0:
+                ms = 1e3 * (walls[1] - walls[0]) / (k2 - k1)
+                out["reference_cudg_fp32"] = {"steps": [k1, k2], "wall_s": walls, "ms_per_step": ms,
+                                              "value": dof_step / (ms * 1e-3), "unit": UNIT}
+            else:
+                out["reference_cudg_fp32"] = {"unavailable": f"exited {rc}: {r.stderr.decode()[-200:]}"}
+        else:
+            out["reference_cudg_fp32"] = {"unavailable": "oracle/_ref/cudg was not built"}
+        if os.path.exists(ours):
+            import dgpr_b200 as dg
+            import torch
+            subprocess.run([ours] + args + ["-niter", "0", "-ofile", os.path.join(d, "init")],
+                           stdout=subprocess.DEVNULL, check=True, timeout=300)
+            _, mesh, U = dg.read_state(os.path.join(d, "init.dg"))
+            stream = torch.cuda.Stream()
+            for prec, name in ((dg.FP64, "dgb_fp64"), (dg.MIXED_FP32, "dgb_mixed")):
+                with dg.Solver(mesh, dg.make_reference_state(), prec) as s:
+                    s.set_stream(stream.cuda_stream)
+                    s.set_state(U)
+                    _warm(dg, torch, s, 1e-4, 3, min_seconds=0.2)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    ev_ms = _timed_steps(dg, torch, s, stream, 1e-4, ours_steps)
+                    wall_ms = 1e3 * (time.perf_counter() - t0) / ours_steps
+                out[name] = {"steps": ours_steps, "ms_per_step": wall_ms, "value": dof_step / (wall_ms * 1e-3),
+                             "unit": UNIT, "device_ms_per_step": ev_ms / ours_steps}
+    r = out.get("reference_cudg_fp32", {})
+    for name in ("dgb_fp64", "dgb_mixed"):
+        o = out.get(name, {})
+        if "value" in r and "value" in o:
+            out[f"{name}_over_reference_cuda"] = o["value"] / r["value"]
     return out
+
+
+def _cpu_config_worker(name):
+    """One process, one core: the reference's FP64 CPU solver on a sample of
+    one benchmark configuration; returns (RK-stage DOF-updates/s, sample)."""
+    import oracle
+    from tests import cases as C
+    ref = oracle.reference()
+    if name == "config1":  # the isentropic vortex in full: 8^3, p = 2, RK4 dt 0.01
+        c = [k for k in C.long_run_cases() if k.name == "vortex_8_p2_100"][0]
+        m = oracle.Mesh(c.nx, c.ny, c.nz, c.p, c.q, c.nodes, c.bounds)
+        prm, U, scheme, dt, nst, steps = c.prm, c.U, 0, c.dt, 4, 2
+        sample = "the whole 8^3 p=2 vortex mesh, 2 RK4 steps"
+    elif name == "config4":  # Fourier modes on a uniform flow, Re 500 Ma 0.3, p = 3
+        import torch
+        from dgpr_b200 import functionals as F
+        n, p = 6, 3
+        L = 2 * math.pi
+        prm = C.params(mu=1.0 / 500.0, c=1.0 / 0.3, u=1.0, v=0.0, w=0.0)
+        nodes = C.box_nodes(n, n, n, 1, L, L, L)
+        xyz = F.box_node_coords(n, n, n, p, L, L, L)
+        modes = F.FourierModes(xyz, 1.4, 1.0, prm[5], (1.0, 0.0, 0.0), nmodes=8, kmax=4, amp=0.05, seed=0)
+        U = modes.state(modes.amplitudes("cpu")).detach().numpy().ravel()
+        m = oracle.Mesh(n, n, n, p, 1, nodes, [-2] * 6)
+        scheme, dt, nst, steps = 0, 0.2 * (L / 16) / (7 * (1 / 0.3 + 1.5)), 4, 1
+        sample = "a periodic 6^3 block of the 16^3 configuration's flow (same p, same per-element work), 1 RK4 step"
+    else:  # config 5: curved channel, q = 2, no-slip walls (the reference's), p = 3, TVD-RK3
+        nx, ny, nz, p, q = 8, 4, 4, 3, 2
+        lx, ly, lz = 4 * math.pi * nx / 64, 2.0 * ny / 32, 2 * math.pi * nz / 32
+        nodes = C.sine_nodes(nx, ny, nz, q, lx, ly, lz, 0.1, walls=True)
+        prm = C.params(mu=2.0 / 5600.0, c=5.0, u=0.0)
+        rng = np.random.default_rng(5)
+        U = C.random_state(prm, nx * ny * nz, (p + 1) ** 3, rng, amp=0.02).ravel()
+        m = oracle.Mesh(nx, ny, nz, p, q, nodes, [-2, -2, -7, -7, -2, -2])
+        scheme, dt, nst, steps = 1, 1e-4, 3, 1
+        sample = "an 8x4x4 block of the channel (q = 2 sinusoidal map, the reference's no-slip walls), 1 TVD-RK3 step"
+    t0 = time.perf_counter()
+    ref.run(m, prm, U, scheme, dt, 0)
+    t1 = time.perf_counter()
+    ref.run(m, prm, U, scheme, dt, steps)
+    t2 = time.perf_counter()
+    stage_s = max((t2 - t1) - (t1 - t0), 1e-9) / (nst * steps)
+    dof = 5 * (m.p + 1) ** 3 * m.nelem
+    return dof / stage_s, sample
+
+
+def _cpu_configs_block():
+    """The reference's FP64 CPU solver on samples of configurations 1, 4 and
+    5, one process per configuration, one core each (the reference has no
+    threads): its single-core RK-stage DOF-updates/s per configuration.
+    Configuration 3 (48^3, p = 4) is out of the reference's reach here: its
+    geometry precompute needs more host memory than the machine has."""
+    import oracle
+    if oracle.reference() is None:
+        return {"unavailable": "oracle/_ref/libdgref.so was not built"}
+    import multiprocessing as mp
+    names = ("config1", "config4", "config5")
+    with mp.get_context("spawn").Pool(len(names)) as pool:
+        res = pool.map(_cpu_config_worker, names)
+    return {n: {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": smp}
+            for n, (v, smp) in zip(names, res)}
 
 
 def _hbm_peak():
@@ -853,6 +944,8 @@ def run_ours(args, rank, world, local_rank):
     channel = _channel_block(dg, torch, min(args.steps, 20)) if rank == 0 and not args.no_channel else None
     geometry = _geometry_block(dg, torch) if rank == 0 and not args.no_geometry else None
     ckpt = _checkpoint_block(dg) if rank == 0 and not args.no_checkpoint else None
+    refcuda = _reference_cuda_block() if rank == 0 and not args.no_reference_cuda else None
+    cpu_cfg = (_cpu_configs_block() if rank == 0 and not args.no_cpu_baseline and world == 1 else None)
     chadj = (_channel_adjoint_block(dg, torch, args.channel_adjoint_steps)
              if rank == 0 and not args.no_channel and args.channel_adjoint_steps > 0 else None)
 
@@ -913,6 +1006,8 @@ def run_ours(args, rank, world, local_rank):
             "geometry": geometry,
             "channel_adjoint": chadj,
             "checkpoint_cadence": ckpt,
+            "reference_cuda": refcuda,
+            "cpu_baseline_configs": cpu_cfg,
             "clocks": clocks,
         }
         if cpu:
@@ -958,6 +1053,8 @@ def main():
                     help="steps of the mixed-vs-FP64 accuracy check (0 skips it)")
     ap.add_argument("--no-config3", action="store_true", help="skip the 48^3 p = 4 block")
     ap.add_argument("--no-checkpoint", action="store_true", help="skip the driver's checkpoint-cadence timing")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own GPU driver beside dgb")
     ap.add_argument("--config3-accuracy-steps", type=int, default=1000,
                     help="steps of the 48^3 p = 4 mixed-vs-FP64 accuracy and kinetic-energy check (0 skips it)")
     args = ap.parse_args()

@@ -339,13 +339,14 @@ int main(int argc, char** argv)
       exit(1);
     }
   };
-  if (in.chkint && in.chkint <= in.niter) {
+  auto writer_buffers = [&]() {  // made at the first checkpoint (whichever step index it falls on)
+    if (writer.d_snap) return;
     const size_t bytes = sizeof(double) * U.size();
     cuda_ok(cudaStreamCreateWithFlags(&writer.copy, cudaStreamNonBlocking), "checkpoint stream");
     cuda_ok(cudaEventCreateWithFlags(&writer.done, cudaEventDisableTiming), "checkpoint event");
     cuda_ok(cudaMalloc(&writer.d_snap, bytes), "checkpoint snapshot");
     cuda_ok(cudaMallocHost(&writer.h_state, bytes), "checkpoint host buffer");
-  }
+  };
 
   // running mean (dg.cpp:123-131): an input file may carry one to continue
   std::vector<double> M(U.size());
@@ -380,6 +381,7 @@ int main(int argc, char** argv)
       char f[1100];
       snprintf(f, sizeof f, "%s%" PRIu64 ".dg", in.ofile.c_str(), (uint64_t)tstep);
       writer.wait();  // the previous checkpoint's file is written: its buffers are free
+      writer_buffers();
       if ((rc = dgb_get_state_device(h, writer.d_snap))) die("dgb_get_state_device", rc);
       // continue from the state as written, as a restart from this file
       // would (dgb_step otherwise continues from its Gauss-point copy)

@@ -33,14 +33,31 @@
 #define DGB_PREFETCH_L2_F32 1
 #endif
 
+// Faces per pass of the Gauss-point kernels' face phase and trace epilogue:
+// 6 is one pass over all 6 P^2 face points, each thread striding over them;
+// 0 takes the nodal kernels' DGB_FACES_PER_PASS (3: two passes, the threads
+// past 3 P^2 idle).  One pass leaves fewer half-empty warps and barriers for
+// more shared memory (still 10 CTAs per SM at p = 3); measured on the B200
+// against two passes, same bits: FP64 stage -4.5% (32^3, p = 3) and -3%
+// (24^3, p = 4), mixed -1.4% and -6.5%.
+#ifndef DGB_VFACES_PER_PASS
+#define DGB_VFACES_PER_PASS 6
+#endif
+
 namespace dgb {
+
+template <int P>
+struct VF {
+  static constexpr int FN = DGB_VFACES_PER_PASS ? DGB_VFACES_PER_PASS : Cfg<P>::FPP;
+  static_assert(6 % FN == 0, "faces per pass must divide 6");
+};
 
 // Shared memory: [operators (T) | element geometry (T)] followed by one
 // scratch region reused by the phases:
 //   volume  V1[5NB] values, G[3][5][NB] gradients then contravariant fluxes
-//   faces   Fa[FPP][5][NQF] Fb[FPP][12][NQF] Gt[FPP][9][NQF]
+//   faces   Fa[FN][5][NQF] Fb[FN][12][NQF] Gt[FN][9][NQF]
 //   norm    Y0[5NB] Y1[5NB] (nodal residual for the printed norm), red[NTS] (FP64)
-//   traces  sN[FPP][10][NQF], then the new state at oTrU
+//   traces  sN[FN][10][NQF], then the new state at oTrU
 template <int P, class T>
 struct VStageSmem {
   using C = Cfg<P>;
@@ -50,10 +67,10 @@ struct VStageSmem {
   static constexpr int oGeo = align16(C::OPS * ST);
   static constexpr int oX = oGeo + align16(kGeoStride * ST);
   static constexpr int VOL = 20 * NB * ST;
-  static constexpr int FACE = C::FPP * (5 + 12 + 9) * NQF * ST;
+  static constexpr int FACE = VF<P>::FN * (5 + 12 + 9) * NQF * ST;
   static constexpr int oRed = align16(10 * NB * ST);
   static constexpr int NORM = oRed + C::NTS * 8;
-  static constexpr int oTrU = align16(10 * C::FPP * NQF * ST);
+  static constexpr int oTrU = align16(10 * VF<P>::FN * NQF * ST);
   static constexpr int TRACE = oTrU + 5 * NB * ST;
   static constexpr int X0 = VOL > FACE ? VOL : FACE;
   static constexpr int X1 = NORM > TRACE ? NORM : TRACE;
@@ -69,21 +86,22 @@ struct VTraceSmem {
   static constexpr int oGeo = align16(C::OPS * ST);
   static constexpr int oU = oGeo + align16(kGeoStride * ST);
   static constexpr int oN = oU + align16(5 * C::NB * ST);
-  static constexpr int TOTAL = oN + align16(10 * C::FPP * C::NQF * ST);
+  static constexpr int TOTAL = oN + align16(10 * VF<P>::FN * C::NQF * ST);
 };
 
-// Traces of a Gauss-point state sV[5][NB] (shared memory) on the FPP faces
-// lf = FPP*half + j, into Te (this element's slice of the trace buffer), in
-// the trace format of trace_half.  Scratch sN[FPP][10][NQF].
+// Traces of a Gauss-point state sV[5][NB] (shared memory) on the FN faces
+// lf = FN*half + j, into Te (this element's slice of the trace buffer), in
+// the trace format of trace_half.  Scratch sN[FN][10][NQF].
 template <int P, class T, bool CV>
 __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const T* so, const T* sg, T mu, T kq,
                                             T* __restrict__ Te, const double* __restrict__ gfe)
 {
   using C = Cfg<P>;
-  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
+  constexpr int NB = C::NB, NQF = C::NQF, FN = VF<P>::FN, NH = FN * NQF;
   const int tid = threadIdx.x;
-  if (tid < NH) {  // along the normal line: value and normal derivative at the face point
-    const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P;
+#pragma unroll 1
+  for (int i = tid; i < NH; i += blockDim.x) {  // along the normal line: value and normal derivative
+    const int j = i / NQF, lf = FN * half + j, fq = i % NQF, t1 = fq % P, t2 = fq / P;
     const int a = lf >> 1, end = lf & 1;
     const T* Ev = so + C::oEh + end * P;
     const T* Dv = so + C::oDh + end * P;
@@ -102,8 +120,9 @@ __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const 
     }
   }
   __syncthreads();
-  if (tid < NH) {  // tangential derivatives on the face, then the viscous normal flux
-    const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
+#pragma unroll 1
+  for (int i = tid; i < NH; i += blockDim.x) {  // tangential derivatives on the face, then the viscous normal flux
+    const int j = i / NQF, lf = FN * half + j, fq = i % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
     const T* in = sN + j * 10 * NQF;
     const T* Dq = so + C::oDq;
     T S[5], g[3][5];
@@ -148,7 +167,7 @@ vtrace_kernel(long E, const double* __restrict__ V, const T* __restrict__ opsg, 
   __syncthreads();
   T* Te = Tr + e * 60 * NQF;
 #pragma unroll 1
-  for (int half = 0; half < 6 / C::FPP; ++half) {
+  for (int half = 0; half < 6 / VF<P>::FN; ++half) {
     if (half) __syncthreads();
     vtrace_half<P, T, CV>(half, sV, sN, so, sg, T(prm.mu), HT ? T(prm.kq) : T(0), Te,
                           CV ? gf + e * 6 * kFaceC * NQF : nullptr);
@@ -203,7 +222,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 {
   using C = Cfg<P>;
   using L = VStageSmem<P, T>;
-  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
+  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* so = reinterpret_cast<T*>(smraw + L::oOps);
   T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
@@ -308,16 +327,18 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* Gt = Fb + FPP * 12 * NQF;   // [FPP][9][NQF]
 #pragma unroll 1
   for (int half = 0; half < 6 / FPP; ++half) {
-    if (tid < NH) {
-      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF;
+#pragma unroll 1
+    for (int i = tid; i < NH; i += blockDim.x) {
+      const int j = i / NQF, lf = FPP * half + j, fq = i % NQF;
       T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
       const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
       face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
                                   sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
     __syncthreads();
-    if (tid < NH) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
-      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
+#pragma unroll 1
+    for (int i = tid; i < NH; i += blockDim.x) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
+      const int j = i / NQF, lf = FPP * half + j, fq = i % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
       const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
       const T* fa = Fa + j * 5 * NQF;
       const T* fb = Fb + j * 12 * NQF;
@@ -519,7 +540,7 @@ vtrace2_kernel(long E, const double* __restrict__ V, const float* __restrict__ o
   __syncthreads();
   f2* Te = Tr2 + k * 60 * NQF;
 #pragma unroll 1
-  for (int half = 0; half < 6 / C::FPP; ++half) {
+  for (int half = 0; half < 6 / VF<P>::FN; ++half) {
     if (half) __syncthreads();
     vtrace_half<P, f2, false>(half, sV, sN, so, sg, f2(prm.mu), HT ? f2(prm.kq) : f2(0.f), Te, nullptr);
   }
@@ -570,7 +591,7 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
   using L = VStageSmem<P, f2>;
   using LP = VPairSmem<P>;
   using T = f2;
-  constexpr int NB = C::NB, NQF = C::NQF, NH = C::NF, FPP = C::FPP;
+  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* so = reinterpret_cast<T*>(smraw + L::oOps);
   T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
@@ -679,8 +700,9 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
   T* Gt = Fb + FPP * 12 * NQF;
 #pragma unroll 1
   for (int half = 0; half < 6 / FPP; ++half) {
-    if (tid < NH) {
-      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF;
+#pragma unroll 1
+    for (int i = tid; i < NH; i += blockDim.x) {
+      const int j = i / NQF, lf = FPP * half + j, fq = i % NQF;
       const int nb0 = nbr[el[0] * 6 + lf], nb1 = nbr[el[1] * 6 + lf];
       const T* To = Tr2 + (k * 6 + lf) * 10 * NQF;
       T* fa = Fa + j * 5 * NQF + fq;
@@ -708,8 +730,9 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
       }
     }
     __syncthreads();
-    if (tid < NH) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
-      const int j = tid / NQF, lf = FPP * half + j, fq = tid % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
+#pragma unroll 1
+    for (int i = tid; i < NH; i += blockDim.x) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
+      const int j = i / NQF, lf = FPP * half + j, fq = i % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
       const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
       const T* fa = Fa + j * 5 * NQF;
       const T* fb = Fb + j * 12 * NQF;

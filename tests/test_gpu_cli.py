@@ -121,3 +121,24 @@ def test_dgb_isothermal_wall_option(tmp_path):
     c = run("c_", ["-bpy", "inviscid_wall", "-twall", "0.003"])
     d = run("d_", ["-bpy", "inviscid_wall"])
     assert np.array_equal(c, d)
+
+
+def test_dgb_checkpoint_index_inside_a_short_restart(tmp_path):
+    """A checkpoint index can fall inside a run shorter than -chkint: the
+    reference checkpoints before every step with (tstep + 1) % chkint == 0,
+    counting from the step the input file resumes at (cudg.cu:112-130).
+    Restarting after step 3 for 4 steps with -chkint 7 writes the checkpoint
+    before step 6, like the reference driver, with the same state."""
+    if not os.path.exists(REF):
+        pytest.skip("reference driver not built here")
+    _run(DGB, "full_", tmp_path)
+    args = ["-niter", "4", "-chkint", "7", "-dt", "1e-3", "-mu", "1e-2", "-u", "0.3", "-scheme", "RK4",
+            "-ifile", "full_3"]
+    for exe, prefix in ((DGB, "ours_"), (REF, "ref_")):
+        out = subprocess.run([exe] + args + ["-ofile", prefix], cwd=tmp_path, capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stderr
+    for suffix in ("6.dg", ".dg"):
+        ta, _, a = dg.read_state(str(tmp_path / f"ours_{suffix}"))
+        tb, _, b = dg.read_state(str(tmp_path / f"ref_{suffix}"))
+        assert ta == tb and np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12, suffix
