@@ -360,6 +360,21 @@ def _adjoint_config(dg, torch, nsteps, budgets):
         an = float((torch.tensor(grad, device="cuda") * d).sum())
         out["fd_check"] = {"directional_adjoint": an, "directional_fd": fd, "rel_err": abs(an - fd) / abs(fd),
                            "h": h}
+        # every one of the 24 components by central differences of FP64 forward
+        # runs, h = 1e-4 |a_k|; the error is taken against the gradient's
+        # largest component
+        a0h = a0.detach().cpu().numpy().ravel()
+        fdv = np.zeros(a0h.size)
+        for k in range(a0h.size):
+            hk = 1e-4 * max(abs(a0h[k]), 1e-3)
+            e = torch.zeros_like(a0).view(-1)
+            e[k] = hk
+            e = e.view_as(a0)
+            fdv[k] = (Jof(a0 + e) - Jof(a0 - e)) / (2 * hk)
+        gv = np.asarray(grad).ravel()
+        out["fd_full"] = {"components": int(a0h.size), "h": "1e-4 |a_k|",
+                          "max_abs_err_over_max_grad": float(np.max(np.abs(gv - fdv)) / np.max(np.abs(gv))),
+                          "rel_l2": float(np.linalg.norm(gv - fdv) / np.linalg.norm(gv))}
         # the same sweep with dJ/d[mu, source] (dgb_backward_params), stage-keeping record
         s.set_state(U0.cpu().numpy())
         s.forward_record_stages(dg.RK4, dt, nsteps, norms=False)
@@ -547,13 +562,16 @@ def _channel_adjoint_block(dg, torch, nsteps, slots=50):
 
 def _checkpoint_block(dg, steps=600, chkints=(30, 150)):
     """Checkpoint cadence of the dgb driver (C++ host code over the C ABI,
-    the drop-in for the reference's cudg): wall time of `steps` RK4 steps of
-    the TGV workload read from a .dg file, writing a .dg checkpoint every
-    `chkint` steps, against the same run with none.  The driver writes each
-    checkpoint from a device snapshot on a host thread while the steps go on,
-    so a checkpoint costs only what its file write exceeds the steps until
-    the next one.  Process start, set-up and the final file are in every
-    time."""
+    the drop-in for the reference's cudg): the wall time of its stepping
+    loop (`-timing`: the steps and every checkpoint file, not the set-up or
+    the final file) for `steps` RK4 steps of the TGV workload read from a
+    .dg file, writing a .dg checkpoint every `chkint` steps, against the
+    same loop with none.  The driver writes each checkpoint from a device
+    snapshot on a host thread while the steps go on, so a checkpoint costs
+    only what its file write exceeds the steps until the next one; with
+    -chksync it writes each file before the next step, as the reference's
+    cudg does, for comparison."""
+    import re
     import tempfile
     exe = os.path.join(ROOT, "dgpr_b200", "_lib", "dgb")
     if not os.path.exists(exe):
@@ -565,18 +583,24 @@ def _checkpoint_block(dg, steps=600, chkints=(30, 150)):
     with tempfile.TemporaryDirectory() as d:
         dg.write_state(os.path.join(d, "tgv.dg"), 0, mesh, {"state": U0})
         args = [exe, "-ifile", os.path.join(d, "tgv"), "-niter", str(steps), "-scheme", "RK4", "-dt", repr(dt),
-                "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0",
+                "-mu", repr(1.0 / 1600.0), "-c", "10", "-u", "0", "-v", "0", "-w", "0", "-timing",
                 "-ofile", os.path.join(d, "out")]
-        runs = [("no_checkpoints_s", 10 * steps)] + [(f"checkpoint_every_{c}_s", c) for c in chkints] + \
-               [("no_checkpoints_again_s", 10 * steps)]
-        for name, ci in runs:
-            t0 = time.perf_counter()
-            subprocess.run(args + ["-chkint", str(ci)], stdout=subprocess.DEVNULL, check=True, timeout=600)
-            out[name] = time.perf_counter() - t0
-    base = min(out["no_checkpoints_s"], out["no_checkpoints_again_s"])
-    for c in chkints:
-        out[f"overhead_frac_every_{c}"] = out[f"checkpoint_every_{c}_s"] / base - 1.0
-        out[f"checkpoints_written_every_{c}"] = steps // c
+        runs = [("no_checkpoints_s", 10 * steps, [])] + \
+               [(f"checkpoint_every_{c}_s", c, []) for c in chkints] + \
+               [(f"checkpoint_every_{c}_written_before_the_next_step_s", c, ["-chksync"]) for c in chkints] + \
+               [("no_checkpoints_again_s", 10 * steps, [])]
+        for name, ci, extra in runs:
+            r = subprocess.run(args + extra + ["-chkint", str(ci)], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                               check=True, timeout=600)
+            m = re.search(r"steps in ([0-9.]+) s", r.stderr.decode())
+            out[name] = float(m.group(1)) if m else None
+    if all(out[n] for n, _, _ in runs):
+        base = min(out["no_checkpoints_s"], out["no_checkpoints_again_s"])
+        for c in chkints:
+            out[f"overhead_frac_every_{c}"] = out[f"checkpoint_every_{c}_s"] / base - 1.0
+            out[f"overhead_frac_every_{c}_written_before_the_next_step"] = \
+                out[f"checkpoint_every_{c}_written_before_the_next_step_s"] / base - 1.0
+            out[f"checkpoints_written_every_{c}"] = steps // c
     return out
 
 
@@ -1023,6 +1047,7 @@ def run_ours(args, rank, world, local_rank):
             head["adjoint_reverse_over_forward"] = adj["reverse_over_forward"]
             head["adjoint_config_backward_over_forward"] = {
                 str(b["slots"]): round(b["backward_over_plain_forward"], 3) for b in adj["config"]["budgets"]}
+            head["adjoint_config_fd_rel_l2"] = adj["config"]["fd_full"]["rel_l2"]
         if chadj:
             head["channel_grad_rel_err_fp64"] = chadj["rel_err_fp64_adjoint_vs_fd"]
             head["channel_grad_rel_err_mixed"] = chadj["rel_err_mixed_forward_vs_fd"]

@@ -15,6 +15,7 @@
 // extension; 0, the default, is the reference's physics).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cinttypes>
 #include <cmath>
 #include <cstdio>
@@ -47,6 +48,8 @@ struct Inputs {
   int precision = DGB_FP64;
   double prandtl = 0.;
   double twall = -1.;  // isothermal walls' temperature (< 0: the reference temperature)
+  bool timing = false;  // report the stepping loop's wall time on stderr
+  bool chksync = false;  // write each checkpoint before the next step, as cudg.cu does
 };
 
 enum Kind { K_U64, K_DBL, K_STR, K_BOOL, K_BTYPE, K_SCHEME, K_PREC };
@@ -125,6 +128,8 @@ int parse(int argc, char** argv, Inputs& in)
       {"precision", "arithmetic: fp64 or mixed", K_PREC, &in.precision},
       {"prandtl", "Prandtl number of the heat flux (0: none)", K_DBL, &in.prandtl},
       {"twall", "temperature of isothermal_wall sides (default: reference T)", K_DBL, &in.twall},
+      {"timing", "print the stepping loop's wall time (checkpoints included) on stderr", K_BOOL, &in.timing},
+      {"chksync", "write each checkpoint before the next step (the reference's order)", K_BOOL, &in.chksync},
   };
   const int nopt = (int)(sizeof opts / sizeof opts[0]);
   if (argc > 1 && !strcmp(argv[1], "-h")) {
@@ -374,7 +379,8 @@ int main(int argc, char** argv)
   // satisfies (tstep + 1) % chkint == 0 (cudg.cu:112-130); between checkpoints
   // the steps run as one dgb_step call (one CUDA graph replay per step), or
   // one at a time once the running mean is being accumulated
-  const unsigned long long tfinal = tstep + in.niter;
+  const unsigned long long tfinal = tstep + in.niter, tstart = tstep;
+  const auto t_loop = std::chrono::steady_clock::now();
   std::vector<double> norms;
   while (tstep < tfinal) {
     if (in.chkint && (tstep + 1) % in.chkint == 0) {
@@ -403,7 +409,7 @@ int main(int argc, char** argv)
         const double* d[2] = {writer.h_state, M.data()};
         writer.rc = dgb_write_state(file.c_str(), ts, &mesh, with_mean ? 2 : 1, k, d);
       });
-      if (with_mean) writer.wait();  // the mean's host copy is reused by the next update
+      if (with_mean || in.chksync) writer.wait();  // the mean's host copy is reused by the next update
     }
     unsigned long long n = tfinal - tstep;
     if (in.chkint) {  // up to, not including, the next checkpointing step
@@ -431,6 +437,11 @@ int main(int argc, char** argv)
     }
   }
   writer.wait();
+  if (in.timing) {  // the steps and every checkpoint file, not the set-up or the final file
+    const double s_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();
+    fprintf(stderr, "dgb: %" PRIu64 " steps in %.6f s (%.6f ms/step)\n", (uint64_t)(tstep - tstart), s_loop,
+            tstep > tstart ? 1e3 * s_loop / (double)(tstep - tstart) : 0.);
+  }
   write(in.ofile + ".dg", tstep - 1);  // the index of the last step taken, as cudg.cu:140-141 writes
   dgb_destroy(h);
   return 0;
