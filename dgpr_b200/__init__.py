@@ -94,6 +94,8 @@ def lib():
             "dgb_residual": (ctypes.c_int, [vp, _dp, _dp, _dp]),
             "dgb_residual_device": (ctypes.c_int, [vp, vp, vp, vp]),
             "dgb_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp]),
+            "dgb_step_host": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp, _dp,
+                                             _dp]),
             "dgb_last_launch_count": (ctypes.c_longlong, [vp]),
             "dgb_profile_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
                                                 ctypes.POINTER(ctypes.c_int)]),
@@ -381,6 +383,16 @@ class Solver:
         out = np.zeros(max(int(nsteps), 1))
         _check(lib().dgb_step(self.h, int(scheme), float(dt), int(nsteps), _p(out) if norms else None))
         return out[:nsteps]
+
+    def step_host(self, scheme, dt, nsteps, U_in, U_out, norms=True):
+        """dgb_step_host: nsteps steps of the host state U_in into U_out
+        (float64 numpy arrays, page-locked for the overlap), the copies
+        overlapped with the work; returns the per-step norms."""
+        assert U_in.dtype == np.float64 and U_out.dtype == np.float64 and U_in.size == U_out.size == self.n
+        out = np.zeros(max(int(nsteps), 1)) if norms else None
+        _check(lib().dgb_step_host(self.h, int(scheme), float(dt), int(nsteps), _p(U_in), _p(U_out),
+                                   _p(out) if norms else None))
+        return out[:nsteps] if norms else None
 
     def profile_step(self, scheme, dt, reps):
         """Mean per-launch durations (ms) of one RK step, CUDA events on the

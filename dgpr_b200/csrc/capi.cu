@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -72,7 +73,17 @@ int enqueue_initial_traces(dgb_handle* h, bool gauss)
 // With ev != null, ev[i] is recorded before launch i and ev[nlaunch] after the
 // last one (per-kernel timing by dgb_profile_step).  gauss: the Gauss-point
 // form on d_V (vspace.cuh), else the nodal form on d_U.
-int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr, bool gauss = false)
+// The last stage of a step in pieces of elements [bound[c], bound[c+1]),
+// with after(c) enqueued behind piece c (dgb_step_host copies each piece out
+// while the next one computes).
+struct LastStagePieces {
+  int n = 0;
+  const long* bound = nullptr;
+  std::function<int(int)> after;
+};
+
+int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr, bool gauss = false,
+                 const LastStagePieces* pieces = nullptr)
 {
   double* Ures = gauss ? h->d_V : h->d_U;
   const KLaunch L = klaunch(h);
@@ -93,10 +104,20 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
     const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-    if (gauss)
+    if (pieces && gauss && s == nst - 1) {
+      for (int c = 0; c < pieces->n; ++c) {
+        if (pieces->bound[c + 1] == pieces->bound[c]) continue;  // (an ecount of 0 would mean all elements)
+        a.e0 = pieces->bound[c];
+        a.ecount = pieces->bound[c + 1] - pieces->bound[c];
+        CK(launch_vstage(L, in, tin, a, h->stream));
+        const int rc = pieces->after(c);
+        if (rc) return rc;
+      }
+    } else if (gauss) {
       CK(launch_vstage(L, in, tin, a, h->stream));
-    else
+    } else {
       CK(launch_stage(L, in, tin, a, h->stream));
+    }
     if (s == 0) {
       if (ev) CK(cudaEventRecord(ev[k++], h->stream));
       CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
@@ -118,6 +139,8 @@ void free_all(dgb_handle* h)
   for (void* p : ptrs)
     if (p) cudaFree(p);
   free_adjoint(h);
+  for (cudaEvent_t e : h->host_events) cudaEventDestroy(e);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -578,6 +601,97 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
   if (norms_host)
     CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
+  return DGB_OK;
+}
+
+int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
+                  double* U_out, double* norms_host)
+{
+  if (!h || !U_in || !U_out) return fail(DGB_ERR_ARG, "null argument");
+  if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
+  if (!(dt == dt)) return fail(DGB_ERR_ARG, "dt is NaN");
+  CK(cudaSetDevice(h->device));
+  int rc;
+  if (nsteps == 0 || !h->gauss_step) {  // nothing to overlap: the plain calls
+    if ((rc = dgb_set_state(h, U_in))) return rc;
+    if (nsteps && (rc = dgb_step(h, scheme, dt, nsteps, norms_host))) return rc;
+    return dgb_get_state(h, U_out);
+  }
+  // pieces of elements with even boundaries (the paired kernels take
+  // elements two by two); an odd element count, whose traces are not paired,
+  // copies in as one piece (a piece of even count would take the paired
+  // trace kernel)
+  constexpr int K = 8;
+  long bound[K + 1];
+  for (int c = 0; c <= K; ++c) bound[c] = (h->E * c / K) & ~1L;
+  bound[K] = h->E;
+  const bool one_in = h->E % 2 != 0;
+  if (!h->copy_stream) CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  while (h->host_events.size() < 2 * K + 1) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->host_events.push_back(e);
+  }
+  cudaEvent_t* ev_in = h->host_events.data();
+  cudaEvent_t* ev_out = ev_in + K;
+  cudaEvent_t ev_start = ev_in[2 * K];
+  if ((rc = ensure_step_graph(h, scheme, dt, nsteps, true))) return rc;
+  CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  // the copies in start once the handle's earlier work is done with d_U
+  CK(cudaEventRecord(ev_start, h->stream));
+  CK(cudaStreamWaitEvent(h->copy_stream, ev_start, 0));
+  const KLaunch L = klaunch(h);
+  const long nbv = 5L * h->NB;  // values per element of a state
+  const size_t tb = trace_elem_bytes(h->precision);
+  auto piece = [&](long e0, long e1) {  // the launch description of elements [e0, e1): own data only
+    KLaunch Lc = L;
+    Lc.E = e1 - e0;
+    Lc.geo = L.geo + e0 * kGeoStride;
+    Lc.gv = L.gv ? L.gv + e0 * (long)kVolC * h->NB : nullptr;
+    Lc.gf = L.gf ? L.gf + e0 * 6L * kFaceC * h->NQF : nullptr;
+    return Lc;
+  };
+  // in: each piece's copy, then its basis change and face traces (element-local work)
+  for (int c = 0; c < K; ++c) {
+    const long e0 = one_in ? (c ? h->E : 0) : bound[c], e1 = one_in ? h->E : bound[c + 1];
+    if (e1 == e0) continue;
+    CK(cudaMemcpyAsync(h->d_U + e0 * nbv, U_in + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
+                       cudaMemcpyHostToDevice, h->copy_stream));
+    CK(cudaEventRecord(ev_in[c], h->copy_stream));
+    CK(cudaStreamWaitEvent(h->stream, ev_in[c], 0));
+    const KLaunch Lc = piece(e0, e1);
+    CK(launch_gauss_basis(Lc, h->d_U + e0 * nbv, h->d_V + e0 * nbv, true, h->stream));
+    CK(launch_vtrace(Lc, h->d_V + e0 * nbv, static_cast<char*>(h->d_trace[0]) + (size_t)e0 * 60 * h->NQF * tb,
+                     h->stream));
+  }
+  for (unsigned long long s = 0; s + 1 < nsteps; ++s) CK(cudaGraphLaunch(h->ggraph.exec, h->stream));
+  // out: the last stage of the last step piece by piece, each piece changed
+  // back to nodal values and copied out while the next one computes
+  LastStagePieces lp;
+  lp.n = K;
+  lp.bound = bound;
+  lp.after = [&](int c) -> int {
+    const long e0 = bound[c], e1 = bound[c + 1];
+    if (e1 == e0) return DGB_OK;
+    CK(launch_gauss_basis(piece(e0, e1), h->d_V + e0 * nbv, h->d_U + e0 * nbv, false, h->stream));
+    CK(cudaEventRecord(ev_out[c], h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, ev_out[c], 0));
+    CK(cudaMemcpyAsync(U_out + e0 * nbv, h->d_U + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
+                       cudaMemcpyDeviceToHost, h->copy_stream));
+    return DGB_OK;
+  };
+  if ((rc = enqueue_step(h, scheme, dt, nullptr, true, &lp))) return rc;
+  h->v_current = true;
+  h->last_launches = 2L * K + (long long)(nsteps - 1) * h->launches_per_step + h->launches_per_step + K - 1 + K;
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (norms_host)
+    CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaStreamSynchronize(h->copy_stream));
   if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   return DGB_OK;

@@ -67,6 +67,10 @@ struct dgb_handle {
   bool v_current = false;
   long long launches_per_step = 0;
   long long last_launches = 0;
+  // dgb_step_host: a second stream for the host copies and the events that
+  // order them against the pieces of work on the handle's stream
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> host_events;
 
   // ---- adjoint (allocated on first use, adjoint_capi.cu)
   // state-sized buffers: stage states S0..S2, stage adjoints A0 A1, the

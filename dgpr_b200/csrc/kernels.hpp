@@ -31,6 +31,10 @@ struct StageArgs {
   double* part;  // per-element sum of R^2 (stage 1 of a step), or null
   int* flag;     // bit 1: non-finite norm, bit 2: inflow without a Mach root
   void* Tnext;   // face traces of Uout for the next stage (compute type), or null
+  // Gauss-point stage kernels only: elements [e0, e0 + ecount) (ecount 0: all;
+  // both even for the paired kernel), so a stage can run in pieces whose
+  // results are copied out while the next piece computes
+  long e0, ecount;
 };
 
 // everything the kernels read that does not change between stages

@@ -228,7 +228,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
   unsigned char* sXb = smraw + L::oX;
   T* sX = reinterpret_cast<T*>(sXb);
-  const long e = blockIdx.x;
+  const long e = blockIdx.x + sa.e0;
   const int tid = threadIdx.x;
   const bool node = tid < NB;  // thread owns Gauss point `tid`
   const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
@@ -599,7 +599,7 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
   float* sgf = reinterpret_cast<float*>(smraw + LP::oGeoF);  // [2][kGeoStride]
   unsigned char* sXb = smraw + L::oX;
   T* sX = reinterpret_cast<T*>(sXb);
-  const long k = blockIdx.x, e0 = 2 * k;
+  const long k = blockIdx.x + sa.e0 / 2, e0 = 2 * k;
   const long el[2] = {e0, e0 + 1};
   const int tid = threadIdx.x;
   const bool node = tid < NB;
@@ -862,7 +862,7 @@ template <int P, bool HT>
 cudaError_t vlaunch_stage2_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                              cudaStream_t st)
 {
-  vstage2_kernel<P, HT><<<(unsigned)(L.E / 2), Cfg<P>::NTS, VPairSmem<P>::TOTAL, st>>>(
+  vstage2_kernel<P, HT><<<(unsigned)((sa.ecount ? sa.ecount : L.E) / 2), Cfg<P>::NTS, VPairSmem<P>::TOTAL, st>>>(
       L.E, Vs, reinterpret_cast<const f2*>(Tin), reinterpret_cast<const float*>(L.ops), L.opsd, L.geo, L.nbr,
       L.prm, sa);
   return cudaGetLastError();
@@ -955,12 +955,13 @@ template <int P, class T, bool HT>
 cudaError_t vlaunch_stage_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                             cudaStream_t st)
 {
+  const unsigned grid = (unsigned)(sa.ecount ? sa.ecount : L.E);
   if (L.gv)
-    vstage_kernel<P, T, true, HT><<<(unsigned)L.E, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
+    vstage_kernel<P, T, true, HT><<<grid, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
         L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
         L.nbr, L.prm, sa);
   else
-    vstage_kernel<P, T, false, HT><<<(unsigned)L.E, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
+    vstage_kernel<P, T, false, HT><<<grid, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
         L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
         nullptr, L.nbr, L.prm, sa);
   return cudaGetLastError();

@@ -224,6 +224,22 @@ int dgb_residual_device(dgb_handle* h, const double* U_dev, double* R_dev, doubl
 int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps,
              double* norms_host);
 
+/* dgb_step for a state kept in host memory: U_in (host, layout U[e][r][b])
+ * is copied in, nsteps RK steps are taken, and the state after them is
+ * written to U_out (host; may equal U_in), with the printed norm of every
+ * step in norms_host (may be NULL).  The same kernels and results as
+ * dgb_set_state + dgb_step + dgb_get_state, bit for bit, with the copies
+ * overlapped with the work: the state comes in in pieces on a second stream
+ * while the pieces already in are changed to Gauss-point values and their
+ * face traces computed, and the last stage of the last step runs in pieces,
+ * each copied out while the next one computes.  Overlap needs page-locked
+ * (pinned) host buffers; pageable ones give the same results.  The nodal
+ * step form (dgb_set_step_form) takes the plain calls.  No counterpart in
+ * the reference, whose driver copies the state in once and out at each
+ * checkpoint (cudg.cu:96-126). */
+int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
+                  double* U_out, double* norms_host);
+
 /* Kernel launches issued by the last dgb_step / dgb_residual call. */
 long long dgb_last_launch_count(const dgb_handle* h);
 
