@@ -773,9 +773,11 @@ def _config3_block(dg, torch, steps, acc_steps, ke_every=100):
     out = {"workload": f"TGV Re 1600 Ma 0.1, periodic [0,2pi]^3, {n}^3 hexes, p = {p}, RK4 dt={dt:.4e}",
            "dof_per_stage": dof_stage, "algorithmic_bytes_per_stage_launch": alg, "peak_gbs": peak,
            "peak_source": peak_src}
-    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed")):
+    for prec, name in ((dg.FP64, "fp64"), (dg.MIXED_FP32, "mixed"), (dg.MIXED_FP32, "mixed_tensor_core")):
         with dg.Solver(mesh, dg.Params.from_array(prm), prec) as s:
             s.set_stream(stream.cuda_stream)
+            if name == "mixed_tensor_core":
+                s.set_step_form(dg.STEP_GAUSS_TC)
             s.set_state(U0)
             _warm(dg, torch, s, dt, 3)
             ms = _timed_steps(dg, torch, s, stream, dt, steps) / steps
@@ -784,6 +786,7 @@ def _config3_block(dg, torch, steps, acc_steps, ke_every=100):
                      "stage_kernel_ms": kms, "trace_kernel_ms": tms,
                      "stage_roofline_frac": alg / (kms * 1e-3) / 1e9 / peak}
     out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["speedup_mixed_tensor_core_vs_fp64"] = out["mixed_tensor_core"]["value"] / out["fp64"]["value"]
     if acc_steps > 0:
         L = 2 * math.pi
         quad = F.BoxQuadrature(n, n, n, p, L, L, L, device="cuda")
@@ -940,6 +943,14 @@ def run_ours(args, rank, world, local_rank):
     ms_mixed = max_over_ranks(_timed_steps(dg, torch, sm, stream, dt, args.steps))
     value_mixed = replica_rate(world, dof_stage, 4, args.steps, ms_mixed)
     stage_ms_mixed, trace_ms_mixed = _stage_kernel_ms(dg, sm, U0, dt, reps)
+    # the same mixed form with its volume contractions on the tensor cores
+    sm.set_step_form(dg.STEP_GAUSS_TC)
+    sm.set_state(U0)
+    _warm(dg, torch, sm, dt, 3)
+    barrier()
+    torch.cuda.synchronize()
+    ms_tc = max_over_ranks(_timed_steps(dg, torch, sm, stream, dt, args.steps))
+    stage_ms_tc, _ = _stage_kernel_ms(dg, sm, U0, dt, reps)
     sm.close()
 
     # ---- accuracy of the mixed form against the FP64 form after many steps
@@ -1033,7 +1044,13 @@ def run_ours(args, rank, world, local_rank):
                       "roofline": {"bound": "hbm", "achieved": achieved_mixed, "peak": peak, "unit": "GB/s",
                                    "frac": achieved_mixed / peak, "algorithmic_bytes_per_launch": alg_bytes},
                       "dtype": "f32 contractions/fluxes, f64 geometry/inverse mass/RK state",
-                      "accuracy": acc},
+                      "accuracy": acc,
+                      "tensor_core": {"what": "volume contractions on tcgen05 (kind::tf32, 3 TF32 products, "
+                                              "FP32 accumulation), one element per 128-thread CTA",
+                                      "ms_per_step": ms_tc / args.steps,
+                                      "value": replica_rate(world, dof_stage, 4, args.steps, ms_tc),
+                                      "speedup_vs_fp64": (ms / ms_tc), "stage_kernel_ms": stage_ms_tc,
+                                      "stage_vs_fp32x2_stage": stage_ms_tc / stage_ms_mixed}},
             "adjoint": adj,
             "config3": config3,
             "curved": curved,

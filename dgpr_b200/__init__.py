@@ -21,7 +21,7 @@ INTERIOR, PERIODIC, FREESTREAM, INVISCID_WALL, SUBSONIC_INFLOW, SUBSONIC_OUTFLOW
 ISOTHERMAL_WALL = -8  # an extension: no-slip wall at Solver.set_wall_temperature (default: params T)
 RK4, TVDRK3 = 0, 1
 FP64, MIXED_FP32 = 0, 1
-STEP_GAUSS, STEP_NODAL = 0, 1  # dgb_set_step_form
+STEP_GAUSS, STEP_NODAL, STEP_GAUSS_TC = 0, 1, 2  # dgb_set_step_form
 GEO_ELEMENT, GEO_VOLUME, GEO_FACE = 0, 1, 2  # dgb_get_geometry parts
 DPARAM_MU, DPARAM_SOURCE, DPARAM_TWALL, NDPARAMS = 0, 1, 6, 7  # dgb_backward_params: dJ/d[mu, source[0..4], Tw]
 

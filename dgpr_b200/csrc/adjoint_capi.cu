@@ -520,6 +520,7 @@ int dgb_forward_record(dgb_handle* h, int scheme, double dt, unsigned long long 
     CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   h->plan_pos = h->plan.first_reverse;
   h->recorded = true;
@@ -618,6 +619,7 @@ int dgb_forward_record_stages(dgb_handle* h, int scheme, double dt, unsigned lon
     CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   h->recorded = true;
   h->rec_stages = true;

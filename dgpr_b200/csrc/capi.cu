@@ -76,6 +76,14 @@ int enqueue_initial_traces(dgb_handle* h, bool gauss)
 // The last stage of a step in pieces of elements [bound[c], bound[c+1]),
 // with after(c) enqueued behind piece c (dgb_step_host copies each piece out
 // while the next one computes).
+// Odd stages of a Gauss-point step take the elements in descending order:
+// a stage then starts on the elements whose state, accumulator and traces the
+// stage before wrote last, which the L2 still holds.  The order changes no
+// result (every element's work is independent of it).
+#ifndef DGB_ALT_ORDER
+#define DGB_ALT_ORDER 1
+#endif
+
 struct LastStagePieces {
   int n = 0;
   const long* bound = nullptr;
@@ -102,6 +110,7 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     a.part = s == 0 ? h->d_part : nullptr;
     a.flag = h->d_flag;
     a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
+    a.rev = DGB_ALT_ORDER && gauss && (s & 1);
     const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
     if (pieces && gauss && s == nst - 1) {
@@ -538,8 +547,24 @@ int dgb_state_device_ptr(dgb_handle* h, double** U_dev)
 int dgb_set_step_form(dgb_handle* h, int form)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
-  if (form != DGB_STEP_GAUSS && form != DGB_STEP_NODAL) return fail(DGB_ERR_ARG, "unknown step form");
-  h->gauss_step = form == DGB_STEP_GAUSS;
+  if (form != DGB_STEP_GAUSS && form != DGB_STEP_NODAL && form != DGB_STEP_GAUSS_TC)
+    return fail(DGB_ERR_ARG, "unknown step form");
+  const bool tc = form == DGB_STEP_GAUSS_TC;
+  if (tc) {
+    if (h->precision != DGB_MIXED_FP32 || !tc_supported(h->P) || h->d_gv || h->dprm.kq != 0.)
+      return fail(DGB_ERR_UNSUPPORTED, "tensor-core stage: mixed precision, p = 3 or 4, affine, no heat flux only");
+    CK(cudaSetDevice(h->device));
+    CK(vprepare_tc(h->P));
+  }
+  if (tc != h->tc_step) {  // the captured graphs hold the other stage kernel
+    CK(cudaStreamSynchronize(h->stream));
+    drop_step_graphs(h);
+    if (h->rev_graph) cudaGraphExecDestroy(h->rev_graph);
+    h->rev_graph = nullptr;
+    h->rev_scheme = -1;
+  }
+  h->gauss_step = form != DGB_STEP_NODAL;
+  h->tc_step = tc;
   h->v_current = false;
   return DGB_OK;
 }
@@ -602,6 +627,7 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
     CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   return DGB_OK;
 }
@@ -693,6 +719,7 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaStreamSynchronize(h->copy_stream));
   if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
   if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   return DGB_OK;
 }

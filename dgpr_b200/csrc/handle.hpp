@@ -60,6 +60,7 @@ struct dgb_handle {
   };
   StepGraph graph, ggraph;
   bool gauss_step = true;    // dgb_step in the Gauss-point form (dgb_set_step_form)
+  bool tc_step = false;      // ... with tensor-core volume contractions (mixed precision)
   double* d_V = nullptr;     // Gauss-point values of the state during dgb_step
   // d_V holds the state that d_U is the nodal image of (set by dgb_step,
   // cleared by everything that writes d_U otherwise): consecutive dgb_step
@@ -119,6 +120,7 @@ inline KLaunch klaunch(const dgb_handle* h)
   L.gf = h->d_gf;
   L.nbr = h->d_nbr;
   L.prm = h->dprm;
+  L.tc = h->tc_step && h->precision == DGB_MIXED_FP32;
   return L;
 }
 

@@ -35,7 +35,24 @@ struct StageArgs {
   // both even for the paired kernel), so a stage can run in pieces whose
   // results are copied out while the next piece computes
   long e0, ecount;
+  // Gauss-point stage kernels only: 1 takes the elements in descending order,
+  // so a stage that follows an ascending one first reads what the L2 still
+  // holds of the previous stage's writes
+  int rev;
+  // set by the launcher from e0, ecount and rev (element_order): CTA b takes
+  // element (or, in the paired kernel, pair) ebase + estep * b
+  long ebase, estep;
 };
+
+// The CTA-to-element map of a Gauss-point stage launch over units of `unit`
+// elements (1, or 2 for the paired kernel).
+inline StageArgs element_order(StageArgs sa, long E, long unit)
+{
+  const long cnt = (sa.ecount ? sa.ecount : E) / unit, first = sa.e0 / unit;
+  sa.ebase = sa.rev ? first + cnt - 1 : first;
+  sa.estep = sa.rev ? -1 : 1;
+  return sa;
+}
 
 // everything the kernels read that does not change between stages
 struct KLaunch {
@@ -49,6 +66,7 @@ struct KLaunch {
   const double* gf;    // curved meshes: per-point face geometry [E][6][kFaceC][P^2], else null
   const int* nbr;      // [E][6]
   DevParams prm;
+  bool tc;             // mixed Gauss-point stages with tensor-core volume contractions
 };
 
 int ops_table_size(int P);
@@ -120,5 +138,10 @@ cudaError_t vprepare_fp32_heat(int P);
 cudaError_t vlaunch_trace_fp32_heat(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
 cudaError_t vlaunch_stage_fp32_heat(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                                     cudaStream_t st);
+// the mixed stage with tensor-core volume contractions (tc.cuh, vspace_tc.cu)
+bool tc_supported(int P);
+cudaError_t vprepare_tc(int P);
+cudaError_t vlaunch_stage_tc(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                             cudaStream_t st);
 
 }  // namespace dgb

@@ -58,9 +58,10 @@ struct VF {
 //   faces   Fa[FN][5][NQF] Fb[FN][12][NQF] Gt[FN][9][NQF]
 //   norm    Y0[5NB] Y1[5NB] (nodal residual for the printed norm), red[NTS] (FP64)
 //   traces  sN[FN][10][NQF], then the new state at oTrU
-template <int P, class T>
+template <int P, class T, int NTHREADS = Cfg<P>::NTS>
 struct VStageSmem {
   using C = Cfg<P>;
+  static constexpr int NT = NTHREADS;  // threads of the CTA (the norm reduction buffer)
   static constexpr int NB = C::NB, NQF = C::NQF;
   static constexpr int ST = (int)sizeof(T);
   static constexpr int oOps = 0;
@@ -69,7 +70,7 @@ struct VStageSmem {
   static constexpr int VOL = 20 * NB * ST;
   static constexpr int FACE = VF<P>::FN * (5 + 12 + 9) * NQF * ST;
   static constexpr int oRed = align16(10 * NB * ST);
-  static constexpr int NORM = oRed + C::NTS * 8;
+  static constexpr int NORM = oRed + NT * 8;
   static constexpr int oTrU = align16(10 * VF<P>::FN * NQF * ST);
   static constexpr int TRACE = oTrU + 5 * NB * ST;
   static constexpr int X0 = VOL > FACE ? VOL : FACE;
@@ -210,118 +211,73 @@ __device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, do
   return un;
 }
 
-// One RK stage on Gauss-point states: Vs (stage input), sa.Ubase / sa.acc /
-// sa.Uout are Gauss-point arrays, Tr the traces of Vs; sa.mode is an RK mode
-// (MODE_RESIDUAL writes f_V to sa.fout).  sa.part gets the element's sum of
-// the squared nodal residual, the reference's printed norm.
-template <int P, class T, bool CV, bool HT>
-__global__ void __launch_bounds__(Cfg<P>::NTS, (MinBlocks<P, T>::value))
-vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
-              const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
-              const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm, StageArgs sa)
+// The volume flux at Gauss point o (solve.cpp:276-341): from the state V1 and
+// the reference gradients G[3][5][NB] the contravariant flux
+// Ghat_i = w detJ (J^-T)_i . (F_visc - F_inv), passed to out(i, r, value);
+// returns w detJ at the point.  Affine elements take Ji / detJ, curved ones
+// the per-point record gve.
+template <int P, class T, bool CV, class Out>
+__device__ __forceinline__ T vpoint_flux(const T* so, const T* V1, const T* G, const T* Ji, T detJ,
+                                         const double* gve, T gamma, T mu, T kq, int o, Out out)
 {
   using C = Cfg<P>;
-  using L = VStageSmem<P, T>;
-  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* so = reinterpret_cast<T*>(smraw + L::oOps);
-  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
-  unsigned char* sXb = smraw + L::oX;
-  T* sX = reinterpret_cast<T*>(sXb);
-  const long e = blockIdx.x + sa.e0;
+  constexpr int NB = C::NB;
+  const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
+  const T* w = so + C::oW;
+  T wJq;
+  T Jbuf[9];
+  if constexpr (CV) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) Jbuf[c] = T(gve[c * NB + o]);
+    wJq = w[qx] * w[qy] * w[qz] * T(gve[kVolDetJ * NB + o]);
+  } else {
+    wJq = w[qx] * w[qy] * w[qz] * detJ;
+  }
+  const T* Jq = CV ? Jbuf : Ji;
+  T S[5], Gp[3][5], H[3][5];
+#pragma unroll
+  for (int r = 0; r < 5; ++r) {
+    S[r] = V1[r * NB + o];
+    const T g0 = G[r * NB + o], g1 = G[5 * NB + r * NB + o], g2 = G[10 * NB + r * NB + o];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Gp[c][r] = Jq[c] * g0 + Jq[3 + c] * g1 + Jq[6 + c] * g2;
+  }
+  euler_flux(S, gamma, H);
+  if (mu != T(0)) {
+    T Q[3][5];
+    visc_flux(S, Gp, mu, Q, kq);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int r = 0; r < 5; ++r) out(i, r, wJq * (Jq[3 * i] * H[0][r] + Jq[3 * i + 1] * H[1][r] + Jq[3 * i + 2] * H[2][r]));
+  return wJq;
+}
+
+// Face phase of the Gauss-point stage (solve.cpp:393-794): adds the face
+// terms of element e to Rv (Y = B3^-T R at Gauss point tid, node threads).
+// Scratch: sX, [FPP][5 + 12 + 9][NQF].  Any CTA size whose threads cover the
+// Gauss points.
+template <int P, class T, bool CV>
+__device__ __forceinline__ void vstage_faces(long e, const T* __restrict__ Tr, const int* __restrict__ nbr,
+                                             const T* so, const T* sg, T* sX, const double* __restrict__ geo,
+                                             const double* __restrict__ gf, const double* gfe, const DevParams& prm,
+                                             T gamma, T mu, T kq, T detJ, const T* Ji, int* flag, bool node, int qx,
+                                             int qy, int qz, T* Rv)
+{
+  using C = Cfg<P>;
+  constexpr int NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
   const int tid = threadIdx.x;
-  const bool node = tid < NB;  // thread owns Gauss point `tid`
-  const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
-
-  T* V1 = sX;
-  T* G = sX + 5 * NB;
-  if (DGB_PREFETCH_L2 && (sizeof(T) == 8 || DGB_PREFETCH_L2_F32)) {  // data read much later
-    const int nt = blockDim.x;
-    prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), tid, nt);
-    if (tid < 6) {
-      const int nb = nbr[e * 6 + tid];
-      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (tid ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
-    }
-    if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, tid, nt);
-    if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
-      prefetch_range(sa.acc + e * 5 * NB, 40L * NB, tid, nt);
-  }
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
-  const double* Ve = Vs + e * 5 * NB;
-  for (int i = tid; i < 5 * NB; i += blockDim.x) V1[i] = T(Ve[i]);
-  __syncthreads();
-
   const T* Dq = so + C::oDq;
-  const double detJd = geo[e * kGeoStride + kGeoDetJ];
-  const T detJ = sg[kGeoDetJ];
-  const T* Ji = sg + kGeoJinv;
-  const T gamma = T(prm.gamma), mu = T(prm.mu), kq = HT ? T(prm.kq) : T(0);
-  T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // Y = B3^-T R at Gauss point tid
-  const double* gve = CV ? gv + e * kVolC * NB : nullptr;
-  const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
-
-  // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
-  if (node) {  // reference gradients at the Gauss points
-    contract<P, 0, false, false>(Dq, V1, G, tid);
-    contract<P, 1, false, false>(Dq, V1, G + 5 * NB, tid);
-    contract<P, 2, false, false>(Dq, V1, G + 10 * NB, tid);
-  }
-  __syncthreads();
-  T wJq = T(0);
-  if (node) {  // pointwise flux at Gauss point tid
-    const T* w = so + C::oW;
-    T Jbuf[9];
-    if constexpr (CV) {
-#pragma unroll
-      for (int c = 0; c < 9; ++c) Jbuf[c] = T(gve[c * NB + tid]);
-      wJq = w[qx] * w[qy] * w[qz] * T(gve[kVolDetJ * NB + tid]);
-    } else {
-      wJq = w[qx] * w[qy] * w[qz] * detJ;
-    }
-    const T* Jq = CV ? Jbuf : Ji;
-    T S[5], Gp[3][5], H[3][5];
-#pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      S[r] = V1[r * NB + tid];
-      const T g0 = G[r * NB + tid], g1 = G[5 * NB + r * NB + tid], g2 = G[10 * NB + r * NB + tid];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) Gp[c][r] = Jq[c] * g0 + Jq[3 + c] * g1 + Jq[6 + c] * g2;
-    }
-    euler_flux(S, gamma, H);
-    if (mu != T(0)) {
-      T Q[3][5];
-      visc_flux(S, Gp, mu, Q, kq);
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int r = 0; r < 5; ++r)
-        G[i * 5 * NB + r * NB + tid] = wJq * (Jq[3 * i] * H[0][r] + Jq[3 * i + 1] * H[1][r] + Jq[3 * i + 2] * H[2][r]);
-  }
-  __syncthreads();
-  if (node) {  // Y = sum_i Dq_i^T Ghat_i, minus the source tested with w detJ
-    T y[5];
-    contract_reg<P, 0, true>(Dq, G, tid, Rv);
-    contract_reg<P, 1, true>(Dq, G + 5 * NB, tid, y);
-#pragma unroll
-    for (int r = 0; r < 5; ++r) Rv[r] += y[r];
-    contract_reg<P, 2, true>(Dq, G + 10 * NB, tid, y);
-#pragma unroll
-    for (int r = 0; r < 5; ++r) Rv[r] = Rv[r] + y[r] - T(prm.src[r]) * wJq;
-  }
-  __syncthreads();
-
-  // ---------------- faces (solve.cpp:393-794), FPP at a time
   T* Fa = sX;                    // [FPP][5][NQF]
   T* Fb = Fa + FPP * 5 * NQF;    // [FPP][12][NQF]
   T* Gt = Fb + FPP * 12 * NQF;   // [FPP][9][NQF]
@@ -333,7 +289,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
       T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
       const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
       face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
-                                  sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
+                                  flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
     __syncthreads();
 #pragma unroll 1
@@ -374,7 +330,22 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     }
     __syncthreads();
   }
+}
 
+// The end of the Gauss-point stage: the norm partial (the nodal residual
+// R = B3^T Y), f_V = -Y / (w detJ) in FP64 with the RK update, and the face
+// traces of the new state for the next stage.  L: the shared-memory layout
+// (VStageSmem), whose reduction buffer holds one FP64 per thread.
+template <int P, class T, bool CV, class L>
+__device__ __forceinline__ void vstage_finish(long e, const StageArgs& sa, const T* Rv, const double* Ve,
+                                              const double* gve, double detJd, unsigned char* sXb, const T* so,
+                                              const T* sg, const double* __restrict__ opsd, T mu, T kq,
+                                              const double* gfe, bool node, int qx, int qy, int qz)
+{
+  using C = Cfg<P>;
+  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN;
+  const int tid = threadIdx.x;
+  T* sX = reinterpret_cast<T*>(sXb);
   // ---------------- norm partial: the nodal residual R = B3^T Y
   if (sa.part) {
     const T* B = so + C::oB;
@@ -401,7 +372,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     __syncthreads();
     if (tid == 0) {
       double t = 0.;
-      for (int i = 0; i < C::NTS; ++i) t += red[i];
+      for (int i = 0; i < L::NT; ++i) t += red[i];
       sa.part[e] = t;
     }
     __syncthreads();
@@ -437,6 +408,86 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
       vtrace_half<P, T, CV>(half, sVn, sX, so, sg, mu, kq, Te, gfe);
     }
   }
+}
+
+// One RK stage on Gauss-point states: Vs (stage input), sa.Ubase / sa.acc /
+// sa.Uout are Gauss-point arrays, Tr the traces of Vs; sa.mode is an RK mode
+// (MODE_RESIDUAL writes f_V to sa.fout).  sa.part gets the element's sum of
+// the squared nodal residual, the reference's printed norm.
+template <int P, class T, bool CV, bool HT>
+__global__ void __launch_bounds__(Cfg<P>::NTS, (MinBlocks<P, T>::value))
+vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
+              const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
+              const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm, StageArgs sa)
+{
+  using C = Cfg<P>;
+  using L = VStageSmem<P, T>;
+  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw + L::oOps);
+  T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
+  unsigned char* sXb = smraw + L::oX;
+  T* sX = reinterpret_cast<T*>(sXb);
+  const long e = sa.ebase + sa.estep * (long)blockIdx.x;
+  const int tid = threadIdx.x;
+  const bool node = tid < NB;  // thread owns Gauss point `tid`
+  const int qx = tid % P, qy = (tid / P) % P, qz = tid / (P * P);
+
+  T* V1 = sX;
+  T* G = sX + 5 * NB;
+  if (DGB_PREFETCH_L2 && (sizeof(T) == 8 || DGB_PREFETCH_L2_F32)) {  // data read much later
+    const int nt = blockDim.x;
+    prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), tid, nt);
+    if (tid < 6) {
+      const int nb = nbr[e * 6 + tid];
+      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (tid ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
+    }
+    if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, tid, nt);
+    if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
+      prefetch_range(sa.acc + e * 5 * NB, 40L * NB, tid, nt);
+  }
+  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
+  const double* Ve = Vs + e * 5 * NB;
+  for (int i = tid; i < 5 * NB; i += blockDim.x) V1[i] = T(Ve[i]);
+  __syncthreads();
+
+  const T* Dq = so + C::oDq;
+  const double detJd = geo[e * kGeoStride + kGeoDetJ];
+  const T detJ = sg[kGeoDetJ];
+  const T* Ji = sg + kGeoJinv;
+  const T gamma = T(prm.gamma), mu = T(prm.mu), kq = HT ? T(prm.kq) : T(0);
+  T Rv[5] = {T(0), T(0), T(0), T(0), T(0)};  // Y = B3^-T R at Gauss point tid
+  const double* gve = CV ? gv + e * kVolC * NB : nullptr;
+  const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
+
+  // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
+  if (node) {  // reference gradients at the Gauss points
+    contract<P, 0, false, false>(Dq, V1, G, tid);
+    contract<P, 1, false, false>(Dq, V1, G + 5 * NB, tid);
+    contract<P, 2, false, false>(Dq, V1, G + 10 * NB, tid);
+  }
+  __syncthreads();
+  T wJq = T(0);
+  if (node)  // pointwise flux at Gauss point tid
+    wJq = vpoint_flux<P, T, CV>(so, V1, G, Ji, detJ, gve, gamma, mu, kq, tid,
+                                [&](int i, int r, T v) { G[i * 5 * NB + r * NB + tid] = v; });
+  __syncthreads();
+  if (node) {  // Y = sum_i Dq_i^T Ghat_i, minus the source tested with w detJ
+    T y[5];
+    contract_reg<P, 0, true>(Dq, G, tid, Rv);
+    contract_reg<P, 1, true>(Dq, G + 5 * NB, tid, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Rv[r] += y[r];
+    contract_reg<P, 2, true>(Dq, G + 10 * NB, tid, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Rv[r] = Rv[r] + y[r] - T(prm.src[r]) * wJq;
+  }
+  __syncthreads();
+
+  vstage_faces<P, T, CV>(e, Tr, nbr, so, sg, sX, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag, node, qx, qy,
+                         qz, Rv);
+  vstage_finish<P, T, CV, L>(e, sa, Rv, Ve, gve, detJd, sXb, so, sg, opsd, mu, kq, gfe, node, qx, qy, qz);
 }
 
 // The basis changes at the edges of the Gauss-point form, per element, FP64
@@ -599,7 +650,7 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
   float* sgf = reinterpret_cast<float*>(smraw + LP::oGeoF);  // [2][kGeoStride]
   unsigned char* sXb = smraw + L::oX;
   T* sX = reinterpret_cast<T*>(sXb);
-  const long k = blockIdx.x + sa.e0 / 2, e0 = 2 * k;
+  const long k = sa.ebase + sa.estep * (long)blockIdx.x, e0 = 2 * k;
   const long el[2] = {e0, e0 + 1};
   const int tid = threadIdx.x;
   const bool node = tid < NB;
@@ -864,13 +915,13 @@ cudaError_t vlaunch_stage2_p(const KLaunch& L, const double* Vs, const void* Tin
 {
   vstage2_kernel<P, HT><<<(unsigned)((sa.ecount ? sa.ecount : L.E) / 2), Cfg<P>::NTS, VPairSmem<P>::TOTAL, st>>>(
       L.E, Vs, reinterpret_cast<const f2*>(Tin), reinterpret_cast<const float*>(L.ops), L.opsd, L.geo, L.nbr,
-      L.prm, sa);
+      L.prm, element_order(sa, L.E, 2));
   return cudaGetLastError();
 }
 
 // the paired form serves an FP32 launch on an affine mesh with an even
 // element count; everything else takes the one-element kernels
-inline bool use_pair(const KLaunch& L) { return L.E % 2 == 0 && !L.gv; }
+inline bool use_pair(const KLaunch& L) { return L.E % 2 == 0 && !L.gv && !L.tc; }
 
 template <bool HT>
 cudaError_t vprepare2_t(int P)
@@ -956,14 +1007,15 @@ cudaError_t vlaunch_stage_p(const KLaunch& L, const double* Vs, const void* Tin,
                             cudaStream_t st)
 {
   const unsigned grid = (unsigned)(sa.ecount ? sa.ecount : L.E);
+  const StageArgs so = element_order(sa, L.E, 1);
   if (L.gv)
     vstage_kernel<P, T, true, HT><<<grid, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
         L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
-        L.nbr, L.prm, sa);
+        L.nbr, L.prm, so);
   else
     vstage_kernel<P, T, false, HT><<<grid, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
         L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
-        nullptr, L.nbr, L.prm, sa);
+        nullptr, L.nbr, L.prm, so);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@ cudaError_t vlaunch_trace_fp32(const KLaunch& L, const double* V, void* Tout, cu
 cudaError_t vlaunch_stage_fp32(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                                cudaStream_t st)
 {
+  if (L.tc) return vlaunch_stage_tc(L, Vs, Tin, sa, st);
   if (L.prm.kq != 0.) return vlaunch_stage_fp32_heat(L, Vs, Tin, sa, st);
   return use_pair(L) ? vlaunch_stage2_t<false>(L, Vs, Tin, sa, st) : vlaunch_stage_t<float, false>(L, Vs, Tin, sa, st);
 }

@@ -201,8 +201,13 @@ int dgb_state_device_ptr(dgb_handle* h, double** U_dev);
  * discretisation; they agree to rounding.  The recorded runs of the adjoint
  * (dgb_forward_record*) step in the same form as dgb_step, and the backward
  * sweep reverses that form; its adjoint vectors enter and leave in the nodal
- * layout. */
-enum { DGB_STEP_GAUSS = 0, DGB_STEP_NODAL = 1 };
+ * layout.  DGB_STEP_GAUSS_TC is the Gauss-point form whose mixed-precision
+ * stage does its volume contractions on the tensor cores (three TF32
+ * products per term, FP32 accumulation); it takes mixed-precision handles
+ * with p = 3 or 4, affine elements and no heat flux (else
+ * DGB_ERR_UNSUPPORTED), and is slower than the default FP32x2 stage: it is
+ * kept as the measured alternative. */
+enum { DGB_STEP_GAUSS = 0, DGB_STEP_NODAL = 1, DGB_STEP_GAUSS_TC = 2 };
 int dgb_set_step_form(dgb_handle* h, int form);
 
 /* One residual evaluation of U: R = un-inverted residual (may be NULL) and
