@@ -13,7 +13,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr"]
 SOURCES = ["host.cpp", "io.cpp", "checkpoint.cpp", "capi.cu", "kernels_fp64.cu", "kernels_fp32.cu",
            "kernels_heat_fp64.cu", "kernels_heat_fp32.cu", "vspace_fp64.cu", "vspace_fp32.cu", "vspace_heat_fp64.cu",
-           "vspace_heat_fp32.cu", "vspace_tc.cu", "noalloc.cu", "check.cu", "adjoint.cu", "adjoint_heat.cu", "adjoint_gauss.cu",
+           "vspace_heat_fp32.cu", "vspace_tc.cu", "vspace_visc.cu", "noalloc.cu", "check.cu", "adjoint.cu", "adjoint_heat.cu", "adjoint_gauss.cu",
            "adjoint_gauss_heat.cu", "adjoint_capi.cu", "geometry.cu"]
 
 

@@ -63,7 +63,8 @@ VjpArgs vjp(const double* U, double cx, const double* X, double cy = 0., const d
 }
 
 // ---- parameter gradient (dgb_backward_params)
-// Per element e: part[e][0] = sum W . (F1 - F0) * inv_mu1 and
+// Per element e: part[e][0] = sum W . (F1 - F0) * inv_mu1 (F1 alone when F0
+// is null) and
 // part[e][1 + r] = sum_b W[r][b], with W = cx X + cy Y + cz Z the adjoint
 // weight of one residual VJP; fixed-order block sums.
 __global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __restrict__ F1,
@@ -78,7 +79,7 @@ __global__ void param_dot_kernel(long E, int nb, VjpArgs v, const double* __rest
     double w = v.cx * v.X[g];
     if (v.Y) w = fma(v.cy, v.Y[g], w);
     if (v.Z) w = fma(v.cz, v.Z[g], w);
-    acc[0] = fma(w, (F1[g] - F0[g]) * inv_mu1, acc[0]);
+    acc[0] = fma(w, (F0 ? F1[g] - F0[g] : F1[g]) * inv_mu1, acc[0]);
     acc[1 + i / nb] += w;
   }
   for (int k = 0; k < DGB_NDPARAMS; ++k) red[k][tid] = acc[k];
@@ -148,7 +149,9 @@ int ensure_pgrad(dgb_handle* h)
 // W^T df/dtheta for one residual VJP v (before it runs: it may overwrite
 // v.Y in place), added into dpar.  f is affine in mu (the viscous flux and
 // the heat flux at fixed Pr are linear in it), so df/dmu = (f(mu1) - f(0)) /
-// mu1, both FP64 residuals of v.U; df/dsource[r] = 1 on variable r.
+// mu1, both FP64 residuals of v.U, in the nodal form; the Gauss-point form
+// evaluates the viscous terms alone at mu1 (vlaunch_stage_visc), f(mu1) - f(0)
+// in one residual.  df/dsource[r] = 1 on variable r.
 int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar, bool gauss)
 {
   KLaunch L = klaunch(h);
@@ -167,16 +170,24 @@ int enqueue_param_terms(dgb_handle* h, const VjpArgs& v, double* dpar, bool gaus
   double* F0 = F1 + h->n;
   double* trp = F0 + h->n;
   double* part = trp + (size_t)h->E * 60 * h->NQF;
-  const KLaunch* Ls[2] = {&L1, &L0};
-  double* Fs[2] = {F1, F0};
-  for (int k = 0; k < 2; ++k) {  // f (or f_V in the Gauss-point form: df_V/dsource is 1 as well)
+  if (gauss) {  // f_V's viscous terms alone at mu1, without the source: mu1 df_V/dmu in one residual
+    KLaunch Lv = L1;
+    for (int r = 0; r < 5; ++r) Lv.prm.src[r] = 0.;
     StageArgs a = stage_args(MODE_RESIDUAL, 0.);
-    a.fout = Fs[k];
+    a.fout = F1;
     a.flag = h->d_flag;
-    if (gauss) {
-      CK(launch_vtrace(*Ls[k], v.U, trp, h->stream));
-      CK(launch_vstage(*Ls[k], v.U, trp, a, h->stream));
-    } else {
+    // the VJP's FP64 traces of v.U are these traces when mu1 is the handle's mu
+    const double* tr = v.Tr && h->dprm.mu != 0. ? v.Tr : trp;
+    if (tr == trp) CK(launch_vtrace(Lv, v.U, trp, h->stream));
+    CK(vlaunch_stage_visc(Lv, v.U, tr, a, h->stream));
+    F0 = nullptr;
+  } else {
+    const KLaunch* Ls[2] = {&L1, &L0};
+    double* Fs[2] = {F1, F0};
+    for (int k = 0; k < 2; ++k) {  // f(mu1) and f(0)
+      StageArgs a = stage_args(MODE_RESIDUAL, 0.);
+      a.fout = Fs[k];
+      a.flag = h->d_flag;
       CK(launch_trace(*Ls[k], v.U, trp, h->stream));
       CK(launch_stage(*Ls[k], v.U, trp, a, h->stream));
     }
@@ -260,10 +271,18 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
   auto vjp_launch = [&](const VjpArgs& w) {
     return gauss ? launch_residual_vjp_gauss(L, w, sc, h->stream) : launch_residual_vjp(L, w, sc, h->stream);
   };
-  auto run_vjp = [&](const VjpArgs& w) -> int {
+  auto run_vjp = [&](const VjpArgs& w0) -> int {
     if (!dpar) {
-      CK(vjp_launch(w));
+      CK(vjp_launch(w0));
       return DGB_OK;
+    }
+    VjpArgs w = w0;
+    if (gauss && h->dprm.mu != 0. && !w.Tr) {  // one set of FP64 traces for the parameter terms and the VJP
+      KLaunch L64 = klaunch(h);
+      L64.precision = DGB_FP64;
+      L64.ops = L64.opsd;
+      CK(launch_vtrace(L64, w.U, sc.trace, h->stream));
+      w.Tr = sc.trace;
     }
     const int r = enqueue_param_terms(h, w, dpar, gauss);
     if (r) return r;

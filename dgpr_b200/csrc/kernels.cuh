@@ -409,10 +409,12 @@ trace_kernel(long E, const double* __restrict__ U, const T* __restrict__ opsg, c
 // fb[(i * 4 + r - 1) * OS] = the dual-consistency coefficient of
 // d(phi)/d(xi_i) for variables 1..4.  Uo, Qo: the element's trace (values,
 // viscous normal flux) at the point; nb = nbr[e][lf]; for nb >= 0 also the
-// neighbour's (Un, Qn) and its lifting scale lift_n.  Shared by the nodal,
+// neighbour's (Un, Qn) and its lifting scale lift_n.  VO: the viscous terms
+// alone (no Roe or boundary Euler flux), for the derivative of the residual
+// in the viscosity, in which it is linear.  Shared by the nodal,
 // the Gauss-point and the paired Gauss-point stage kernels, so their face
 // arithmetic is the same; a pair (T = f2) takes interior faces only.
-template <int P, class T, bool CV, int OS = P * P>
+template <int P, class T, bool CV, int OS = P * P, bool VO = false>
 __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const T* Uo, const T* Qo, const T* Un,
                                                   const T* Qn, T lift_n, const T* so, const T* sg,
                                                   const double* __restrict__ gfe, const DevParams& prm, T gamma,
@@ -444,7 +446,8 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
       // the face on its high side is "left"; the other side negates it
       T F[5];
       const T sgn = end ? T(1) : T(-1);
-      if constexpr (!std::is_same<T, double>::value) {  // FP32 and pairs measured better with the copies
+      if constexpr (VO) {  // no inviscid flux
+      } else if constexpr (!std::is_same<T, double>::value) {  // FP32 and pairs measured better with the copies
         T UL[5], UR[5];
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
@@ -457,7 +460,7 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
         roe_flux_oriented(Uo, Un, end, n, gamma, F);
       }
 #pragma unroll
-      for (int r = 0; r < 5; ++r) fa[r * OS] = sgn * F[r] - qd[r];
+      for (int r = 0; r < 5; ++r) fa[r * OS] = VO ? -qd[r] : sgn * F[r] - qd[r];
     }
     if (mu != T(0)) {
       T d[5];
@@ -486,7 +489,10 @@ __device__ __forceinline__ void face_point_fluxes(int lf, int fq, int nb, const 
     T Ub[5];
     const int bad = boundary_state(nb, Uo, n, prm, Ub);
     if (bad && flag) atomicOr(flag, 2);
-    {
+    if constexpr (VO) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r) fa[r * OS] = -Qo[r];
+    } else {
       T F[5];
       euler_flux_n(Ub, gamma, n, F);
 #pragma unroll

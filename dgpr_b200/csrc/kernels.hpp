@@ -138,6 +138,9 @@ cudaError_t vprepare_fp32_heat(int P);
 cudaError_t vlaunch_trace_fp32_heat(const KLaunch& L, const double* V, void* Tout, cudaStream_t st);
 cudaError_t vlaunch_stage_fp32_heat(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                                     cudaStream_t st);
+// the viscous terms alone of the FP64 Gauss-point residual (vspace_visc.cu)
+cudaError_t vlaunch_stage_visc(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
+                               cudaStream_t st);
 // the mixed stage with tensor-core volume contractions (tc.cuh, vspace_tc.cu)
 bool tc_supported(int P);
 cudaError_t vprepare_tc(int P);

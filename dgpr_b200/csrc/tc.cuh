@@ -327,7 +327,7 @@ vstage_tc_kernel(long E, const double* Vs, const float* __restrict__ Tr, const f
   const T gamma = T(prm.gamma), mu = T(prm.mu), kq = T(0);
   T wJq = T(0);
   if (node)
-    wJq = vpoint_flux<P, T, false>(so, V1, G, Ji, detJ, nullptr, gamma, mu, kq, tid, [&](int i, int r, T v) {
+    wJq = vpoint_flux<P, T, false, false>(so, V1, G, Ji, detJ, nullptr, gamma, mu, kq, tid, [&](int i, int r, T v) {
       int mm, k;
       tc::row_of<P>(i, r, tid, mm, k);
       const int off = tc::kmajor_off(mm, k, TL::CHUNK);

@@ -215,8 +215,8 @@ __device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, do
 // the reference gradients G[3][5][NB] the contravariant flux
 // Ghat_i = w detJ (J^-T)_i . (F_visc - F_inv), passed to out(i, r, value);
 // returns w detJ at the point.  Affine elements take Ji / detJ, curved ones
-// the per-point record gve.
-template <int P, class T, bool CV, class Out>
+// the per-point record gve.  VO: the viscous flux alone.
+template <int P, class T, bool CV, bool VO, class Out>
 __device__ __forceinline__ T vpoint_flux(const T* so, const T* V1, const T* G, const T* Ji, T detJ,
                                          const double* gve, T gamma, T mu, T kq, int o, Out out)
 {
@@ -242,19 +242,23 @@ __device__ __forceinline__ T vpoint_flux(const T* so, const T* V1, const T* G, c
 #pragma unroll
     for (int c = 0; c < 3; ++c) Gp[c][r] = Jq[c] * g0 + Jq[3 + c] * g1 + Jq[6 + c] * g2;
   }
-  euler_flux(S, gamma, H);
-  if (mu != T(0)) {
-    T Q[3][5];
-    visc_flux(S, Gp, mu, Q, kq);
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
+  if constexpr (VO) {
+    visc_flux(S, Gp, mu, H, kq);
   } else {
+    euler_flux(S, gamma, H);
+    if (mu != T(0)) {
+      T Q[3][5];
+      visc_flux(S, Gp, mu, Q, kq);
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+      for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
+        for (int r = 0; r < 5; ++r) H[c][r] = Q[c][r] - H[c][r];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) H[c][r] = -H[c][r];
+    }
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -267,7 +271,7 @@ __device__ __forceinline__ T vpoint_flux(const T* so, const T* V1, const T* G, c
 // terms of element e to Rv (Y = B3^-T R at Gauss point tid, node threads).
 // Scratch: sX, [FPP][5 + 12 + 9][NQF].  Any CTA size whose threads cover the
 // Gauss points.
-template <int P, class T, bool CV>
+template <int P, class T, bool CV, bool VO = false>
 __device__ __forceinline__ void vstage_faces(long e, const T* __restrict__ Tr, const int* __restrict__ nbr,
                                              const T* so, const T* sg, T* sX, const double* __restrict__ geo,
                                              const double* __restrict__ gf, const double* gfe, const DevParams& prm,
@@ -288,8 +292,8 @@ __device__ __forceinline__ void vstage_faces(long e, const T* __restrict__ Tr, c
       const int j = i / NQF, lf = FPP * half + j, fq = i % NQF;
       T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
       const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
-      face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
-                                  flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
+      face_point_fluxes<P, T, CV, P * P, VO>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq,
+                                             detJ, Ji, flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
     __syncthreads();
 #pragma unroll 1
@@ -413,8 +417,10 @@ __device__ __forceinline__ void vstage_finish(long e, const StageArgs& sa, const
 // One RK stage on Gauss-point states: Vs (stage input), sa.Ubase / sa.acc /
 // sa.Uout are Gauss-point arrays, Tr the traces of Vs; sa.mode is an RK mode
 // (MODE_RESIDUAL writes f_V to sa.fout).  sa.part gets the element's sum of
-// the squared nodal residual, the reference's printed norm.
-template <int P, class T, bool CV, bool HT>
+// the squared nodal residual, the reference's printed norm.  VO: the viscous
+// terms alone (MODE_RESIDUAL with the source zeroed: df_V/dmu times mu, the
+// residual being linear in mu), for the parameter gradients.
+template <int P, class T, bool CV, bool HT, bool VO = false>
 __global__ void __launch_bounds__(Cfg<P>::NTS, (MinBlocks<P, T>::value))
 vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
               const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
@@ -470,7 +476,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   __syncthreads();
   T wJq = T(0);
   if (node)  // pointwise flux at Gauss point tid
-    wJq = vpoint_flux<P, T, CV>(so, V1, G, Ji, detJ, gve, gamma, mu, kq, tid,
+    wJq = vpoint_flux<P, T, CV, VO>(so, V1, G, Ji, detJ, gve, gamma, mu, kq, tid,
                                 [&](int i, int r, T v) { G[i * 5 * NB + r * NB + tid] = v; });
   __syncthreads();
   if (node) {  // Y = sum_i Dq_i^T Ghat_i, minus the source tested with w detJ
@@ -485,8 +491,8 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   }
   __syncthreads();
 
-  vstage_faces<P, T, CV>(e, Tr, nbr, so, sg, sX, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag, node, qx, qy,
-                         qz, Rv);
+  vstage_faces<P, T, CV, VO>(e, Tr, nbr, so, sg, sX, geo, gf, gfe, prm, gamma, mu, kq, detJ, Ji, sa.flag, node, qx,
+                             qy, qz, Rv);
   vstage_finish<P, T, CV, L>(e, sa, Rv, Ve, gve, detJd, sXb, so, sg, opsd, mu, kq, gfe, node, qx, qy, qz);
 }
 

@@ -65,3 +65,21 @@ def test_tc_form_rejected_where_not_built():
     with solver(c2, dg.MIXED_FP32) as s:
         with pytest.raises(dg.DgbError):
             s.set_step_form(dg.STEP_GAUSS_TC)
+
+
+@pytest.mark.parametrize("n", [4, 3], ids=["even", "odd"])
+def test_tc_step_host_equals_set_step_get(n):
+    """dgb_step_host runs the tensor-core stage in pieces of elements (its
+    last stage): the same bits as the plain calls."""
+    c, dt = _tgv(n, 3)
+    with solver(c, dg.MIXED_FP32) as s:
+        s.set_step_form(dg.STEP_GAUSS_TC)
+        s.set_state(c.U)
+        norms_a = s.step(dg.RK4, dt, 2)
+        Ua = s.get_state()
+    with solver(c, dg.MIXED_FP32) as s:
+        s.set_step_form(dg.STEP_GAUSS_TC)
+        Uout = np.zeros(c.U.size)
+        norms_b = s.step_host(dg.RK4, dt, 2, np.array(c.U, dtype=np.float64), Uout)
+    assert np.array_equal(Uout, Ua)
+    assert np.array_equal(norms_b, norms_a[:2])
