@@ -351,7 +351,10 @@ int ensure_rev_graph(dgb_handle* h, int scheme, double dt, bool gauss)
   int rc = enqueue_reverse_step(h, scheme, dt, gauss ? h->d_V : h->d_U, h->d_adj[dgb_handle::ADJ_LAM], &nl,
                                 nullptr, nullptr, gauss);
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-  if (rc) return rc;
+  if (rc) {
+    if (ce == cudaSuccess) cudaGraphDestroy(g);
+    return rc;
+  }
   if (ce != cudaSuccess) return cuda_status(ce, "cudaStreamEndCapture");
   ce = cudaGraphInstantiate(&h->rev_graph, g, 0);
   cudaGraphDestroy(g);

@@ -182,6 +182,8 @@ namespace {
 int replace_device_params(dgb_handle* h, const DevParams& d)
 {
   if (!std::memcmp(&d, &h->dprm, sizeof d)) return DGB_OK;
+  if (h->tc_step && d.kq != 0.)
+    return fail(DGB_ERR_UNSUPPORTED, "the tensor-core step form has no heat flux: select another form first");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   h->dprm = d;
@@ -224,7 +226,10 @@ int dgb::ensure_step_graph(dgb_handle* h, int scheme, double dt, unsigned long l
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int rc = enqueue_step(h, scheme, dt, nullptr, gauss);
   cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-  if (rc) return rc;
+  if (rc) {
+    if (ce == cudaSuccess) cudaGraphDestroy(g);
+    return rc;
+  }
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
   ce = cudaGraphInstantiate(&sg.exec, g, 0);
   cudaGraphDestroy(g);

@@ -557,6 +557,42 @@ __device__ __forceinline__ int load_face_point(long e, int lf, int fq, const T* 
   return nb;
 }
 
+// The RK stage value of one entry (time_distributed.cpp:46-102, stage 3 of
+// RK4 with dt as the reference's CPU solver): updates the accumulator and
+// returns the new stage state.  ue: the stage input state at this entry.
+__device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, double fr, double ue)
+{
+  const double dt = sa.dt;
+  double un = 0.;
+  switch (sa.mode) {
+    case MODE_RK4_0:
+      sa.acc[i] = fr;
+      un = sa.Ubase[i] + dt * fr * 0.5;
+      break;
+    case MODE_RK4_1:
+      sa.acc[i] = sa.acc[i] + 2. * fr;
+      un = sa.Ubase[i] + dt * fr * 0.5;
+      break;
+    case MODE_RK4_2:
+      sa.acc[i] = sa.acc[i] + 2. * fr;
+      un = sa.Ubase[i] + dt * fr;
+      break;
+    case MODE_RK4_3:
+      un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
+      break;
+    case MODE_TVD_0:
+      un = sa.Ubase[i] + dt * fr;
+      break;
+    case MODE_TVD_1:
+      un = 0.75 * sa.Ubase[i] + 0.25 * ue + 0.25 * dt * fr;
+      break;
+    case MODE_TVD_2:
+      un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * ue + (2. / 3.) * dt * fr;
+      break;
+  }
+  return un;
+}
+
 // ------------------------------------------------------------- stage kernel
 //
 // Shared memory: [operators (T) | inverse 1D mass matrix (FP64) | element
@@ -895,43 +931,15 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     }
     const double sc = CV ? -1.0 : -1.0 / detJd;
     const long base = e * 5 * NB;
-    const double dt = sa.dt;
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       const long i = base + r * NB + tid;
       const double fr = f[r] * sc;
-      double un = 0.;
-      switch (sa.mode) {
-        case MODE_RESIDUAL:
-          sa.fout[i] = fr;
-          if (sa.Rout) sa.Rout[i] = double(Rv[r]);
-          break;
-        case MODE_RK4_0:
-          sa.acc[i] = fr;
-          un = sa.Ubase[i] + dt * fr * 0.5;
-          break;
-        case MODE_RK4_1:
-          sa.acc[i] = sa.acc[i] + 2. * fr;
-          un = sa.Ubase[i] + dt * fr * 0.5;
-          break;
-        case MODE_RK4_2:
-          sa.acc[i] = sa.acc[i] + 2. * fr;
-          un = sa.Ubase[i] + dt * fr;
-          break;
-        case MODE_RK4_3:
-          un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
-          break;
-        case MODE_TVD_0:
-          un = sa.Ubase[i] + dt * fr;
-          break;
-        case MODE_TVD_1:
-          un = 0.75 * sa.Ubase[i] + 0.25 * Ue[r * NB + tid] + 0.25 * dt * fr;
-          break;
-        case MODE_TVD_2:
-          un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * Ue[r * NB + tid] + (2. / 3.) * dt * fr;
-          break;
-      }
-      if (sa.mode != MODE_RESIDUAL) {
+      if (sa.mode == MODE_RESIDUAL) {
+        sa.fout[i] = fr;
+        if (sa.Rout) sa.Rout[i] = double(Rv[r]);
+      } else {
+        const double un = rk_stage_value(sa, i, fr, Ue[r * NB + tid]);
         sa.Uout[i] = un;
         sUn[r * NB + tid] = T(un);
       }

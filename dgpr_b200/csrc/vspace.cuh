@@ -175,41 +175,6 @@ vtrace_kernel(long E, const double* __restrict__ V, const T* __restrict__ opsg, 
   }
 }
 
-// The RK stage value of one entry (time_distributed.cpp:46-102, stage 3 of
-// RK4 with dt as the reference's CPU solver): updates the accumulator and
-// returns the new stage state.  ue: the stage input state at this entry.
-__device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, double fr, double ue)
-{
-  const double dt = sa.dt;
-  double un = 0.;
-  switch (sa.mode) {
-    case MODE_RK4_0:
-      sa.acc[i] = fr;
-      un = sa.Ubase[i] + dt * fr * 0.5;
-      break;
-    case MODE_RK4_1:
-      sa.acc[i] = sa.acc[i] + 2. * fr;
-      un = sa.Ubase[i] + dt * fr * 0.5;
-      break;
-    case MODE_RK4_2:
-      sa.acc[i] = sa.acc[i] + 2. * fr;
-      un = sa.Ubase[i] + dt * fr;
-      break;
-    case MODE_RK4_3:
-      un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
-      break;
-    case MODE_TVD_0:
-      un = sa.Ubase[i] + dt * fr;
-      break;
-    case MODE_TVD_1:
-      un = 0.75 * sa.Ubase[i] + 0.25 * ue + 0.25 * dt * fr;
-      break;
-    case MODE_TVD_2:
-      un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * ue + (2. / 3.) * dt * fr;
-      break;
-  }
-  return un;
-}
 
 // The volume flux at Gauss point o (solve.cpp:276-341): from the state V1 and
 // the reference gradients G[3][5][NB] the contravariant flux

@@ -65,6 +65,13 @@ def test_tc_form_rejected_where_not_built():
     with solver(c2, dg.MIXED_FP32) as s:
         with pytest.raises(dg.DgbError):
             s.set_step_form(dg.STEP_GAUSS_TC)
+    with solver(c, dg.MIXED_FP32) as s:  # the heat flux cannot be switched on under the form
+        s.set_step_form(dg.STEP_GAUSS_TC)
+        with pytest.raises(dg.DgbError) as ex:
+            s.set_prandtl(0.71)
+        assert ex.value.code == dg.ERR_UNSUPPORTED
+        s.set_step_form(dg.STEP_GAUSS)
+        s.set_prandtl(0.71)
 
 
 @pytest.mark.parametrize("n", [4, 3], ids=["even", "odd"])
