@@ -73,9 +73,28 @@ int enqueue_initial_traces(dgb_handle* h, bool gauss)
 // With ev != null, ev[i] is recorded before launch i and ev[nlaunch] after the
 // last one (per-kernel timing by dgb_profile_step).  gauss: the Gauss-point
 // form on d_V (vspace.cuh), else the nodal form on d_U.
-// The last stage of a step in pieces of elements [bound[c], bound[c+1]),
-// with after(c) enqueued behind piece c (dgb_step_host copies each piece out
-// while the next one computes).
+// Pieces of the elements, [bound[c], bound[c+1]) (dgb_step_host): a step may
+// run its first stage, or its last two, piece by piece so that host copies
+// overlap the work.  deps[c] has bit c' set when an element of piece c has a
+// neighbour in piece c' (bit c always); a stage's piece reads the previous
+// stage's traces of exactly those pieces.
+//   in(c)   enqueues what piece c's first-stage input needs (its copy in, its
+//           basis change and traces); piece k of the first stage runs as soon
+//           as in() has been enqueued for every piece in deps[k]
+//   out(c)  is enqueued behind piece c of the last stage; the last two stages
+//           run interleaved, piece k of the last one as soon as the one
+//           before has run every piece in deps[k]
+// The neighbour relation is symmetric, so a last-stage piece also runs only
+// after every piece of the stage before that reads its traces: the trace
+// buffer the last stage writes may be the one the stage before reads
+// (RK4: T0), and no piece reads a trace after it was overwritten.
+struct StepPieces {
+  int n = 0;
+  const long* bound = nullptr;
+  const unsigned* deps = nullptr;
+  std::function<int(int)> in;   // set: the first stage in pieces
+  std::function<int(int)> out;  // set: the last two stages in pieces
+};
 // Odd stages of a Gauss-point step take the elements in descending order:
 // a stage then starts on the elements whose state, accumulator and traces the
 // stage before wrote last, which the L2 still holds.  The order changes no
@@ -84,14 +103,8 @@ int enqueue_initial_traces(dgb_handle* h, bool gauss)
 #define DGB_ALT_ORDER 1
 #endif
 
-struct LastStagePieces {
-  int n = 0;
-  const long* bound = nullptr;
-  std::function<int(int)> after;
-};
-
 int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr, bool gauss = false,
-                 const LastStagePieces* pieces = nullptr)
+                 const StepPieces* pieces = nullptr, long long* nl = nullptr)
 {
   double* Ures = gauss ? h->d_V : h->d_U;
   const KLaunch L = klaunch(h);
@@ -100,9 +113,8 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
   const int modes3[3] = {MODE_TVD_0, MODE_TVD_1, MODE_TVD_2};
   const int tin4[4] = {0, 1, 0, 1}, tout4[4] = {1, 0, 1, 0};
   const int tin3[3] = {0, 1, 2}, tout3[3] = {1, 2, 0};
-  int k = 0;
-  for (int s = 0; s < nst; ++s) {
-    const double* in = s == 0 ? Ures : h->d_Us;
+  long long launched = 0;
+  auto args = [&](int s) {
     StageArgs a = stage_args(scheme == DGB_RK4 ? modes4[s] : modes3[s], dt);
     a.Ubase = Ures;
     a.acc = h->d_acc;
@@ -111,29 +123,63 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     a.flag = h->d_flag;
     a.Tnext = h->d_trace[scheme == DGB_RK4 ? tout4[s] : tout3[s]];
     a.rev = DGB_ALT_ORDER && gauss && (s & 1);
-    const void* tin = h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]];
+    return a;
+  };
+  auto stage_in = [&](int s) -> const double* { return s == 0 ? Ures : h->d_Us; };
+  auto stage_tin = [&](int s) -> const void* { return h->d_trace[scheme == DGB_RK4 ? tin4[s] : tin3[s]]; };
+  auto piece_launch = [&](int s, StageArgs a, int c) -> cudaError_t {  // piece c of stage s (none if empty)
+    if (pieces->bound[c + 1] == pieces->bound[c]) return cudaSuccess;  // (an ecount of 0 would mean all elements)
+    a.e0 = pieces->bound[c];
+    a.ecount = pieces->bound[c + 1] - pieces->bound[c];
+    ++launched;
+    return launch_vstage(L, stage_in(s), stage_tin(s), a, h->stream);
+  };
+  const bool pieced = pieces && gauss;
+  int k = 0;
+  for (int s = 0; s < nst; ++s) {
+    const StageArgs a = args(s);
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
-    if (pieces && gauss && s == nst - 1) {
+    if (pieced && pieces->in && s == 0) {
+      unsigned have = 0, done = 0;
       for (int c = 0; c < pieces->n; ++c) {
-        if (pieces->bound[c + 1] == pieces->bound[c]) continue;  // (an ecount of 0 would mean all elements)
-        a.e0 = pieces->bound[c];
-        a.ecount = pieces->bound[c + 1] - pieces->bound[c];
-        CK(launch_vstage(L, in, tin, a, h->stream));
-        const int rc = pieces->after(c);
-        if (rc) return rc;
+        if (const int rc = pieces->in(c)) return rc;
+        have |= 1u << c;
+        for (int q = 0; q < pieces->n; ++q) {
+          if (((done >> q) & 1) || (pieces->deps[q] & ~have)) continue;
+          done |= 1u << q;
+          CK(piece_launch(s, a, q));
+        }
       }
-    } else if (gauss) {
-      CK(launch_vstage(L, in, tin, a, h->stream));
+    } else if (pieced && pieces->out && s == nst - 2) {
+      const StageArgs b = args(s + 1);
+      unsigned have = 0, done = 0;
+      for (int c = 0; c < pieces->n; ++c) {
+        CK(piece_launch(s, a, c));
+        have |= 1u << c;
+        for (int q = 0; q < pieces->n; ++q) {
+          if (((done >> q) & 1) || (pieces->deps[q] & ~have)) continue;
+          done |= 1u << q;
+          CK(piece_launch(s + 1, b, q));
+          if (const int rc = pieces->out(q)) return rc;
+        }
+      }
+      ++s;  // the last stage ran with this one
     } else {
-      CK(launch_stage(L, in, tin, a, h->stream));
+      ++launched;
+      if (gauss)
+        CK(launch_vstage(L, stage_in(s), stage_tin(s), a, h->stream));
+      else
+        CK(launch_stage(L, stage_in(s), stage_tin(s), a, h->stream));
     }
     if (s == 0) {
       if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+      ++launched;
       CK(launch_norm(h->E, h->d_part, 1.0 / (double)h->n, h->d_norms, (long)h->norms_cap, h->d_counter,
                      h->d_flag, h->stream));
     }
   }
   if (ev) CK(cudaEventRecord(ev[k++], h->stream));
+  if (nl) *nl += launched;
   return DGB_OK;
 }
 
@@ -651,14 +697,29 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
     return dgb_get_state(h, U_out);
   }
   // pieces of elements with even boundaries (the paired kernels take
-  // elements two by two); an odd element count, whose traces are not paired,
-  // copies in as one piece (a piece of even count would take the paired
-  // trace kernel)
+  // elements two by two), and which pieces each one's neighbours lie in
   constexpr int K = 8;
   long bound[K + 1];
   for (int c = 0; c <= K; ++c) bound[c] = (h->E * c / K) & ~1L;
   bound[K] = h->E;
-  const bool one_in = h->E % 2 != 0;
+  if ((long)h->piece_deps.size() != K || h->piece_deps_E != h->E) {
+    std::vector<int> nb((size_t)h->E * 6);
+    CK(cudaMemcpyAsync(nb.data(), h->d_nbr, sizeof(int) * nb.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->piece_deps.assign(K, 0u);
+    for (int c = 0; c < K; ++c) {
+      h->piece_deps[c] |= 1u << c;
+      for (long e = bound[c]; e < bound[c + 1]; ++e)
+        for (int f = 0; f < 6; ++f) {
+          const long m = nb[(size_t)e * 6 + f];
+          if (m < 0) continue;
+          int q = 0;
+          while (m >= bound[q + 1]) ++q;
+          h->piece_deps[c] |= 1u << q;
+        }
+    }
+    h->piece_deps_E = h->E;
+  }
   if (!h->copy_stream) CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   while (h->host_events.size() < 2 * K + 1) {
     cudaEvent_t e;
@@ -685,10 +746,15 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
     Lc.gf = L.gf ? L.gf + e0 * 6L * kFaceC * h->NQF : nullptr;
     return Lc;
   };
+  long long nl = 0;
+  StepPieces sp;
+  sp.n = K;
+  sp.bound = bound;
+  sp.deps = h->piece_deps.data();
   // in: each piece's copy, then its basis change and face traces (element-local work)
-  for (int c = 0; c < K; ++c) {
-    const long e0 = one_in ? (c ? h->E : 0) : bound[c], e1 = one_in ? h->E : bound[c + 1];
-    if (e1 == e0) continue;
+  auto in = [&](int c) -> int {
+    const long e0 = bound[c], e1 = bound[c + 1];
+    if (e1 == e0) return DGB_OK;
     CK(cudaMemcpyAsync(h->d_U + e0 * nbv, U_in + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
                        cudaMemcpyHostToDevice, h->copy_stream));
     CK(cudaEventRecord(ev_in[c], h->copy_stream));
@@ -697,26 +763,37 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
     CK(launch_gauss_basis(Lc, h->d_U + e0 * nbv, h->d_V + e0 * nbv, true, h->stream));
     CK(launch_vtrace(Lc, h->d_V + e0 * nbv, static_cast<char*>(h->d_trace[0]) + (size_t)e0 * 60 * h->NQF * tb,
                      h->stream));
-  }
-  for (unsigned long long s = 0; s + 1 < nsteps; ++s) CK(cudaGraphLaunch(h->ggraph.exec, h->stream));
-  // out: the last stage of the last step piece by piece, each piece changed
-  // back to nodal values and copied out while the next one computes
-  LastStagePieces lp;
-  lp.n = K;
-  lp.bound = bound;
-  lp.after = [&](int c) -> int {
+    nl += 2;
+    return DGB_OK;
+  };
+  // out: behind each piece of the last stage of the last step, that piece
+  // changed back to nodal values and copied out while the next ones compute
+  auto out = [&](int c) -> int {
     const long e0 = bound[c], e1 = bound[c + 1];
     if (e1 == e0) return DGB_OK;
     CK(launch_gauss_basis(piece(e0, e1), h->d_V + e0 * nbv, h->d_U + e0 * nbv, false, h->stream));
+    ++nl;
     CK(cudaEventRecord(ev_out[c], h->stream));
     CK(cudaStreamWaitEvent(h->copy_stream, ev_out[c], 0));
     CK(cudaMemcpyAsync(U_out + e0 * nbv, h->d_U + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
                        cudaMemcpyDeviceToHost, h->copy_stream));
     return DGB_OK;
   };
-  if ((rc = enqueue_step(h, scheme, dt, nullptr, true, &lp))) return rc;
+  sp.in = in;
+  if (nsteps == 1) {
+    sp.out = out;
+    if ((rc = enqueue_step(h, scheme, dt, nullptr, true, &sp, &nl))) return rc;
+  } else {
+    if ((rc = enqueue_step(h, scheme, dt, nullptr, true, &sp, &nl))) return rc;
+    for (unsigned long long s = 0; s + 2 < nsteps; ++s) CK(cudaGraphLaunch(h->ggraph.exec, h->stream));
+    nl += (long long)(nsteps - 2) * h->launches_per_step;
+    StepPieces last = sp;
+    last.in = nullptr;
+    last.out = out;
+    if ((rc = enqueue_step(h, scheme, dt, nullptr, true, &last, &nl))) return rc;
+  }
   h->v_current = true;
-  h->last_launches = 2L * K + (long long)(nsteps - 1) * h->launches_per_step + h->launches_per_step + K - 1 + K;
+  h->last_launches = nl;
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   if (norms_host)

@@ -72,6 +72,8 @@ struct dgb_handle {
   // order them against the pieces of work on the handle's stream
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> host_events;
+  std::vector<unsigned> piece_deps;  // per piece, the pieces its elements' neighbours lie in (bit mask)
+  long piece_deps_E = -1;
 
   // ---- adjoint (allocated on first use, adjoint_capi.cu)
   // state-sized buffers: stage states S0..S2, stage adjoints A0 A1, the
@@ -121,6 +123,7 @@ inline KLaunch klaunch(const dgb_handle* h)
   L.nbr = h->d_nbr;
   L.prm = h->dprm;
   L.tc = h->tc_step && h->precision == DGB_MIXED_FP32;
+  L.pair = h->E % 2 == 0 && !h->d_gv && !L.tc;
   return L;
 }
 

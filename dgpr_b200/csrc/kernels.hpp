@@ -67,6 +67,10 @@ struct KLaunch {
   const int* nbr;      // [E][6]
   DevParams prm;
   bool tc;             // mixed Gauss-point stages with tensor-core volume contractions
+  // the mixed Gauss-point kernels take elements two by two (FP32x2 pairs):
+  // decided once for the whole mesh (even element count, affine, not tc), so
+  // a launch over a piece of the elements keeps the mesh's trace layout
+  bool pair;
 };
 
 int ops_table_size(int P);

@@ -892,7 +892,7 @@ cudaError_t vlaunch_stage2_p(const KLaunch& L, const double* Vs, const void* Tin
 
 // the paired form serves an FP32 launch on an affine mesh with an even
 // element count; everything else takes the one-element kernels
-inline bool use_pair(const KLaunch& L) { return L.E % 2 == 0 && !L.gv && !L.tc; }
+inline bool use_pair(const KLaunch& L) { return L.pair; }
 
 template <bool HT>
 cudaError_t vprepare2_t(int P)

@@ -234,10 +234,12 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps,
  * written to U_out (host; may equal U_in), with the printed norm of every
  * step in norms_host (may be NULL).  The same kernels and results as
  * dgb_set_state + dgb_step + dgb_get_state, bit for bit, with the copies
- * overlapped with the work: the state comes in in pieces on a second stream
- * while the pieces already in are changed to Gauss-point values and their
- * face traces computed, and the last stage of the last step runs in pieces,
- * each copied out while the next one computes.  Overlap needs page-locked
+ * overlapped with the work: the state comes in in pieces of elements on a
+ * second stream while the pieces already in are changed to Gauss-point
+ * values and their face traces computed, the first stage runs on a piece as
+ * soon as the pieces its neighbours lie in are in, and the last two stages
+ * of the last step run piece by piece, each last-stage piece copied out
+ * while the others compute.  Overlap needs page-locked
  * (pinned) host buffers; pageable ones give the same results.  The nodal
  * step form (dgb_set_step_form) takes the plain calls.  No counterpart in
  * the reference, whose driver copies the state in once and out at each

@@ -283,18 +283,21 @@ def test_step_forms_agree_at_every_order(p):
 @pytest.mark.parametrize("prec", [dg.FP64, dg.MIXED_FP32], ids=["fp64", "mixed"])
 def test_step_host_equals_set_step_get(prec):
     """dgb_step_host (host state in, the copies overlapped with the work in
-    pieces) gives dgb_set_state + dgb_step + dgb_get_state bit for bit: the
-    same kernels on the same elements.  Cases: the TGV and vortex run cases
-    (even element counts: paired traces in the mixed form), an odd element
-    count, a curved channel, RK4 and TVD-RK3, one and three steps, pinned
-    and pageable buffers, and the output written over the input."""
+    pieces: the first stage piece by piece as its neighbours' pieces land, the
+    last two stages interleaved piece by piece) gives dgb_set_state +
+    dgb_step + dgb_get_state bit for bit: the same kernels on the same
+    elements.  Cases: the TGV and vortex run cases (even element counts:
+    paired traces in the mixed form), an odd element count, a curved channel,
+    RK4 and TVD-RK3, one, two and three steps (pieced first and last steps
+    with and without captured steps between them), pinned and pageable
+    buffers, and the output written over the input."""
     import torch
     cs = [c for c in C.run_cases() if c.name in ("tgv_rk4", "vortex_rk4", "sine_channel_tvdrk3", "channel_tvdrk3")]
     odd = C.Case("odd", 3, 3, 3, 2, 1, C.box_nodes(3, 3, 3, 1, 1.0, 1.0, 1.0), [C.P_] * 6, C.params(mu=1e-2, u=0.3),
                  C.random_state(C.params(mu=1e-2, u=0.3), 27, 27, np.random.default_rng(3), 0.02), scheme=0,
                  dt=1e-3, nsteps=3)
     for c in cs + [odd]:
-        for n in (1, 3):
+        for n in (1, 2, 3):
             with solver(c, prec) as s:
                 s.set_state(c.U)
                 norms_a = s.step(c.scheme, c.dt, n)
