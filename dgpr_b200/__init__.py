@@ -96,6 +96,8 @@ def lib():
             "dgb_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp]),
             "dgb_step_host": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp, _dp,
                                              _dp]),
+            "dgb_step_host_async": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _dp,
+                                                   _dp, _dp]),
             "dgb_last_launch_count": (ctypes.c_longlong, [vp]),
             "dgb_profile_step": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp,
                                                 ctypes.POINTER(ctypes.c_int)]),
@@ -318,11 +320,13 @@ class Solver:
         _check(lib().dgb_create(ctypes.byref(self._desc), ctypes.byref(self.params), precision, ctypes.byref(h)))
         self.h = h
         self.n = lib().dgb_state_size(h)
+        self._pending = []  # host arrays that queued copies still read or write
 
     def close(self):
         if self.h:
-            lib().dgb_destroy(self.h)
+            lib().dgb_destroy(self.h)  # waits for the queued copies
             self.h = None
+            self._pending = []
 
     def __del__(self):
         try:
@@ -384,14 +388,18 @@ class Solver:
         _check(lib().dgb_step(self.h, int(scheme), float(dt), int(nsteps), _p(out) if norms else None))
         return out[:nsteps]
 
-    def step_host(self, scheme, dt, nsteps, U_in, U_out, norms=True):
+    def step_host(self, scheme, dt, nsteps, U_in, U_out, norms=True, wait=True):
         """dgb_step_host: nsteps steps of the host state U_in into U_out
         (float64 numpy arrays, page-locked for the overlap), the copies
-        overlapped with the work; returns the per-step norms."""
+        overlapped with the work; returns the per-step norms.  wait=False:
+        dgb_step_host_async, the arrays (and the returned norms array) are
+        filled by the time synchronize() returns."""
         assert U_in.dtype == np.float64 and U_out.dtype == np.float64 and U_in.size == U_out.size == self.n
         out = np.zeros(max(int(nsteps), 1)) if norms else None
-        _check(lib().dgb_step_host(self.h, int(scheme), float(dt), int(nsteps), _p(U_in), _p(U_out),
-                                   _p(out) if norms else None))
+        fn = lib().dgb_step_host if wait else lib().dgb_step_host_async
+        if not wait:
+            self._pending.append((U_in, U_out, out))
+        _check(fn(self.h, int(scheme), float(dt), int(nsteps), _p(U_in), _p(U_out), _p(out) if norms else None))
         return out[:nsteps] if norms else None
 
     def profile_step(self, scheme, dt, reps):
@@ -417,7 +425,10 @@ class Solver:
         return M
 
     def synchronize(self):
-        _check(lib().dgb_synchronize(self.h))
+        try:
+            _check(lib().dgb_synchronize(self.h))
+        finally:
+            self._pending = []
 
     def set_prandtl(self, prandtl):
         """Heat conduction with Prandtl number `prandtl` (0 or inf: off, the

@@ -92,6 +92,7 @@ struct StepPieces {
   int n = 0;
   const long* bound = nullptr;
   const unsigned* deps = nullptr;
+  const int* in_order = nullptr;  // the order of in() (null: 0, 1, ...)
   std::function<int(int)> in;   // set: the first stage in pieces
   std::function<int(int)> out;  // set: the last two stages in pieces
 };
@@ -141,7 +142,8 @@ int enqueue_step(dgb_handle* h, int scheme, double dt, cudaEvent_t* ev = nullptr
     if (ev) CK(cudaEventRecord(ev[k++], h->stream));
     if (pieced && pieces->in && s == 0) {
       unsigned have = 0, done = 0;
-      for (int c = 0; c < pieces->n; ++c) {
+      for (int i = 0; i < pieces->n; ++i) {
+        const int c = pieces->in_order ? pieces->in_order[i] : i;
         if (const int rc = pieces->in(c)) return rc;
         have |= 1u << c;
         for (int q = 0; q < pieces->n; ++q) {
@@ -187,15 +189,18 @@ long long launches_per_step(const dgb_handle*, int scheme) { return (scheme == D
 
 void free_all(dgb_handle* h)
 {
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  if (h->copy_out) cudaStreamSynchronize(h->copy_out);
   drop_step_graphs(h);
   void* ptrs[] = {h->d_ops, h->d_opsf, h->d_geo, h->d_gv, h->d_gf, h->d_nbr, h->d_wallf, h->d_mean, h->d_U, h->d_V, h->d_Us, h->d_acc, h->d_trace[0],
                   h->d_trace[1], h->d_trace[2], h->d_in, h->d_f, h->d_R, h->d_part, h->d_norms,
-                  h->d_counter, h->d_flag};
+                  h->d_counter, h->d_flag, h->d_out, h->d_hnorms};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   free_adjoint(h);
   for (cudaEvent_t e : h->host_events) cudaEventDestroy(e);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->copy_out) cudaStreamDestroy(h->copy_out);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -463,6 +468,10 @@ int dgb_destroy(dgb_handle* h)
 int dgb_set_stream(dgb_handle* h, void* stream)
 {
   if (!h) return fail(DGB_ERR_ARG, "null handle");
+  if (h->host_pipe) {  // the copies of unsynchronized dgb_step_host_async calls
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    if (h->copy_out) cudaStreamSynchronize(h->copy_out);
+  }
   if (h->own_stream && h->stream) {
     cudaStreamSynchronize(h->stream);
     cudaStreamDestroy(h->stream);
@@ -508,6 +517,15 @@ int dgb_synchronize(dgb_handle* h)
   if (!h) return fail(DGB_ERR_ARG, "null handle");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
+  if (h->copy_stream) CK(cudaStreamSynchronize(h->copy_stream));
+  if (h->copy_out) CK(cudaStreamSynchronize(h->copy_out));
+  if (!h->host_pipe) return DGB_OK;
+  h->host_pipe = false;  // the status of the dgb_step_host_async calls since the last synchronization
+  int flag = 0;
+  CK(cudaMemcpy(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
+  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
+  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
   return DGB_OK;
 }
 
@@ -683,8 +701,23 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, do
   return DGB_OK;
 }
 
-int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
-                  double* U_out, double* norms_host)
+namespace {
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+__global__ void copy_doubles_kernel(const double* __restrict__ src, double* __restrict__ dst, long n)
+{
+  for (long i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// dgb_step_host and dgb_step_host_async.  Asynchronous calls return once the
+// work is queued: a call's copy of piece c in waits for the handle's earlier
+// work on its stream (the previous call's stepping included) and for the
+// previous call's copy of piece c out (U_in may be that call's U_out), but
+// not for its other copies out, which read d_out: consecutive calls overlap
+// the copies out of one with the copies in of the next.
+int step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in, double* U_out,
+              double* norms_host, bool async)
 {
   if (!h || !U_in || !U_out) return fail(DGB_ERR_ARG, "null argument");
   if (scheme != DGB_RK4 && scheme != DGB_TVDRK3) return fail(DGB_ERR_ARG, "unknown time scheme");
@@ -692,10 +725,12 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
   CK(cudaSetDevice(h->device));
   int rc;
   if (nsteps == 0 || !h->gauss_step) {  // nothing to overlap: the plain calls
+    if (h->host_pipe && (rc = dgb_synchronize(h))) return rc;
     if ((rc = dgb_set_state(h, U_in))) return rc;
     if (nsteps && (rc = dgb_step(h, scheme, dt, nsteps, norms_host))) return rc;
     return dgb_get_state(h, U_out);
   }
+  if (!h->d_out) CK(cudaMalloc(&h->d_out, sizeof(double) * (size_t)h->n));
   // pieces of elements with even boundaries (the paired kernels take
   // elements two by two), and which pieces each one's neighbours lie in
   constexpr int K = 8;
@@ -718,20 +753,47 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
           h->piece_deps[c] |= 1u << q;
         }
     }
+    // the order in which the interleaved last two stages release pieces
+    // (out), which the copies in follow: a call's copy in of a piece waits
+    // for the previous call's copy out of it
+    h->piece_order.clear();
+    unsigned have = 0, done = 0;
+    for (int c = 0; c < K; ++c) {
+      have |= 1u << c;
+      for (int q = 0; q < K; ++q)
+        if (!((done >> q) & 1) && !(h->piece_deps[q] & ~have)) {
+          done |= 1u << q;
+          h->piece_order.push_back(q);
+        }
+    }
     h->piece_deps_E = h->E;
   }
   if (!h->copy_stream) CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-  while (h->host_events.size() < 2 * K + 1) {
+  if (!h->copy_out) CK(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
+  while (h->host_events.size() < 3 * K + 2) {
     cudaEvent_t e;
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     h->host_events.push_back(e);
   }
-  cudaEvent_t* ev_in = h->host_events.data();
-  cudaEvent_t* ev_out = ev_in + K;
-  cudaEvent_t ev_start = ev_in[2 * K];
+  cudaEvent_t* ev_in = h->host_events.data();  // piece c landed
+  cudaEvent_t* ev_out = ev_in + K;              // piece c's nodal state is in d_out
+  cudaEvent_t* ev_done = ev_in + 2 * K;         // piece c copied out (the last call's)
+  cudaEvent_t ev_start = ev_in[3 * K];  // (and ev_in[3 K + 1]: the call's norms are staged)
   if ((rc = ensure_step_graph(h, scheme, dt, nsteps, true))) return rc;
-  CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-  CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  // the call's norms are staged in one half of d_hnorms (alternating between
+  // calls) for their copy out, so later work may write d_norms at once
+  if (norms_host && h->hnorms_cap < nsteps) {
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->copy_out) CK(cudaStreamSynchronize(h->copy_out));
+    if (h->d_hnorms) CK(cudaFree(h->d_hnorms));
+    h->d_hnorms = nullptr;
+    CK(cudaMalloc(&h->d_hnorms, sizeof(double) * 2 * nsteps));
+    h->hnorms_cap = nsteps;
+  }
+  set_int_kernel<<<1, 1, 0, h->stream>>>(h->d_counter, 0);  // (a kernel: a memset may queue behind copies)
+  CK(cudaGetLastError());
+  if (!h->host_pipe)  // (else the status of the unsynchronized calls keeps accumulating)
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
   // the copies in start once the handle's earlier work is done with d_U
   CK(cudaEventRecord(ev_start, h->stream));
   CK(cudaStreamWaitEvent(h->copy_stream, ev_start, 0));
@@ -746,15 +808,18 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
     Lc.gf = L.gf ? L.gf + e0 * 6L * kFaceC * h->NQF : nullptr;
     return Lc;
   };
-  long long nl = 0;
+  long long nl = 1;  // the norm counter set above
   StepPieces sp;
   sp.n = K;
   sp.bound = bound;
   sp.deps = h->piece_deps.data();
+  sp.in_order = h->piece_order.data();
   // in: each piece's copy, then its basis change and face traces (element-local work)
   auto in = [&](int c) -> int {
     const long e0 = bound[c], e1 = bound[c + 1];
     if (e1 == e0) return DGB_OK;
+    // U_in may be the previous call's U_out: its piece is read once written
+    CK(cudaStreamWaitEvent(h->copy_stream, ev_done[c], 0));
     CK(cudaMemcpyAsync(h->d_U + e0 * nbv, U_in + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
                        cudaMemcpyHostToDevice, h->copy_stream));
     CK(cudaEventRecord(ev_in[c], h->copy_stream));
@@ -767,16 +832,21 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
     return DGB_OK;
   };
   // out: behind each piece of the last stage of the last step, that piece
-  // changed back to nodal values and copied out while the next ones compute
+  // changed back to nodal values into d_out (once the previous call has copied
+  // its piece out) and copied out while the next ones compute; d_U gets the
+  // nodal state too, as after dgb_step
   auto out = [&](int c) -> int {
     const long e0 = bound[c], e1 = bound[c + 1];
     if (e1 == e0) return DGB_OK;
-    CK(launch_gauss_basis(piece(e0, e1), h->d_V + e0 * nbv, h->d_U + e0 * nbv, false, h->stream));
+    const size_t bytes = sizeof(double) * (size_t)(e1 - e0) * nbv;
+    CK(cudaStreamWaitEvent(h->stream, ev_done[c], 0));
+    CK(launch_gauss_basis(piece(e0, e1), h->d_V + e0 * nbv, h->d_out + e0 * nbv, false, h->stream,
+                          h->d_U + e0 * nbv));
     ++nl;
     CK(cudaEventRecord(ev_out[c], h->stream));
-    CK(cudaStreamWaitEvent(h->copy_stream, ev_out[c], 0));
-    CK(cudaMemcpyAsync(U_out + e0 * nbv, h->d_U + e0 * nbv, sizeof(double) * (size_t)(e1 - e0) * nbv,
-                       cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(cudaStreamWaitEvent(h->copy_out, ev_out[c], 0));
+    CK(cudaMemcpyAsync(U_out + e0 * nbv, h->d_out + e0 * nbv, bytes, cudaMemcpyDeviceToHost, h->copy_out));
+    CK(cudaEventRecord(ev_done[c], h->copy_out));
     return DGB_OK;
   };
   sp.in = in;
@@ -794,16 +864,36 @@ int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nstep
   }
   h->v_current = true;
   h->last_launches = nl;
-  int flag = 0;
-  CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  if (norms_host)
-    CK(cudaMemcpyAsync(norms_host, h->d_norms, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
-  CK(cudaStreamSynchronize(h->copy_stream));
-  if (flag & 1) return fail(DGB_ERR_NONFINITE, "residual norm became NaN/Inf");
-  if (flag & 16) return fail(DGB_ERR_CUDA, "tensor-core stage: a wait for the tensor cores gave up");
-  if (flag & 2) return fail(DGB_ERR_BOUNDARY, "subsonic inflow without a non-negative Mach root");
-  return DGB_OK;
+  // the norms go out behind the state, from their staging half: a copy out
+  // on the handle's stream would queue behind the state's copies out and
+  // hold up the next call's start
+  if (norms_host) {
+    h->norm_half ^= 1;
+    double* stage = h->d_hnorms + (h->norm_half ? h->hnorms_cap : 0);
+    copy_doubles_kernel<<<1, 256, 0, h->stream>>>(h->d_norms, stage, (long)nsteps);
+    CK(cudaGetLastError());
+    ++nl;
+    cudaEvent_t ev_norms = ev_in[3 * K + 1];
+    CK(cudaEventRecord(ev_norms, h->stream));
+    CK(cudaStreamWaitEvent(h->copy_out, ev_norms, 0));
+    CK(cudaMemcpyAsync(norms_host, stage, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, h->copy_out));
+  }
+  h->host_pipe = true;
+  return async ? DGB_OK : dgb_synchronize(h);
+}
+
+}  // namespace
+
+int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
+                  double* U_out, double* norms_host)
+{
+  return step_host(h, scheme, dt, nsteps, U_in, U_out, norms_host, false);
+}
+
+int dgb_step_host_async(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
+                        double* U_out, double* norms_host)
+{
+  return step_host(h, scheme, dt, nsteps, U_in, U_out, norms_host, true);
 }
 
 int dgb_profile_step(dgb_handle* h, int scheme, double dt, int reps, double* ms_out, int* nk)

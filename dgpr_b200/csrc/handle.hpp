@@ -68,11 +68,19 @@ struct dgb_handle {
   bool v_current = false;
   long long launches_per_step = 0;
   long long last_launches = 0;
-  // dgb_step_host: a second stream for the host copies and the events that
-  // order them against the pieces of work on the handle's stream
+  // dgb_step_host: streams for the host copies in (copy_stream) and out
+  // (copy_out), the events that order them against the pieces of work on the
+  // handle's stream, and the nodal state the copies out read (d_out)
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t copy_out = nullptr;
   std::vector<cudaEvent_t> host_events;
+  double* d_out = nullptr;
+  bool host_pipe = false;  // dgb_step_host_async work not yet synchronized
+  double* d_hnorms = nullptr;          // dgb_step_host's norms on their way out: 2 halves
+  unsigned long long hnorms_cap = 0;   // doubles per half
+  int norm_half = 0;                   // the half the last call staged
   std::vector<unsigned> piece_deps;  // per piece, the pieces its elements' neighbours lie in (bit mask)
+  std::vector<int> piece_order;      // the order the interleaved last stages release the pieces
   long piece_deps_E = -1;
 
   // ---- adjoint (allocated on first use, adjoint_capi.cu)

@@ -118,12 +118,14 @@ cudaError_t launch_vstage(const KLaunch& L, const double* Vs, const void* Tin, c
                           cudaStream_t st);
 // the basis changes of the Gauss-point form, FP64, per element (vspace.cuh)
 enum { GB_TO_GAUSS = 0, GB_TO_NODAL = 1, GB_ADJ_TO_GAUSS = 2, GB_ADJ_TO_NODAL = 3 };
-cudaError_t launch_gauss_basis_mode(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st);
+// out2, when given, receives the same values as out
+cudaError_t launch_gauss_basis_mode(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st,
+                                    double* out2 = nullptr);
 // V = B3 U (to_gauss) or U = B3^-1 V
 inline cudaError_t launch_gauss_basis(const KLaunch& L, const double* in, double* out, bool to_gauss,
-                                      cudaStream_t st)
+                                      cudaStream_t st, double* out2 = nullptr)
 {
-  return launch_gauss_basis_mode(L, in, out, to_gauss ? GB_TO_GAUSS : GB_TO_NODAL, st);
+  return launch_gauss_basis_mode(L, in, out, to_gauss ? GB_TO_GAUSS : GB_TO_NODAL, st, out2);
 }
 // per compute type and heat flag (vspace_*.cu)
 cudaError_t vprepare_fp64(int P, bool heat);

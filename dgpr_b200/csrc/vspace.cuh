@@ -461,14 +461,16 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   vstage_finish<P, T, CV, L>(e, sa, Rv, Ve, gve, detJd, sXb, so, sg, opsd, mu, kq, gfe, node, qx, qy, qz);
 }
 
-// The basis changes at the edges of the Gauss-point form, per element, FP64
+// The basis changes at the edges of the Gauss-point form, per element, FP64;
+// out2 (may be null) receives a second copy of the result
 // (mode: GB_TO_GAUSS V = B3 U, GB_TO_NODAL U = B3^-1 V; for adjoint vectors,
 // J(U) = J(B3^-1 V): GB_ADJ_TO_GAUSS dJ/dV = B3^-T dJ/dU, GB_ADJ_TO_NODAL
 // dJ/dU = B3^T dJ/dV).
 template <int P, int MODE>
 __global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const double* __restrict__ in,
                                                                  double* __restrict__ out,
-                                                                 const double* __restrict__ opsd)
+                                                                 const double* __restrict__ opsd,
+                                                                 double* __restrict__ out2)
 {
   using C = Cfg<P>;
   constexpr int NB = C::NB;
@@ -492,6 +494,10 @@ __global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const d
     contract_reg<P, 2, TR>(M, A, tid, v);
 #pragma unroll
     for (int r = 0; r < 5; ++r) out[e * 5 * NB + r * NB + tid] = v[r];
+    if (out2) {
+#pragma unroll
+      for (int r = 0; r < 5; ++r) out2[e * 5 * NB + r * NB + tid] = v[r];
+    }
   }
 }
 

@@ -42,33 +42,35 @@ cudaError_t launch_vstage(const KLaunch& L, const double* Vs, const void* Tin, c
 }
 
 template <int P>
-static cudaError_t gauss_basis_p(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st)
+static cudaError_t gauss_basis_p(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st,
+                                 double* out2)
 {
   const unsigned g = (unsigned)L.E;
   switch (mode) {
-    case GB_TO_GAUSS: gauss_basis_kernel<P, GB_TO_GAUSS><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd); break;
-    case GB_TO_NODAL: gauss_basis_kernel<P, GB_TO_NODAL><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd); break;
+    case GB_TO_GAUSS: gauss_basis_kernel<P, GB_TO_GAUSS><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd, out2); break;
+    case GB_TO_NODAL: gauss_basis_kernel<P, GB_TO_NODAL><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd, out2); break;
     case GB_ADJ_TO_GAUSS:
-      gauss_basis_kernel<P, GB_ADJ_TO_GAUSS><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd);
+      gauss_basis_kernel<P, GB_ADJ_TO_GAUSS><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd, out2);
       break;
     case GB_ADJ_TO_NODAL:
-      gauss_basis_kernel<P, GB_ADJ_TO_NODAL><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd);
+      gauss_basis_kernel<P, GB_ADJ_TO_NODAL><<<g, Cfg<P>::NT, 0, st>>>(L.E, in, out, L.opsd, out2);
       break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_gauss_basis_mode(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st)
+cudaError_t launch_gauss_basis_mode(const KLaunch& L, const double* in, double* out, int mode, cudaStream_t st,
+                                    double* out2)
 {
   switch (L.P) {
-    case 1: return gauss_basis_p<1>(L, in, out, mode, st);
-    case 2: return gauss_basis_p<2>(L, in, out, mode, st);
-    case 3: return gauss_basis_p<3>(L, in, out, mode, st);
-    case 4: return gauss_basis_p<4>(L, in, out, mode, st);
-    case 5: return gauss_basis_p<5>(L, in, out, mode, st);
-    case 6: return gauss_basis_p<6>(L, in, out, mode, st);
-    case 7: return gauss_basis_p<7>(L, in, out, mode, st);
+    case 1: return gauss_basis_p<1>(L, in, out, mode, st, out2);
+    case 2: return gauss_basis_p<2>(L, in, out, mode, st, out2);
+    case 3: return gauss_basis_p<3>(L, in, out, mode, st, out2);
+    case 4: return gauss_basis_p<4>(L, in, out, mode, st, out2);
+    case 5: return gauss_basis_p<5>(L, in, out, mode, st, out2);
+    case 6: return gauss_basis_p<6>(L, in, out, mode, st, out2);
+    case 7: return gauss_basis_p<7>(L, in, out, mode, st, out2);
   }
   return cudaErrorInvalidValue;
 }

@@ -138,7 +138,9 @@ int dgb_destroy(dgb_handle* h);
  * NULL = legacy default stream, the reference's only stream). */
 int dgb_set_stream(dgb_handle* h, void* stream);
 
-/* Waits for the work the handle has queued on its stream. */
+/* Waits for the work the handle has queued: its stream and the host copies
+ * of dgb_step_host_async; returns the status of the asynchronous host steps
+ * since the last synchronization. */
 int dgb_synchronize(dgb_handle* h);
 
 /* Optional heat conduction, an extension the reference does not have (its
@@ -246,6 +248,22 @@ int dgb_step(dgb_handle* h, int scheme, double dt, unsigned long long nsteps,
  * checkpoint (cudg.cu:96-126). */
 int dgb_step_host(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
                   double* U_out, double* norms_host);
+
+/* dgb_step_host without waiting: the copies and the steps are queued and the
+ * call returns.  U_in is read and U_out and norms_host written as the queued
+ * copies run, so none of them may be touched before dgb_synchronize(h),
+ * which also reports the status of the steps (a non-finite norm, a boundary
+ * without a Mach root).  Consecutive calls on a handle pipeline: a call's
+ * copy in of a piece waits for the handle's earlier work and for the
+ * previous call's copy out of that piece (U_in may be the previous U_out),
+ * not for the rest of the previous copies out, so stepping a host state in
+ * place call after call overlaps each call's copies out with the next one's
+ * copies in.  Other calls on the handle may follow without synchronizing
+ * (they are ordered after the queued steps); a dgb_step in between resets
+ * the status the synchronization reports.  No counterpart
+ * in the reference. */
+int dgb_step_host_async(dgb_handle* h, int scheme, double dt, unsigned long long nsteps, const double* U_in,
+                        double* U_out, double* norms_host);
 
 /* Kernel launches issued by the last dgb_step / dgb_residual call. */
 long long dgb_last_launch_count(const dgb_handle* h);

@@ -315,3 +315,41 @@ def test_step_host_equals_set_step_get(prec):
                     assert np.array_equal(s.get_state(), Ua)
                     s.step_host(c.scheme, c.dt, n, Uin, Uin)  # in place: the same step again from c.U
                     assert np.array_equal(Uin, Ua), (c.name, n, "in place")
+
+
+@pytest.mark.parametrize("prec", [dg.FP64, dg.MIXED_FP32], ids=["fp64", "mixed"])
+def test_step_host_async_pipeline_equals_sync_calls(prec):
+    """dgb_step_host_async called step after step on a host state in place
+    (each call's copies in overlapping the previous call's copies out) leaves
+    the same state and norms as the synchronous calls, bit for bit; calls on
+    the handle after the queued ones need no synchronization; the status of
+    the queued steps comes back from dgb_synchronize."""
+    import torch
+    cs = [c for c in C.run_cases() if c.name in ("tgv_rk4", "channel_tvdrk3")]
+    odd = C.Case("odd", 3, 3, 3, 2, 1, C.box_nodes(3, 3, 3, 1, 1.0, 1.0, 1.0), [C.P_] * 6, C.params(mu=1e-2, u=0.3),
+                 C.random_state(C.params(mu=1e-2, u=0.3), 27, 27, np.random.default_rng(3), 0.02), scheme=0,
+                 dt=1e-3, nsteps=3)
+    for c in cs + [odd]:
+        with solver(c, prec) as s:
+            U = np.array(c.U, dtype=np.float64)
+            na = [s.step_host(c.scheme, c.dt, 1, U, U) for _ in range(4)]
+            Ua = U.copy()
+        with solver(c, prec) as s:
+            U = torch.tensor(c.U, dtype=torch.float64).pin_memory().numpy()
+            nb = [s.step_host(c.scheme, c.dt, 1, U, U, wait=False) for _ in range(4)]
+            Ud = s.get_state()  # ordered after the queued steps
+            s.step(c.scheme, c.dt, 1)  # writes the norm buffer before the queued norms are out
+            s.synchronize()
+            assert np.array_equal(U, Ua), c.name
+            assert np.array_equal(Ud, Ua), c.name
+            assert all(np.array_equal(x, y) for x, y in zip(na, nb)), c.name
+    c = cs[0]
+    with solver(c, prec) as s:  # a non-finite state: the error comes with the synchronization
+        U = np.array(c.U, dtype=np.float64)
+        U[7] = np.nan
+        s.step_host(c.scheme, c.dt, 1, U, U, wait=False)
+        with pytest.raises(dg.DgbError) as ex:
+            s.synchronize()
+        assert ex.value.code == dg.ERR_NONFINITE
+        s.set_state(c.U)  # the handle stays usable
+        s.step(c.scheme, c.dt, 1)
