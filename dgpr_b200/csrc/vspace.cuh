@@ -92,16 +92,19 @@ struct VTraceSmem {
 
 // Traces of a Gauss-point state sV[5][NB] (shared memory) on the FN faces
 // lf = FN*half + j, into Te (this element's slice of the trace buffer), in
-// the trace format of trace_half.  Scratch sN[FN][10][NQF].
-template <int P, class T, bool CV>
+// the trace format of trace_half.  Scratch sN[FN][10][NQF].  WARP: one warp
+// owns the element (its lanes stride over the face points, __syncwarp),
+// else the CTA does.
+template <int P, class T, bool CV, int FN = VF<P>::FN, bool WARP = false>
 __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const T* so, const T* sg, T mu, T kq,
                                             T* __restrict__ Te, const double* __restrict__ gfe)
 {
   using C = Cfg<P>;
-  constexpr int NB = C::NB, NQF = C::NQF, FN = VF<P>::FN, NH = FN * NQF;
-  const int tid = threadIdx.x;
+  constexpr int NB = C::NB, NQF = C::NQF, NH = FN * NQF;
+  const int tid = WARP ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+  const int nt = WARP ? 32 : (int)blockDim.x;
 #pragma unroll 1
-  for (int i = tid; i < NH; i += blockDim.x) {  // along the normal line: value and normal derivative
+  for (int i = tid; i < NH; i += nt) {  // along the normal line: value and normal derivative
     const int j = i / NQF, lf = FN * half + j, fq = i % NQF, t1 = fq % P, t2 = fq / P;
     const int a = lf >> 1, end = lf & 1;
     const T* Ev = so + C::oEh + end * P;
@@ -120,9 +123,12 @@ __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const 
       out[(5 + r) * NQF + fq] = dn;
     }
   }
-  __syncthreads();
+  if (WARP)
+    __syncwarp();
+  else
+    __syncthreads();
 #pragma unroll 1
-  for (int i = tid; i < NH; i += blockDim.x) {  // tangential derivatives on the face, then the viscous normal flux
+  for (int i = tid; i < NH; i += nt) {  // tangential derivatives on the face, then the viscous normal flux
     const int j = i / NQF, lf = FN * half + j, fq = i % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
     const T* in = sN + j * 10 * NQF;
     const T* Dq = so + C::oDq;
@@ -979,12 +985,40 @@ cudaError_t vlaunch_trace_p(const KLaunch& L, const double* V, void* Tout, cudaS
   return cudaGetLastError();
 }
 
+// The stage with one warp per element (wstage.cuh, included at the end of
+// this header), for p = 3 where a warp's lanes take two Gauss points and one
+// face point of a two-face pass each.
+#ifndef DGB_WARP_STAGE
+#define DGB_WARP_STAGE 1
+#endif
+constexpr int kWarpElems = 2;  // elements (warps) per CTA of the warp-per-element stage
+template <int P, class T>
+struct WStageSmem;
+template <int P, class T, bool CV, bool HT>
+__global__ void wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
+                              const double* __restrict__ opsd, const double* __restrict__ geo,
+                              const double* __restrict__ gv, const double* __restrict__ gf,
+                              const int* __restrict__ nbr, DevParams prm, StageArgs sa);
+
 template <int P, class T, bool HT>
 cudaError_t vlaunch_stage_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                             cudaStream_t st)
 {
   const unsigned grid = (unsigned)(sa.ecount ? sa.ecount : L.E);
   const StageArgs so = element_order(sa, L.E, 1);
+  if constexpr (DGB_WARP_STAGE && P == 4) {
+    const unsigned g = (grid + kWarpElems - 1) / kWarpElems;
+    const int smem = WStageSmem<P, T>::TOTAL;
+    if (L.gv)
+      wstage_kernel<P, T, true, HT><<<g, 32 * kWarpElems, smem, st>>>(
+          L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
+          L.nbr, L.prm, so);
+    else
+      wstage_kernel<P, T, false, HT><<<g, 32 * kWarpElems, smem, st>>>(
+          L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
+          nullptr, L.nbr, L.prm, so);
+    return cudaGetLastError();
+  }
   if (L.gv)
     vstage_kernel<P, T, true, HT><<<grid, Cfg<P>::NTS, VStageSmem<P, T>::TOTAL, st>>>(
         L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
@@ -1043,3 +1077,5 @@ cudaError_t vlaunch_stage_t(const KLaunch& L, const double* Vs, const void* Tin,
 }
 
 }  // namespace dgb
+
+#include "wstage.cuh"
