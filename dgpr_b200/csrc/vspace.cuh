@@ -46,6 +46,19 @@
 
 namespace dgb {
 
+// Synchronizes the threads that own an element: the CTA (GT = 0), a warp
+// (GT = 32), or a group of GT threads on named barrier id.
+template <int GT>
+__device__ __forceinline__ void group_sync(int id)
+{
+  if constexpr (GT == 0)
+    __syncthreads();
+  else if constexpr (GT == 32)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(GT) : "memory");
+}
+
 template <int P>
 struct VF {
   static constexpr int FN = DGB_VFACES_PER_PASS ? DGB_VFACES_PER_PASS : Cfg<P>::FPP;
@@ -92,17 +105,17 @@ struct VTraceSmem {
 
 // Traces of a Gauss-point state sV[5][NB] (shared memory) on the FN faces
 // lf = FN*half + j, into Te (this element's slice of the trace buffer), in
-// the trace format of trace_half.  Scratch sN[FN][10][NQF].  WARP: one warp
-// owns the element (its lanes stride over the face points, __syncwarp),
-// else the CTA does.
-template <int P, class T, bool CV, int FN = VF<P>::FN, bool WARP = false>
+// the trace format of trace_half.  Scratch sN[FN][10][NQF].  GT: the
+// element belongs to a group of GT threads of the CTA (32: a warp, ordered by
+// __syncwarp; more: named barrier gbar), 0: to the whole CTA.
+template <int P, class T, bool CV, int FN = VF<P>::FN, int GT = 0>
 __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const T* so, const T* sg, T mu, T kq,
-                                            T* __restrict__ Te, const double* __restrict__ gfe)
+                                            T* __restrict__ Te, const double* __restrict__ gfe, int gbar = 0)
 {
   using C = Cfg<P>;
   constexpr int NB = C::NB, NQF = C::NQF, NH = FN * NQF;
-  const int tid = WARP ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
-  const int nt = WARP ? 32 : (int)blockDim.x;
+  const int tid = GT ? (int)(threadIdx.x % GT) : (int)threadIdx.x;
+  const int nt = GT ? GT : (int)blockDim.x;
 #pragma unroll 1
   for (int i = tid; i < NH; i += nt) {  // along the normal line: value and normal derivative
     const int j = i / NQF, lf = FN * half + j, fq = i % NQF, t1 = fq % P, t2 = fq / P;
@@ -123,10 +136,7 @@ __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const 
       out[(5 + r) * NQF + fq] = dn;
     }
   }
-  if (WARP)
-    __syncwarp();
-  else
-    __syncthreads();
+  group_sync<GT>(gbar);
 #pragma unroll 1
   for (int i = tid; i < NH; i += nt) {  // tangential derivatives on the face, then the viscous normal flux
     const int j = i / NQF, lf = FN * half + j, fq = i % NQF, q1 = fq % P, q2 = fq / P, a = lf >> 1;
@@ -892,10 +902,40 @@ cudaError_t vlaunch_trace2_p(const KLaunch& L, const double* V, void* Tout, cuda
   return cudaGetLastError();
 }
 
+// The stages with a group of warps per element (one warp at p = 3, two at
+// p = 4) or per pair of elements (p = 4) (wstage.cuh, included at the end of
+// this header).
+#ifndef DGB_WARP_STAGE
+#define DGB_WARP_STAGE 1
+#endif
+constexpr int kWarpElems = 2;  // elements (or pairs) per CTA of the warp-group stages
+template <int P, class T>
+struct WStageSmem;
+template <int P, class T, bool CV, bool HT>
+__global__ void wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
+                              const double* __restrict__ opsd, const double* __restrict__ geo,
+                              const double* __restrict__ gv, const double* __restrict__ gf,
+                              const int* __restrict__ nbr, DevParams prm, StageArgs sa);
+
+template <int P>
+struct WPairSmem;
+template <int P, bool HT>
+__global__ void wstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float* __restrict__ opsg,
+                               const double* __restrict__ opsd, const double* __restrict__ geo,
+                               const int* __restrict__ nbr, DevParams prm, StageArgs sa);
+
 template <int P, bool HT>
 cudaError_t vlaunch_stage2_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                              cudaStream_t st)
 {
+  if constexpr (DGB_WARP_STAGE && P == 5) {  // (at p = 3 measured 1% slower than a CTA per pair)
+    const unsigned npair = (unsigned)((sa.ecount ? sa.ecount : L.E) / 2);
+    wstage2_kernel<P, HT><<<(npair + kWarpElems - 1) / kWarpElems, WPairSmem<P>::GT * kWarpElems,
+                            WPairSmem<P>::TOTAL, st>>>(
+        L.E, Vs, reinterpret_cast<const f2*>(Tin), reinterpret_cast<const float*>(L.ops), L.opsd, L.geo, L.nbr,
+        L.prm, element_order(sa, L.E, 2));
+    return cudaGetLastError();
+  }
   vstage2_kernel<P, HT><<<(unsigned)((sa.ecount ? sa.ecount : L.E) / 2), Cfg<P>::NTS, VPairSmem<P>::TOTAL, st>>>(
       L.E, Vs, reinterpret_cast<const f2*>(Tin), reinterpret_cast<const float*>(L.ops), L.opsd, L.geo, L.nbr,
       L.prm, element_order(sa, L.E, 2));
@@ -985,36 +1025,22 @@ cudaError_t vlaunch_trace_p(const KLaunch& L, const double* V, void* Tout, cudaS
   return cudaGetLastError();
 }
 
-// The stage with one warp per element (wstage.cuh, included at the end of
-// this header), for p = 3 where a warp's lanes take two Gauss points and one
-// face point of a two-face pass each.
-#ifndef DGB_WARP_STAGE
-#define DGB_WARP_STAGE 1
-#endif
-constexpr int kWarpElems = 2;  // elements (warps) per CTA of the warp-per-element stage
-template <int P, class T>
-struct WStageSmem;
-template <int P, class T, bool CV, bool HT>
-__global__ void wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
-                              const double* __restrict__ opsd, const double* __restrict__ geo,
-                              const double* __restrict__ gv, const double* __restrict__ gf,
-                              const int* __restrict__ nbr, DevParams prm, StageArgs sa);
-
 template <int P, class T, bool HT>
 cudaError_t vlaunch_stage_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                             cudaStream_t st)
 {
   const unsigned grid = (unsigned)(sa.ecount ? sa.ecount : L.E);
   const StageArgs so = element_order(sa, L.E, 1);
-  if constexpr (DGB_WARP_STAGE && P == 4) {
+  if constexpr (DGB_WARP_STAGE && (P == 4 || P == 5)) {
     const unsigned g = (grid + kWarpElems - 1) / kWarpElems;
     const int smem = WStageSmem<P, T>::TOTAL;
+    constexpr int NT = WStageSmem<P, T>::GT * kWarpElems;
     if (L.gv)
-      wstage_kernel<P, T, true, HT><<<g, 32 * kWarpElems, smem, st>>>(
+      wstage_kernel<P, T, true, HT><<<g, NT, smem, st>>>(
           L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, L.gv, L.gf,
           L.nbr, L.prm, so);
     else
-      wstage_kernel<P, T, false, HT><<<g, 32 * kWarpElems, smem, st>>>(
+      wstage_kernel<P, T, false, HT><<<g, NT, smem, st>>>(
           L.E, Vs, reinterpret_cast<const T*>(Tin), reinterpret_cast<const T*>(L.ops), L.opsd, L.geo, nullptr,
           nullptr, L.nbr, L.prm, so);
     return cudaGetLastError();

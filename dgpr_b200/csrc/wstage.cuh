@@ -1,9 +1,10 @@
-// The Gauss-point stage with one warp per element (p = 3: 64 Gauss points,
-// two per lane; 16 face points per face, two faces per pass, one per lane).
-// A CTA holds two independent elements, one per warp, sharing the operator
-// table: the only block barrier is the one after the table is loaded, the
-// phases of an element are ordered by __syncwarp alone, and faces go two at
-// a time, so each pass is one full round of the warp.  The arithmetic is the
+// The Gauss-point stage with a group of warps per element: one warp at p = 3
+// (64 Gauss points, two per lane; 16 face points per face, two faces per
+// pass, one per lane), two at p = 4 (125 Gauss points; 50 face points a pass;
+// the group on a named barrier).  A CTA holds two independent elements, one
+// per group, sharing the operator table: the only block barrier is the one
+// after the table is loaded, and the phases of an element are ordered by its
+// group's own synchronization.  The arithmetic is the
 // element-per-CTA kernel's own (vpoint_flux, load_face_point,
 // face_point_fluxes, vtrace_half, rk_stage_value in the same order), so the
 // state comes out bit for bit the same; only the per-element residual norm
@@ -19,7 +20,8 @@ struct WStageSmem {
   using C = Cfg<P>;
   static constexpr int NB = C::NB, NQF = C::NQF;
   static constexpr int ST = (int)sizeof(T);
-  static constexpr int FPW = 2;  // faces per pass
+  static constexpr int FPW = 2;                // faces per pass
+  static constexpr int GT = P <= 4 ? 32 : 64;  // threads per element
   static constexpr int OPSB = align16(C::OPS * ST);
   // per element: [geometry | Y (V first) : 5 NB | R]
   static constexpr int eGeo = 0;
@@ -35,12 +37,30 @@ struct WStageSmem {
   static constexpr int RT = 5 * NB * ST + FPW * 10 * NQF * ST;
   static constexpr int RMAX = RG > RF ? (RG > RN ? (RG > RT ? RG : RT) : (RN > RT ? RN : RT))
                                       : (RF > RN ? (RF > RT ? RF : RT) : (RN > RT ? RN : RT));
-  static constexpr int ELEM = eR + align16(RMAX);
+  static constexpr int eRed = eR + align16(RMAX);  // per-warp sums of the norm partial
+  static constexpr int ELEM = eRed + 16;
   static constexpr int TOTAL = OPSB + kWarpElems * ELEM;
 };
 
+// The sum over a group's threads of one value each, in a fixed order; valid
+// in thread 0 of the group.
+template <int GT>
+__device__ __forceinline__ double group_sum(double s, int t, double* slots, int bar)
+{
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+  if constexpr (GT > 32) {
+    if ((t & 31) == 0) slots[t >> 5] = s;
+    group_sync<GT>(bar);
+    if (t == 0)
+      for (int w = 1; w < GT / 32; ++w) s += slots[w];
+    group_sync<GT>(bar);
+  }
+  return s;
+}
+
 template <int P, class T, bool CV, bool HT>
-__global__ void __launch_bounds__(32 * kWarpElems, (MinBlocks<P, T>::value))
+__global__ void __launch_bounds__(WStageSmem<P, T>::GT * kWarpElems, (MinBlocks<P, T>::value))
 wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __restrict__ opsg,
               const double* __restrict__ opsd, const double* __restrict__ geo, const double* __restrict__ gv,
               const double* __restrict__ gf, const int* __restrict__ nbr, DevParams prm, StageArgs sa)
@@ -52,11 +72,12 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* so = reinterpret_cast<T*>(smraw);
   for (int i = threadIdx.x; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
   __syncthreads();  // the operator table, shared by the CTA's elements
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long u = (long)kWarpElems * blockIdx.x + warp;
+  constexpr int GT = L::GT;
+  const int grp = threadIdx.x / GT, lt = threadIdx.x % GT, bar = 1 + grp;  // element group, thread in it
+  const long u = (long)kWarpElems * blockIdx.x + grp;
   if (u >= (sa.ecount ? sa.ecount : E)) return;
   const long e = sa.ebase + sa.estep * u;
-  unsigned char* eb = smraw + L::OPSB + warp * L::ELEM;
+  unsigned char* eb = smraw + L::OPSB + grp * L::ELEM;
   T* sg = reinterpret_cast<T*>(eb + L::eGeo);
   T* Y = reinterpret_cast<T*>(eb + L::eY);  // the state V first, the Gauss-point residual Y later
   T* V1 = Y;
@@ -64,18 +85,18 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* G = R;
 
   if (DGB_PREFETCH_L2 && (sizeof(T) == 8 || DGB_PREFETCH_L2_F32)) {  // data read much later
-    prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), lane, 32);
-    if (lane < 6) {
-      const int nb = nbr[e * 6 + lane];
-      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (lane ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
+    prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), lt, GT);
+    if (lt < 6) {
+      const int nb = nbr[e * 6 + lt];
+      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (lt ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
     }
-    if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, lane, 32);
-    if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3) prefetch_range(sa.acc + e * 5 * NB, 40L * NB, lane, 32);
+    if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, lt, GT);
+    if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3) prefetch_range(sa.acc + e * 5 * NB, 40L * NB, lt, GT);
   }
-  for (int i = lane; i < kGeoStride; i += 32) sg[i] = T(geo[e * kGeoStride + i]);
+  for (int i = lt; i < kGeoStride; i += GT) sg[i] = T(geo[e * kGeoStride + i]);
   const double* Ve = Vs + e * 5 * NB;
-  for (int i = lane; i < 5 * NB; i += 32) V1[i] = T(Ve[i]);
-  __syncwarp();
+  for (int i = lt; i < 5 * NB; i += GT) V1[i] = T(Ve[i]);
+  group_sync<GT>(bar);
 
   const T* Dq = so + C::oDq;
   const T* w = so + C::oW;
@@ -87,17 +108,17 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   const double* gfe = CV ? gf + e * 6 * kFaceC * NQF : nullptr;
 
   // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
-  for (int o = lane; o < NB; o += 32) {  // reference gradients
+  for (int o = lt; o < NB; o += GT) {  // reference gradients
     contract<P, 0, false, false>(Dq, V1, G, o);
     contract<P, 1, false, false>(Dq, V1, G + 5 * NB, o);
     contract<P, 2, false, false>(Dq, V1, G + 10 * NB, o);
   }
-  __syncwarp();
-  for (int o = lane; o < NB; o += 32)  // pointwise flux at o, in place of its gradients
+  group_sync<GT>(bar);
+  for (int o = lt; o < NB; o += GT)  // pointwise flux at o, in place of its gradients
     vpoint_flux<P, T, CV, false>(so, V1, G, Ji, detJ, gve, gamma, mu, kq, o,
                                  [&](int i, int r, T v) { G[i * 5 * NB + r * NB + o] = v; });
-  __syncwarp();
-  for (int o = lane; o < NB; o += 32) {  // Y = sum_i Dq_i^T Ghat_i minus the source tested with w detJ (over V)
+  group_sync<GT>(bar);
+  for (int o = lt; o < NB; o += GT) {  // Y = sum_i Dq_i^T Ghat_i minus the source tested with w detJ (over V)
     const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
     const T wJq = w[qx] * w[qy] * w[qz] * (CV ? T(gve[kVolDetJ * NB + o]) : detJ);
     T rv[5], y[5];
@@ -109,7 +130,7 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 #pragma unroll
     for (int r = 0; r < 5; ++r) Y[r * NB + o] = rv[r] + y[r] - T(prm.src[r]) * wJq;
   }
-  __syncwarp();
+  group_sync<GT>(bar);
 
   // ---------------- faces (solve.cpp:393-794), FPW at a time
   T* Fa = R;                    // [FPW][5][NQF]
@@ -118,16 +139,16 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 #pragma unroll 1
   for (int pass = 0; pass < 6 / FPW; ++pass) {
 #pragma unroll 1
-    for (int i = lane; i < NH; i += 32) {
+    for (int i = lt; i < NH; i += GT) {
       const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF;
       T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
       const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
       face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
                                   sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
-    __syncwarp();
+    group_sync<GT>(bar);
 #pragma unroll 1
-    for (int i = lane; i < NH; i += 32) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
+    for (int i = lt; i < NH; i += GT) {  // tangential test derivatives: g = fa + Dq^T fb_ax1 + Dq^T fb_ax2, h = fb_a
       const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
       const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
       const T* fa = Fa + j * 5 * NQF;
@@ -146,8 +167,8 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
         gt[(4 + r) * NQF + fq] = fb[(a * 4 + r - 1) * NQF + fq];
       }
     }
-    __syncwarp();
-    for (int o = lane; o < NB; o += 32) {  // each Gauss point gathers from the face points on its normal lines
+    group_sync<GT>(bar);
+    for (int o = lt; o < NB; o += GT) {  // each Gauss point gathers from the face points on its normal lines
       const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
       const T* Ev = so + C::oEh;
       const T* Dv = so + C::oDh;
@@ -168,7 +189,7 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 #pragma unroll
       for (int r = 0; r < 5; ++r) Y[r * NB + o] = rv[r];
     }
-    __syncwarp();
+    group_sync<GT>(bar);
   }
 
   // ---------------- norm partial: the nodal residual R = B3^T Y
@@ -176,26 +197,25 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     const T* B = so + C::oB;
     T* A0 = R;
     T* A1 = R + 5 * NB;
-    for (int o = lane; o < NB; o += 32) contract<P, 0, true, false>(B, Y, A0, o);
-    __syncwarp();
-    for (int o = lane; o < NB; o += 32) contract<P, 1, true, false>(B, A0, A1, o);
-    __syncwarp();
+    for (int o = lt; o < NB; o += GT) contract<P, 0, true, false>(B, Y, A0, o);
+    group_sync<GT>(bar);
+    for (int o = lt; o < NB; o += GT) contract<P, 1, true, false>(B, A0, A1, o);
+    group_sync<GT>(bar);
     double s = 0.;
-    for (int o = lane; o < NB; o += 32) {
+    for (int o = lt; o < NB; o += GT) {
       T rn[5];
       contract_reg<P, 2, true>(B, A1, o, rn);
 #pragma unroll
       for (int r = 0; r < 5; ++r) s += double(rn[r]) * double(rn[r]);
     }
-#pragma unroll
-    for (int k = 16; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k);
-    if (lane == 0) sa.part[e] = s;
-    __syncwarp();
+    s = group_sum<GT>(s, lt, reinterpret_cast<double*>(eb + L::eRed), bar);
+    if (lt == 0) sa.part[e] = s;
+    group_sync<GT>(bar);
   }
 
   // ---------------- f_V = -Y / (w detJ) in FP64, RK update
   T* sVn = R;  // the new state for the epilogue traces
-  for (int o = lane; o < NB; o += 32) {
+  for (int o = lt; o < NB; o += GT) {
     const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
     const double* wd = opsd + C::oW;
     const double jd = CV ? gve[kVolDetJ * NB + o] : detJd;
@@ -216,13 +236,273 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   }
   // ---------------- face traces of the new state for the next stage
   if (sa.Tnext) {
-    __syncwarp();
+    group_sync<GT>(bar);
     T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
     T* sN = R + 5 * NB;
 #pragma unroll 1
     for (int pass = 0; pass < 6 / FPW; ++pass) {
-      if (pass) __syncwarp();
-      vtrace_half<P, T, CV, FPW, true>(pass, sVn, sN, so, sg, mu, kq, Te, gfe);
+      if (pass) group_sync<GT>(bar);
+      vtrace_half<P, T, CV, FPW, GT>(pass, sVn, sN, so, sg, mu, kq, Te, gfe, bar);
+    }
+  }
+}
+
+// The paired mixed stage (vstage2_kernel: two elements per thread in FP32x2)
+// with a group of warps per pair: a CTA holds two independent pairs, one per
+// group, sharing the operator tables.  Same arithmetic as vstage2_kernel.
+// Used at p = 4 (two warps a pair); at p = 3 one warp a pair measured 1%
+// slower than vstage2_kernel's CTA per pair.
+template <int P>
+struct WPairSmem {
+  using C = Cfg<P>;
+  static constexpr int NB = C::NB, NQF = C::NQF;
+  static constexpr int FPW = 2;
+  static constexpr int GT = P <= 4 ? 32 : 64;                // threads per pair
+  static constexpr int oOpsF = align16(C::OPS * 8);         // after the f2 table
+  static constexpr int OPSB = oOpsF + align16(C::OPS * 4);  // f2 and float operator tables
+  // per pair: [f2 geometry | float geometry of each element | Y : 5 NB | R]
+  static constexpr int eGeo = 0;
+  static constexpr int eGeoF = align16(kGeoStride * 8);
+  static constexpr int eY = eGeoF + align16(2 * kGeoStride * 4);
+  static constexpr int eR = eY + align16(5 * NB * 8);
+  static constexpr int RG = 15 * NB * 8;
+  static constexpr int RF = FPW * 26 * NQF * 8;
+  static constexpr int RN = 10 * NB * 8;
+  static constexpr int RT = 5 * NB * 8 + FPW * 10 * NQF * 8;
+  static constexpr int RMAX = RG > RF ? (RG > RN ? (RG > RT ? RG : RT) : (RN > RT ? RN : RT))
+                                      : (RF > RN ? (RF > RT ? RF : RT) : (RN > RT ? RN : RT));
+  static constexpr int eRed = eR + align16(RMAX);  // per-warp sums of the norm partials
+  static constexpr int ELEM = eRed + 32;
+  static constexpr int TOTAL = OPSB + kWarpElems * ELEM;
+};
+
+template <int P, bool HT>
+__global__ void __launch_bounds__(WPairSmem<P>::GT * kWarpElems, (MinBlocksPair<P>::value))
+wstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float* __restrict__ opsg,
+               const double* __restrict__ opsd, const double* __restrict__ geo, const int* __restrict__ nbr,
+               DevParams prm, StageArgs sa)
+{
+  using C = Cfg<P>;
+  using L = WPairSmem<P>;
+  using T = f2;
+  constexpr int NB = C::NB, NQF = C::NQF, FPW = L::FPW, NH = FPW * NQF, GT = L::GT;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* so = reinterpret_cast<T*>(smraw);
+  float* sof = reinterpret_cast<float*>(smraw + L::oOpsF);
+  for (int i = threadIdx.x; i < C::OPS; i += blockDim.x) {
+    so[i] = T(opsg[i]);
+    sof[i] = opsg[i];
+  }
+  __syncthreads();  // the operator tables, shared by the CTA's pairs
+  const int grp = threadIdx.x / GT, lt = threadIdx.x % GT, bar = 1 + grp;  // pair group, thread in it
+  const long u = (long)kWarpElems * blockIdx.x + grp;
+  if (u >= (sa.ecount ? sa.ecount : E) / 2) return;
+  const long k = sa.ebase + sa.estep * u, e0 = 2 * k;
+  const long el[2] = {e0, e0 + 1};
+  unsigned char* eb = smraw + L::OPSB + grp * L::ELEM;
+  T* sg = reinterpret_cast<T*>(eb + L::eGeo);
+  float* sgf = reinterpret_cast<float*>(eb + L::eGeoF);  // [2][kGeoStride]
+  T* Y = reinterpret_cast<T*>(eb + L::eY);
+  T* V1 = Y;
+  T* R = reinterpret_cast<T*>(eb + L::eR);
+  T* G = R;
+
+  if (DGB_PREFETCH_L2 && DGB_PREFETCH_L2_F32) {  // data read much later
+    prefetch_range(Tr2 + k * 60 * NQF, 60L * NQF * sizeof(T), lt, GT);
+    if (lt < 12) {
+      const long e = el[lt / 6];
+      const int lf = lt % 6, nb = nbr[e * 6 + lf];
+      if (nb >= 0) prefetch_range(Tr2 + ((long)(nb / 2) * 6 + (lf ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
+    }
+    for (int l = 0; l < 2; ++l) {
+      if (sa.Ubase) prefetch_range(sa.Ubase + el[l] * 5 * NB, 40L * NB, lt, GT);
+      if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
+        prefetch_range(sa.acc + el[l] * 5 * NB, 40L * NB, lt, GT);
+    }
+  }
+  for (int i = lt; i < kGeoStride; i += GT) {
+    const float g0 = (float)geo[el[0] * kGeoStride + i], g1 = (float)geo[el[1] * kGeoStride + i];
+    sg[i] = T(g0, g1);
+    sgf[i] = g0;
+    sgf[kGeoStride + i] = g1;
+  }
+  const double* Ve0 = Vs + el[0] * 5 * NB;
+  const double* Ve1 = Vs + el[1] * 5 * NB;
+  for (int i = lt; i < 5 * NB; i += GT) V1[i] = T((float)Ve0[i], (float)Ve1[i]);
+  group_sync<GT>(bar);
+
+  const T* Dq = so + C::oDq;
+  const T* w = so + C::oW;
+  const T detJ = sg[kGeoDetJ];
+  const T* Ji = sg + kGeoJinv;
+  const T gamma = T(prm.gamma), mu = T(prm.mu), kq = HT ? T(prm.kq) : T(0.f);
+
+  // ---------------- volume integral (solve.cpp:276-341) + source (345-360)
+  for (int o = lt; o < NB; o += GT) {
+    contract<P, 0, false, false>(Dq, V1, G, o);
+    contract<P, 1, false, false>(Dq, V1, G + 5 * NB, o);
+    contract<P, 2, false, false>(Dq, V1, G + 10 * NB, o);
+  }
+  group_sync<GT>(bar);
+  for (int o = lt; o < NB; o += GT)
+    vpoint_flux<P, T, false, false>(so, V1, G, Ji, detJ, nullptr, gamma, mu, kq, o,
+                                    [&](int i, int r, T v) { G[i * 5 * NB + r * NB + o] = v; });
+  group_sync<GT>(bar);
+  for (int o = lt; o < NB; o += GT) {
+    const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
+    const T wJq = w[qx] * w[qy] * w[qz] * detJ;
+    T rv[5], y[5];
+    contract_reg<P, 0, true>(Dq, G, o, rv);
+    contract_reg<P, 1, true>(Dq, G + 5 * NB, o, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) rv[r] += y[r];
+    contract_reg<P, 2, true>(Dq, G + 10 * NB, o, y);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Y[r * NB + o] = rv[r] + y[r] - T(prm.src[r]) * wJq;
+  }
+  group_sync<GT>(bar);
+
+  // ---------------- faces, FPW at a time
+  T* Fa = R;
+  T* Fb = Fa + FPW * 5 * NQF;
+  T* Gt = Fb + FPW * 12 * NQF;
+#pragma unroll 1
+  for (int pass = 0; pass < 6 / FPW; ++pass) {
+#pragma unroll 1
+    for (int i = lt; i < NH; i += GT) {
+      const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF;
+      const int nb0 = nbr[el[0] * 6 + lf], nb1 = nbr[el[1] * 6 + lf];
+      const T* To = Tr2 + (k * 6 + lf) * 10 * NQF;
+      T* fa = Fa + j * 5 * NQF + fq;
+      T* fb = Fb + j * 12 * NQF + fq;
+      if (nb0 >= 0 && nb1 >= 0) {  // interior for both: paired
+        T Uo[5], Qo[5], Un[5], Qn[5];
+        const long i0 = ((long)(nb0 / 2) * 6 + (lf ^ 1)) * 10 * NQF + fq;
+        const long i1 = ((long)(nb1 / 2) * 6 + (lf ^ 1)) * 10 * NQF + fq;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+          Uo[r] = To[r * NQF + fq];
+          Qo[r] = To[(5 + r) * NQF + fq];
+          Un[r] = T(pair_lane(Tr2, i0 + r * NQF, nb0), pair_lane(Tr2, i1 + r * NQF, nb1));
+          Qn[r] = T(pair_lane(Tr2, i0 + (5 + r) * NQF, nb0), pair_lane(Tr2, i1 + (5 + r) * NQF, nb1));
+        }
+        const T lift_n = T(sof[C::oC + ((lf & 1) ^ 1)]) /
+                         T((float)geo[(long)nb0 * kGeoStride + kGeoDetJ], (float)geo[(long)nb1 * kGeoStride + kGeoDetJ]);
+        face_point_fluxes<P, T, false>(lf, fq, 0, Uo, Qo, Un, Qn, lift_n, so, sg, nullptr, prm, gamma, mu, kq, detJ,
+                                       Ji, sa.flag, fa, fb);
+      } else {  // a boundary in either lane: each lane through the scalar routine
+#pragma unroll 1
+        for (int l = 0; l < 2; ++l)
+          pair_face_lane<P, HT>(l, l ? nb1 : nb0, lf, fq, To, Tr2, sof, sgf + l * kGeoStride, geo, prm, sa.flag,
+                                fa, fb);
+      }
+    }
+    group_sync<GT>(bar);
+#pragma unroll 1
+    for (int i = lt; i < NH; i += GT) {  // tangential test derivatives
+      const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF, t1 = fq % P, t2 = fq / P, a = lf >> 1;
+      const int ax1 = a == 0 ? 1 : 0, ax2 = a == 2 ? 1 : 2;
+      const T* fa = Fa + j * 5 * NQF;
+      const T* fb = Fb + j * 12 * NQF;
+      T* gt = Gt + j * 9 * NQF;
+      gt[fq] = fa[fq];
+#pragma unroll
+      for (int r = 1; r < 5; ++r) {
+        T s = fa[r * NQF + fq];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          s = fma(Dq[q * P + t1], fb[(ax1 * 4 + r - 1) * NQF + q + P * t2], s);
+          s = fma(Dq[q * P + t2], fb[(ax2 * 4 + r - 1) * NQF + t1 + P * q], s);
+        }
+        gt[r * NQF + fq] = s;
+        gt[(4 + r) * NQF + fq] = fb[(a * 4 + r - 1) * NQF + fq];
+      }
+    }
+    group_sync<GT>(bar);
+    for (int o = lt; o < NB; o += GT) {
+      const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
+      const T* Ev = so + C::oEh;
+      const T* Dv = so + C::oDh;
+      T rv[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) rv[r] = Y[r * NB + o];
+#pragma unroll
+      for (int j = 0; j < FPW; ++j) {
+        const int lf = FPW * pass + j, a = lf >> 1, end = lf & 1;
+        const int qa = a == 0 ? qx : a == 1 ? qy : qz;
+        const int t1 = a == 0 ? qy : qx, t2 = a == 2 ? qy : qz;
+        const T ev = Ev[end * P + qa], dv = Dv[end * P + qa];
+        const T* gt = Gt + j * 9 * NQF + t1 + P * t2;
+        rv[0] += ev * gt[0];
+#pragma unroll
+        for (int r = 1; r < 5; ++r) rv[r] += ev * gt[r * NQF] + dv * gt[(4 + r) * NQF];
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Y[r * NB + o] = rv[r];
+    }
+    group_sync<GT>(bar);
+  }
+
+  // ---------------- norm partials: the nodal residual R = B3^T Y of each element
+  if (sa.part) {
+    const T* B = so + C::oB;
+    T* A0 = R;
+    T* A1 = R + 5 * NB;
+    for (int o = lt; o < NB; o += GT) contract<P, 0, true, false>(B, Y, A0, o);
+    group_sync<GT>(bar);
+    for (int o = lt; o < NB; o += GT) contract<P, 1, true, false>(B, A0, A1, o);
+    group_sync<GT>(bar);
+    double s[2] = {0., 0.};
+    for (int o = lt; o < NB; o += GT) {
+      T rn[5];
+      contract_reg<P, 2, true>(B, A1, o, rn);
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int l = 0; l < 2; ++l) s[l] += double(rn[r].lane(l)) * double(rn[r].lane(l));
+    }
+#pragma unroll
+    for (int l = 0; l < 2; ++l) s[l] = group_sum<GT>(s[l], lt, reinterpret_cast<double*>(eb + L::eRed) + 2 * l, bar);
+    if (lt == 0) {
+      sa.part[el[0]] = s[0];
+      sa.part[el[1]] = s[1];
+    }
+    group_sync<GT>(bar);
+  }
+
+  // ---------------- f_V = -Y / (w detJ) in FP64, RK update, per element
+  T* sVn = R;
+  for (int o = lt; o < NB; o += GT) {
+    const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
+    const double* wd = opsd + C::oW;
+    const double wq = wd[qx] * wd[qy] * wd[qz];
+    const double sc0 = -1.0 / (wq * geo[el[0] * kGeoStride + kGeoDetJ]);
+    const double sc1 = -1.0 / (wq * geo[el[1] * kGeoStride + kGeoDetJ]);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const long i0 = el[0] * 5 * NB + r * NB + o, i1 = el[1] * 5 * NB + r * NB + o;
+      const T yv = Y[r * NB + o];
+      const double fr0 = double(yv.lane(0)) * sc0, fr1 = double(yv.lane(1)) * sc1;
+      if (sa.mode == MODE_RESIDUAL) {
+        sa.fout[i0] = fr0;
+        sa.fout[i1] = fr1;
+      } else {
+        const double un0 = rk_stage_value(sa, i0, fr0, Ve0[r * NB + o]);
+        const double un1 = rk_stage_value(sa, i1, fr1, Ve1[r * NB + o]);
+        sa.Uout[i0] = un0;
+        sa.Uout[i1] = un1;
+        sVn[r * NB + o] = T((float)un0, (float)un1);
+      }
+    }
+  }
+  if (sa.Tnext) {
+    group_sync<GT>(bar);
+    T* Te = reinterpret_cast<T*>(sa.Tnext) + k * 60 * NQF;
+    T* sN = R + 5 * NB;
+#pragma unroll 1
+    for (int pass = 0; pass < 6 / FPW; ++pass) {
+      if (pass) group_sync<GT>(bar);
+      vtrace_half<P, T, false, FPW, GT>(pass, sVn, sN, so, sg, mu, kq, Te, nullptr, bar);
     }
   }
 }
