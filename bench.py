@@ -1034,7 +1034,7 @@ def run_ours(args, rank, world, local_rank):
             prof = json.load(open(tpath))
         traffic = prof.get("stage_kernel_bytes_per_launch")
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "vstage_kernel<4,double>", "kernel_ms": stage_ms,
+                "traffic": traffic, "kernel": "wstage_kernel<4,double>", "kernel_ms": stage_ms,
                 "trace_kernel_ms": trace_ms, "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_src}
         fp64_flop = prof.get("stage_kernel_fp64_flop_per_launch")
         if fp64_flop:  # executed FP64 arithmetic (ncu instruction counts, scaled to the launch)
