@@ -38,7 +38,8 @@ struct WStageSmem {
   static constexpr int RMAX = RG > RF ? (RG > RN ? (RG > RT ? RG : RT) : (RN > RT ? RN : RT))
                                       : (RF > RN ? (RF > RT ? RF : RT) : (RN > RT ? RN : RT));
   static constexpr int eRed = eR + align16(RMAX);  // per-warp sums of the norm partial
-  static constexpr int ELEM = eRed + 16;
+  static constexpr int eNb = eRed + 16;              // the neighbours across the six faces
+  static constexpr int ELEM = eNb + 32;
   static constexpr int TOTAL = OPSB + kWarpElems * ELEM;
 };
 
@@ -84,12 +85,17 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* R = reinterpret_cast<T*>(eb + L::eR);
   T* G = R;
 
+  int* sNb = reinterpret_cast<int*>(eb + L::eNb);
+  if (lt < 6) {  // the neighbours, read by the face passes from shared memory
+    const int nb = nbr[e * 6 + lt];
+    sNb[lt] = nb;
+    if (nb >= 0 && DGB_PREFETCH_L2 && (sizeof(T) == 8 || DGB_PREFETCH_L2_F32)) {
+      prefetch_l2(geo + (long)nb * kGeoStride + kGeoDetJ);
+      prefetch_range(Tr + ((long)nb * 6 + (lt ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
+    }
+  }
   if (DGB_PREFETCH_L2 && (sizeof(T) == 8 || DGB_PREFETCH_L2_F32)) {  // data read much later
     prefetch_range(Tr + e * 60 * NQF, 60L * NQF * sizeof(T), lt, GT);
-    if (lt < 6) {
-      const int nb = nbr[e * 6 + lt];
-      if (nb >= 0) prefetch_range(Tr + ((long)nb * 6 + (lt ^ 1)) * 10 * NQF, 10L * NQF * sizeof(T), 0, 1);
-    }
     if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, lt, GT);
     if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3) prefetch_range(sa.acc + e * 5 * NB, 40L * NB, lt, GT);
   }
@@ -141,8 +147,29 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 #pragma unroll 1
     for (int i = lt; i < NH; i += GT) {
       const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF;
-      T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
-      const int nb = load_face_point<P, T, CV>(e, lf, fq, Tr, nbr, so, geo, gf, Uo, Qo, Un, Qn, lift_n);
+      T Uo[5], Qo[5], Un[5], Qn[5], lift_n;  // as load_face_point, the neighbour from shared memory
+      const int nb = sNb[lf];
+      {
+        const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+          Uo[r] = To[r * NQF + fq];
+          Qo[r] = To[(5 + r) * NQF + fq];
+        }
+        lift_n = T(0);
+        if (nb >= 0) {
+          const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+#pragma unroll
+          for (int r = 0; r < 5; ++r) {
+            Un[r] = Tn[r * NQF + fq];
+            Qn[r] = Tn[(5 + r) * NQF + fq];
+          }
+          if constexpr (CV)
+            lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
+          else
+            lift_n = so[C::oC + ((lf & 1) ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+        }
+      }
       face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
                                   sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
     }
