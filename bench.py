@@ -279,6 +279,34 @@ def _reverse_step_ms(dg, torch, s, stream, U0, dt, reps):
     return tot / reps, launches
 
 
+def _reverse_sweep_ms(dg, torch, s, stream, U0, dt, k):
+    """Device time (ms, CUDA events on the handle's stream) per reverse RK4
+    step inside one backward sweep over a recorded run of k steps that kept
+    every state (nothing recomputed): the sweep's k state restores and its
+    two adjoint basis conversions are spread over its k reverse steps, where
+    the single-step call pays three conversions per step."""
+    s.set_state(U0)
+    s.forward_record(dg.RK4, dt, k, k, norms=False)
+    lam = torch.ones(s.n, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(lam)
+    torch.cuda.synchronize()
+    s.backward_device(lam.data_ptr(), out.data_ptr())  # warm-up
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    tot = 0.0
+    for _ in range(3):
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        s.backward_device(lam.data_ptr(), out.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        tot += ev0.elapsed_time(ev1)
+    recomputed, reversed_, _ = s.adjoint_stats()
+    if recomputed != 0 or reversed_ != k:
+        raise RuntimeError(f"sweep recomputed {recomputed} and reversed {reversed_} of {k} steps")
+    return tot / 3 / k
+
+
 def _adjoint_config(dg, torch, nsteps, budgets):
     """Gradient of the final enstrophy w.r.t. the 8 x 3 amplitudes of seeded
     Fourier velocity modes on a uniform flow: periodic [0, 2 pi]^3, 16^3 hexes,
@@ -989,6 +1017,7 @@ def run_ours(args, rank, world, local_rank):
         with dg.Solver(mesh, dg.Params.from_array(prm), dg.FP64) as sa:
             sa.set_stream(stream.cuda_stream)
             rev_ms, rev_launches = _reverse_step_ms(dg, torch, sa, stream, U0, dt, reps)
+            sweep_ms = _reverse_sweep_ms(dg, torch, sa, stream, U0, dt, 20)
             # the forward step the reverse step undoes: the recorded runs step
             # the nodal form
             sa.set_step_form(dg.STEP_NODAL)
@@ -996,7 +1025,9 @@ def run_ours(args, rank, world, local_rank):
             _warm(dg, torch, sa, dt, 3)
             nodal_ms = _timed_steps(dg, torch, sa, stream, dt, min(args.steps, 20)) / min(args.steps, 20)
         adj = {"reverse_step_ms": rev_ms, "forward_step_ms": ms / args.steps,
-               "reverse_over_forward": rev_ms / (ms / args.steps), "forward_step_nodal_ms": nodal_ms,
+               "reverse_over_forward": rev_ms / (ms / args.steps),
+               "sweep_reverse_step_ms": sweep_ms, "sweep_steps": 20,
+               "sweep_reverse_over_forward": sweep_ms / (ms / args.steps), "forward_step_nodal_ms": nodal_ms,
                "reverse_over_nodal_forward": rev_ms / nodal_ms, "reverse_step_launches": rev_launches,
                "config": _adjoint_config(dg, torch, args.adjoint_steps, (args.adjoint_steps, 20, -1))}
 
@@ -1093,6 +1124,7 @@ def run_ours(args, rank, world, local_rank):
             head["mixed_rel_l2_48_p4"] = config3.get("accuracy", {}).get("rel_l2_mixed_vs_fp64")
         if adj:
             head["adjoint_reverse_over_forward"] = adj["reverse_over_forward"]
+            head["adjoint_sweep_reverse_over_forward"] = adj["sweep_reverse_over_forward"]
             head["adjoint_config_backward_over_forward"] = {
                 str(b["slots"]): round(b["backward_over_plain_forward"], 3) for b in adj["config"]["budgets"]}
             head["adjoint_config_fd_rel_l2"] = adj["config"]["fd_full"]["rel_l2"]

@@ -254,7 +254,7 @@ int enqueue_reverse_step(dgb_handle* h, int scheme, double dt, const double* Ui,
     }
     StageArgs a = stage_args(scheme == DGB_RK4 ? rk4[s] : tvd[s], dt);
     a.Ubase = Ui;
-    a.acc = h->d_acc;
+    a.acc = nullptr;  // the RK4 accumulator only forms the step's end state, which a reverse step does not need
     a.Uout = S[s];
     a.flag = h->d_flag;
     a.Tnext = f64 ? tout_f64[s] : tout_mix[s];

@@ -565,16 +565,16 @@ __device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, do
   const double dt = sa.dt;
   double un = 0.;
   switch (sa.mode) {
-    case MODE_RK4_0:
-      sa.acc[i] = fr;
+    case MODE_RK4_0:  // (a null accumulator: a stage state recomputed for a reverse step, which needs none)
+      if (sa.acc) sa.acc[i] = fr;
       un = sa.Ubase[i] + dt * fr * 0.5;
       break;
     case MODE_RK4_1:
-      sa.acc[i] = sa.acc[i] + 2. * fr;
+      if (sa.acc) sa.acc[i] = sa.acc[i] + 2. * fr;
       un = sa.Ubase[i] + dt * fr * 0.5;
       break;
     case MODE_RK4_2:
-      sa.acc[i] = sa.acc[i] + 2. * fr;
+      if (sa.acc) sa.acc[i] = sa.acc[i] + 2. * fr;
       un = sa.Ubase[i] + dt * fr;
       break;
     case MODE_RK4_3:
