@@ -413,14 +413,35 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
   const bool node = tid < NB;
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = geo[e * kGeoStride + i];
-  for (int i = tid; i < 5 * NB; i += blockDim.x) {  // lam = cx X + cy Y + cz Z
-    const long g = e * 5 * NB + i;
-    double l = v.cx * v.X[g];
-    if (v.Y) l = fma(v.cy, v.Y[g], l);
-    if (v.Z) l = fma(v.cz, v.Z[g], l);
-    V0[i] = l;
+  // the element's entries of lam's terms and of the state, per thread, with
+  // all their loads in flight together (the launch has Cfg<P>::NT threads)
+  constexpr int NT = C::NT, NL = (5 * NB + NT - 1) / NT;
+  double ul[NL];
+  {
+    double xl[NL], yl[NL], zl[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+      const int i = tid + k * NT;
+      const long g = e * 5 * NB + i;
+      if (i < 5 * NB) {
+        xl[k] = v.X[g];
+        yl[k] = v.Y ? v.Y[g] : 0.;
+        zl[k] = v.Z ? v.Z[g] : 0.;
+        ul[k] = U[g];
+      }
+    }
+    for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
+    for (int i = tid; i < kGeoStride; i += NT) sg[i] = geo[e * kGeoStride + i];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {  // lam = cx X + cy Y + cz Z
+      const int i = tid + k * NT;
+      if (i < 5 * NB) {
+        double l = v.cx * xl[k];
+        if (v.Y) l = fma(v.cy, yl[k], l);
+        if (v.Z) l = fma(v.cz, zl[k], l);
+        V0[i] = l;
+      }
+    }
   }
   __syncthreads();
   const double* B = so + C::oB;
@@ -467,10 +488,10 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     if (node) contract<P, 2, true, false>(Mi, V0, Mu, tid, -1.0 / detJ);
   }
   __syncthreads();
-  if constexpr (GS) {  // the state is at the Gauss points already
-    for (int i = tid; i < 5 * NB; i += blockDim.x) Sq[i] = U[e * 5 * NB + i];
-  } else {
-    for (int i = tid; i < 5 * NB; i += blockDim.x) V0[i] = U[e * 5 * NB + i];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {  // the state (at the Gauss points already in GS)
+    const int i = tid + k * NT;
+    if (i < 5 * NB) (GS ? Sq : V0)[i] = ul[k];
   }
   __syncthreads();
 
@@ -589,14 +610,30 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   const double* w1 = so + C::oW;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
+    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
+    // this face point's traces, the neighbour and its lifting scale, loaded
+    // before the face values of mu are formed
+    int nb = -1;
+    double Uo[5], Un[5], lift_nb = 0.;
+    if (tid < NH) {
+      nb = nbr[e * 6 + lf];
+      const double* To = Tr + ((e * 6 + lf) * 10) * NQF;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) Uo[r] = To[r * NQF + fq];
+      if (nb >= 0) {
+        const double* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
+        lift_nb = CV ? gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]
+                     : so[C::oC + (end ^ 1)] / geo[(long)nb * kGeoStride + kGeoDetJ];
+      }
+    }
     double Sm[5], gm[3][5];
     if constexpr (GS)  // the gradient of mu is read from sN where the viscous terms need it
       gface_value_grad<P, false>(half, Mu, sN, so, Sm, gm);
     else
       face_value_grad<P>(half, Mu, sN, sY, so, Sm, gm);
-    const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF, q1 = fq % P, q2 = fq / P, end = lf & 1;
     if (tid < NH) {
-      const int nb = nbr[e * 6 + lf];
       const double* gp = CV ? gfe + lf * kFaceC * NQF + fq : nullptr;  // this face point's geometry
       const double fJ = CV ? gp[kFaceFJ * NQF] : sg[kGeoFJ + lf];
       const double fw = fJ * w1[q1] * w1[q2];
@@ -630,16 +667,10 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             dcb[c][r] = -fw * (Ji[c] * gm[0][r] + Ji[3 + c] * gm[1][r] + Ji[6 + c] * gm[2][r]);
         }
       };
-      const double* To = Tr + ((e * 6 + lf) * 10) * NQF;
-      double Uo[5], Uob[5] = {0., 0., 0., 0., 0.}, Qob[5];
-#pragma unroll
-      for (int r = 0; r < 5; ++r) Uo[r] = To[r * NQF + fq];
+      double Uob[5] = {0., 0., 0., 0., 0.}, Qob[5];
       double* TAe = TA + ((e * 6 + lf) * 20) * NQF;
       if (nb >= 0) {
-        const double* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
-        double Un[5], Unb[5] = {0., 0., 0., 0., 0.};
-#pragma unroll
-        for (int r = 0; r < 5; ++r) Un[r] = Tn[r * NQF + fq];
+        double Unb[5] = {0., 0., 0., 0., 0.};
         {  // Roe flux.  The forward orients it (the high side is left) so that
            // both elements compute the same bits; as a function it is
            // f(Uo, Un, n_out) either way (antisymmetric under swapping the
@@ -669,8 +700,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             dbar[r] = 0.;
           }
           const double co = 0.5 * fw * lift;
-          const double cn = 0.5 * fw * (CV ? gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]
-                                           : so[C::oC + (end ^ 1)] / geo[(long)nb * kGeoStride + kGeoDetJ]);
+          const double cn = 0.5 * fw * lift_nb;
           double rob[5], rnb[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
@@ -754,28 +784,36 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
   double* sgr = sv + 15 * NQF;
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = geo[e * kGeoStride + i];
-  for (int i = tid; i < 5 * NB; i += blockDim.x) sU[i] = U[e * 5 * NB + i];
+  constexpr int NT = C::NT, NL = (5 * NB + NT - 1) / NT;  // the launch has NT threads
+  double ul[NL];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {  // all loads in flight together
+    const int i = tid + k * NT;
+    if (i < 5 * NB) ul[k] = U[e * 5 * NB + i];
+  }
   double Racc[5] = {0., 0., 0., 0., 0.};
   if (tid < NB) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) Racc[r] = Ubar_part[e * 5 * NB + r * NB + tid];
   }
+  for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += NT) sg[i] = geo[e * kGeoStride + i];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {
+    const int i = tid + k * NT;
+    if (i < 5 * NB) sU[i] = ul[k];
+  }
   __syncthreads();
   const double mu = prm.mu, kq = HT ? prm.kq : 0.;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
-    double S[5], g[3][5];
-    if constexpr (GS)
-      gface_value_grad<P>(half, sU, sN, so, S, g);
-    else
-      face_value_grad<P>(half, sU, sN, sY, so, S, g);
+    // this face point's trace adjoints (its own and the neighbour's side),
+    // loaded before the face values are formed
+    double vb[5], qb[5];
     if (tid < NH) {
       const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF;
       const int nb = nbr[e * 6 + lf];
       const double* TAo = TA + ((e * 6 + lf) * 20) * NQF;
-      double vb[5], qb[5];
 #pragma unroll
       for (int r = 0; r < 5; ++r) {
         vb[r] = TAo[r * NQF + fq];
@@ -789,6 +827,14 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
           qb[r] += TAn[(15 + r) * NQF + fq];
         }
       }
+    }
+    double S[5], g[3][5];
+    if constexpr (GS)
+      gface_value_grad<P>(half, sU, sN, so, S, g);
+    else
+      face_value_grad<P>(half, sU, sN, sY, so, S, g);
+    if (tid < NH) {
+      const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF;
       double gb[3][5];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -834,11 +880,14 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
       face_test_transpose<P>(half, sv, sgr, su, sc, so, Racc);
   }
   if (tid < NB) {
+    double ai[5];  // the running sum's entries, loaded before any store (acc_out may be acc_in)
+#pragma unroll
+    for (int r = 0; r < 5; ++r) ai[r] = v.acc_out && v.acc_in ? v.acc_in[e * 5 * NB + r * NB + tid] : 0.;
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       const long g = e * 5 * NB + r * NB + tid;
       if (v.a_out) v.a_out[g] = Racc[r];
-      if (v.acc_out) v.acc_out[g] = (v.acc_in ? v.acc_in[g] : 0.) + Racc[r];
+      if (v.acc_out) v.acc_out[g] = ai[r] + Racc[r];
     }
   }
 }

@@ -557,37 +557,61 @@ __device__ __forceinline__ int load_face_point(long e, int lf, int fq, const T* 
   return nb;
 }
 
+// The global operands of one entry's RK stage value: the step's base state
+// and either the RK4 accumulator (stages 2-4) or the stage input (TVD-RK3
+// stages 2-3), never both.  A kernel loads those of all its thread's entries
+// before it stores any result: the stores may alias the loads as far as the
+// compiler knows, so loads interleaved with stores would each wait a full
+// memory round trip.
+struct RkOperands {
+  double ub, x;
+};
+
+__device__ __forceinline__ RkOperands rk_stage_load(const StageArgs& sa, long i, const double* ue)
+{
+  RkOperands q;
+  q.ub = sa.Ubase[i];
+  if (sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
+    q.x = sa.acc ? sa.acc[i] : 0.;
+  else
+    q.x = sa.mode == MODE_TVD_1 || sa.mode == MODE_TVD_2 ? *ue : 0.;
+  return q;
+}
+
 // The RK stage value of one entry (time_distributed.cpp:46-102, stage 3 of
-// RK4 with dt as the reference's CPU solver): updates the accumulator and
-// returns the new stage state.  ue: the stage input state at this entry.
-__device__ __forceinline__ double rk_stage_value(const StageArgs& sa, long i, double fr, double ue)
+// RK4 with dt as the reference's CPU solver) from its loaded operands:
+// updates the accumulator and returns the new stage state.  The products
+// and sums are written as explicit fused multiply-adds, so every stage
+// kernel (FP64, mixed, paired, nodal) rounds the update the same way
+// whatever the compiler would contract on its own.
+__device__ __forceinline__ double rk_stage_apply(const StageArgs& sa, long i, double fr, const RkOperands& q)
 {
   const double dt = sa.dt;
   double un = 0.;
   switch (sa.mode) {
     case MODE_RK4_0:  // (a null accumulator: a stage state recomputed for a reverse step, which needs none)
       if (sa.acc) sa.acc[i] = fr;
-      un = sa.Ubase[i] + dt * fr * 0.5;
+      un = fma(dt * fr, 0.5, q.ub);
       break;
     case MODE_RK4_1:
-      if (sa.acc) sa.acc[i] = sa.acc[i] + 2. * fr;
-      un = sa.Ubase[i] + dt * fr * 0.5;
+      if (sa.acc) sa.acc[i] = fma(2., fr, q.x);
+      un = fma(dt * fr, 0.5, q.ub);
       break;
     case MODE_RK4_2:
-      if (sa.acc) sa.acc[i] = sa.acc[i] + 2. * fr;
-      un = sa.Ubase[i] + dt * fr;
+      if (sa.acc) sa.acc[i] = fma(2., fr, q.x);
+      un = fma(dt, fr, q.ub);
       break;
     case MODE_RK4_3:
-      un = sa.Ubase[i] + (1. / 6.) * (sa.acc[i] + fr) * dt;
+      un = fma((1. / 6.) * (q.x + fr), dt, q.ub);
       break;
     case MODE_TVD_0:
-      un = sa.Ubase[i] + dt * fr;
+      un = fma(dt, fr, q.ub);
       break;
     case MODE_TVD_1:
-      un = 0.75 * sa.Ubase[i] + 0.25 * ue + 0.25 * dt * fr;
+      un = fma(0.25 * dt, fr, fma(0.25, q.x, 0.75 * q.ub));
       break;
     case MODE_TVD_2:
-      un = (1. / 3.) * sa.Ubase[i] + (2. / 3.) * ue + (2. / 3.) * dt * fr;
+      un = fma((2. / 3.) * dt, fr, fma(2. / 3., q.x, (1. / 3.) * q.ub));
       break;
   }
   return un;
@@ -931,16 +955,21 @@ stage_kernel(long E, const double* Us, const T* __restrict__ Tr, const T* __rest
     }
     const double sc = CV ? -1.0 : -1.0 / detJd;
     const long base = e * 5 * NB;
+    if (sa.mode == MODE_RESIDUAL) {
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const long i = base + r * NB + tid;
-      const double fr = f[r] * sc;
-      if (sa.mode == MODE_RESIDUAL) {
-        sa.fout[i] = fr;
+      for (int r = 0; r < 5; ++r) {
+        const long i = base + r * NB + tid;
+        sa.fout[i] = f[r] * sc;
         if (sa.Rout) sa.Rout[i] = double(Rv[r]);
-      } else {
-        const double un = rk_stage_value(sa, i, fr, Ue[r * NB + tid]);
-        sa.Uout[i] = un;
+      }
+    } else {
+      RkOperands q[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) q[r] = rk_stage_load(sa, base + r * NB + tid, Ue + r * NB + tid);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const double un = rk_stage_apply(sa, base + r * NB + tid, f[r] * sc, q[r]);
+        sa.Uout[base + r * NB + tid] = un;
         sUn[r * NB + tid] = T(un);
       }
     }

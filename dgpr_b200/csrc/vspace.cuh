@@ -370,15 +370,17 @@ __device__ __forceinline__ void vstage_finish(long e, const StageArgs& sa, const
     const double jd = CV ? gve[kVolDetJ * NB + tid] : detJd;
     const double sc = -1.0 / (w[qx] * w[qy] * w[qz] * jd);
     const long base = e * 5 * NB;
+    if (sa.mode == MODE_RESIDUAL) {
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const long i = base + r * NB + tid;
-      const double fr = double(Rv[r]) * sc;
-      if (sa.mode == MODE_RESIDUAL) {
-        sa.fout[i] = fr;
-      } else {
-        const double un = rk_stage_value(sa, i, fr, Ve[r * NB + tid]);
-        sa.Uout[i] = un;
+      for (int r = 0; r < 5; ++r) sa.fout[base + r * NB + tid] = double(Rv[r]) * sc;
+    } else {
+      RkOperands q[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) q[r] = rk_stage_load(sa, base + r * NB + tid, Ve + r * NB + tid);
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const double un = rk_stage_apply(sa, base + r * NB + tid, double(Rv[r]) * sc, q[r]);
+        sa.Uout[base + r * NB + tid] = un;
         sVn[r * NB + tid] = T(un);
       }
     }
@@ -856,18 +858,26 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
     const double wq = w[qx] * w[qy] * w[qz];
     const double sc0 = -1.0 / (wq * geo[el[0] * kGeoStride + kGeoDetJ]);
     const double sc1 = -1.0 / (wq * geo[el[1] * kGeoStride + kGeoDetJ]);
+    const long b0 = el[0] * 5 * NB + tid, b1 = el[1] * 5 * NB + tid;
+    if (sa.mode == MODE_RESIDUAL) {
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const long i0 = el[0] * 5 * NB + r * NB + tid, i1 = el[1] * 5 * NB + r * NB + tid;
-      const double fr0 = double(Rv[r].lane(0)) * sc0, fr1 = double(Rv[r].lane(1)) * sc1;
-      if (sa.mode == MODE_RESIDUAL) {
-        sa.fout[i0] = fr0;
-        sa.fout[i1] = fr1;
-      } else {
-        const double un0 = rk_stage_value(sa, i0, fr0, Ve0[r * NB + tid]);
-        const double un1 = rk_stage_value(sa, i1, fr1, Ve1[r * NB + tid]);
-        sa.Uout[i0] = un0;
-        sa.Uout[i1] = un1;
+      for (int r = 0; r < 5; ++r) {
+        sa.fout[b0 + r * NB] = double(Rv[r].lane(0)) * sc0;
+        sa.fout[b1 + r * NB] = double(Rv[r].lane(1)) * sc1;
+      }
+    } else {
+      RkOperands q0[5], q1[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        q0[r] = rk_stage_load(sa, b0 + r * NB, Ve0 + r * NB + tid);
+        q1[r] = rk_stage_load(sa, b1 + r * NB, Ve1 + r * NB + tid);
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const double un0 = rk_stage_apply(sa, b0 + r * NB, double(Rv[r].lane(0)) * sc0, q0[r]);
+        const double un1 = rk_stage_apply(sa, b1 + r * NB, double(Rv[r].lane(1)) * sc1, q1[r]);
+        sa.Uout[b0 + r * NB] = un0;
+        sa.Uout[b1 + r * NB] = un1;
         sVn[r * NB + tid] = T((float)un0, (float)un1);
       }
     }

@@ -6,7 +6,7 @@
 // after the table is loaded, and the phases of an element are ordered by its
 // group's own synchronization.  The arithmetic is the
 // element-per-CTA kernel's own (vpoint_flux, load_face_point,
-// face_point_fluxes, vtrace_half, rk_stage_value in the same order), so the
+// face_point_fluxes, vtrace_half, rk_stage_apply in the same order), so the
 // state comes out bit for bit the same; only the per-element residual norm
 // partial is summed in another order.
 #pragma once
@@ -99,9 +99,20 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     if (sa.Ubase) prefetch_range(sa.Ubase + e * 5 * NB, 40L * NB, lt, GT);
     if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3) prefetch_range(sa.acc + e * 5 * NB, 40L * NB, lt, GT);
   }
-  for (int i = lt; i < kGeoStride; i += GT) sg[i] = T(geo[e * kGeoStride + i]);
   const double* Ve = Vs + e * 5 * NB;
-  for (int i = lt; i < 5 * NB; i += GT) V1[i] = T(Ve[i]);
+  constexpr int NVL = (5 * NB + GT - 1) / GT;  // state entries per thread, all loads in flight together
+  double vl[NVL];
+#pragma unroll
+  for (int k = 0; k < NVL; ++k) {
+    const int i = lt + k * GT;
+    vl[k] = i < 5 * NB ? Ve[i] : 0.;
+  }
+  for (int i = lt; i < kGeoStride; i += GT) sg[i] = T(geo[e * kGeoStride + i]);
+#pragma unroll
+  for (int k = 0; k < NVL; ++k) {
+    const int i = lt + k * GT;
+    if (i < 5 * NB) V1[i] = T(vl[k]);
+  }
   group_sync<GT>(bar);
 
   const T* Dq = so + C::oDq;
@@ -124,6 +135,37 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     vpoint_flux<P, T, CV, false>(so, V1, G, Ji, detJ, gve, gamma, mu, kq, o,
                                  [&](int i, int r, T v) { G[i * 5 * NB + r * NB + o] = v; });
   group_sync<GT>(bar);
+  // This thread's face point in each face pass (one at most: NH <= GT) and
+  // its loads: its traces and the neighbour's as load_face_point, the
+  // neighbour from shared memory.  (Issuing a pass's loads a phase ahead,
+  // during the volume divergence or the previous pass's test-function
+  // phases, measured 4-5% slower: the registers held across them spill.)
+  static_assert(NH <= GT, "one face point per thread and pass");
+  const bool fp = lt < NH;
+  const int fj = lt / NQF, fq0 = lt % NQF;
+  T Uo[5], Qo[5], Un[5], Qn[5], lift_n;
+  auto load_face = [&](int pass) {
+    const int lf = FPW * pass + fj, nb = sNb[lf];
+    const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      Uo[r] = To[r * NQF + fq0];
+      Qo[r] = To[(5 + r) * NQF + fq0];
+    }
+    lift_n = T(0);
+    if (nb >= 0) {
+      const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        Un[r] = Tn[r * NQF + fq0];
+        Qn[r] = Tn[(5 + r) * NQF + fq0];
+      }
+      if constexpr (CV)
+        lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq0]);
+      else
+        lift_n = so[C::oC + ((lf & 1) ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
+    }
+  };
   for (int o = lt; o < NB; o += GT) {  // Y = sum_i Dq_i^T Ghat_i minus the source tested with w detJ (over V)
     const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
     const T wJq = w[qx] * w[qy] * w[qz] * (CV ? T(gve[kVolDetJ * NB + o]) : detJ);
@@ -144,34 +186,11 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   T* Gt = Fb + FPW * 12 * NQF;  // [FPW][9][NQF]
 #pragma unroll 1
   for (int pass = 0; pass < 6 / FPW; ++pass) {
-#pragma unroll 1
-    for (int i = lt; i < NH; i += GT) {
-      const int j = i / NQF, lf = FPW * pass + j, fq = i % NQF;
-      T Uo[5], Qo[5], Un[5], Qn[5], lift_n;  // as load_face_point, the neighbour from shared memory
-      const int nb = sNb[lf];
-      {
-        const T* To = Tr + ((e * 6 + lf) * 10) * NQF;
-#pragma unroll
-        for (int r = 0; r < 5; ++r) {
-          Uo[r] = To[r * NQF + fq];
-          Qo[r] = To[(5 + r) * NQF + fq];
-        }
-        lift_n = T(0);
-        if (nb >= 0) {
-          const T* Tn = Tr + (((long)nb * 6 + (lf ^ 1)) * 10) * NQF;
-#pragma unroll
-          for (int r = 0; r < 5; ++r) {
-            Un[r] = Tn[r * NQF + fq];
-            Qn[r] = Tn[(5 + r) * NQF + fq];
-          }
-          if constexpr (CV)
-            lift_n = T(gf[(((long)nb * 6 + (lf ^ 1)) * kFaceC + kFaceLift) * NQF + fq]);
-          else
-            lift_n = so[C::oC + ((lf & 1) ^ 1)] / T(geo[(long)nb * kGeoStride + kGeoDetJ]);
-        }
-      }
-      face_point_fluxes<P, T, CV>(lf, fq, nb, Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ, Ji,
-                                  sa.flag, Fa + j * 5 * NQF + fq, Fb + j * 12 * NQF + fq);
+    if (fp) {
+      load_face(pass);
+      const int lf = FPW * pass + fj;
+      face_point_fluxes<P, T, CV>(lf, fq0, sNb[lf], Uo, Qo, Un, Qn, lift_n, so, sg, gfe, prm, gamma, mu, kq, detJ,
+                                  Ji, sa.flag, Fa + fj * 5 * NQF + fq0, Fb + fj * 12 * NQF + fq0);
     }
     group_sync<GT>(bar);
 #pragma unroll 1
@@ -242,22 +261,40 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 
   // ---------------- f_V = -Y / (w detJ) in FP64, RK update
   T* sVn = R;  // the new state for the epilogue traces
-  for (int o = lt; o < NB; o += GT) {
+  constexpr int NPT = (NB + GT - 1) / GT;  // Gauss points per thread
+  const long base = e * 5 * NB;
+  const double* wd = opsd + C::oW;
+  auto point_scale = [&](int o) {
     const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
-    const double* wd = opsd + C::oW;
     const double jd = CV ? gve[kVolDetJ * NB + o] : detJd;
-    const double sc = -1.0 / (wd[qx] * wd[qy] * wd[qz] * jd);
-    const long base = e * 5 * NB;
+    return -1.0 / (wd[qx] * wd[qy] * wd[qz] * jd);
+  };
+  if (sa.mode == MODE_RESIDUAL) {
+    for (int o = lt; o < NB; o += GT) {
+      const double sc = point_scale(o);
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const long i = base + r * NB + o;
-      const double fr = double(Y[r * NB + o]) * sc;
-      if (sa.mode == MODE_RESIDUAL) {
-        sa.fout[i] = fr;
-      } else {
-        const double un = rk_stage_value(sa, i, fr, Ve[r * NB + o]);
-        sa.Uout[i] = un;
-        sVn[r * NB + o] = T(un);
+      for (int r = 0; r < 5; ++r) sa.fout[base + r * NB + o] = double(Y[r * NB + o]) * sc;
+    }
+  } else {
+    RkOperands q[NPT][5];
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int o = lt + k * GT;
+      if (o < NB)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) q[k][r] = rk_stage_load(sa, base + r * NB + o, Ve + r * NB + o);
+    }
+#pragma unroll
+    for (int k = 0; k < NPT; ++k) {
+      const int o = lt + k * GT;
+      if (o < NB) {
+        const double sc = point_scale(o);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+          const double un = rk_stage_apply(sa, base + r * NB + o, double(Y[r * NB + o]) * sc, q[k][r]);
+          sa.Uout[base + r * NB + o] = un;
+          sVn[r * NB + o] = T(un);
+        }
       }
     }
   }
@@ -499,25 +536,35 @@ wstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
 
   // ---------------- f_V = -Y / (w detJ) in FP64, RK update, per element
   T* sVn = R;
+  const double* wd = opsd + C::oW;
+  const double dj0 = geo[el[0] * kGeoStride + kGeoDetJ], dj1 = geo[el[1] * kGeoStride + kGeoDetJ];
   for (int o = lt; o < NB; o += GT) {
     const int qx = o % P, qy = (o / P) % P, qz = o / (P * P);
-    const double* wd = opsd + C::oW;
     const double wq = wd[qx] * wd[qy] * wd[qz];
-    const double sc0 = -1.0 / (wq * geo[el[0] * kGeoStride + kGeoDetJ]);
-    const double sc1 = -1.0 / (wq * geo[el[1] * kGeoStride + kGeoDetJ]);
+    const double sc0 = -1.0 / (wq * dj0);
+    const double sc1 = -1.0 / (wq * dj1);
+    const long b0 = el[0] * 5 * NB + o, b1 = el[1] * 5 * NB + o;
+    if (sa.mode == MODE_RESIDUAL) {
 #pragma unroll
-    for (int r = 0; r < 5; ++r) {
-      const long i0 = el[0] * 5 * NB + r * NB + o, i1 = el[1] * 5 * NB + r * NB + o;
-      const T yv = Y[r * NB + o];
-      const double fr0 = double(yv.lane(0)) * sc0, fr1 = double(yv.lane(1)) * sc1;
-      if (sa.mode == MODE_RESIDUAL) {
-        sa.fout[i0] = fr0;
-        sa.fout[i1] = fr1;
-      } else {
-        const double un0 = rk_stage_value(sa, i0, fr0, Ve0[r * NB + o]);
-        const double un1 = rk_stage_value(sa, i1, fr1, Ve1[r * NB + o]);
-        sa.Uout[i0] = un0;
-        sa.Uout[i1] = un1;
+      for (int r = 0; r < 5; ++r) {
+        const T yv = Y[r * NB + o];
+        sa.fout[b0 + r * NB] = double(yv.lane(0)) * sc0;
+        sa.fout[b1 + r * NB] = double(yv.lane(1)) * sc1;
+      }
+    } else {
+      RkOperands q0[5], q1[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        q0[r] = rk_stage_load(sa, b0 + r * NB, Ve0 + r * NB + o);
+        q1[r] = rk_stage_load(sa, b1 + r * NB, Ve1 + r * NB + o);
+      }
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const T yv = Y[r * NB + o];
+        const double un0 = rk_stage_apply(sa, b0 + r * NB, double(yv.lane(0)) * sc0, q0[r]);
+        const double un1 = rk_stage_apply(sa, b1 + r * NB, double(yv.lane(1)) * sc1, q1[r]);
+        sa.Uout[b0 + r * NB] = un0;
+        sa.Uout[b1 + r * NB] = un1;
         sVn[r * NB + o] = T((float)un0, (float)un1);
       }
     }
