@@ -97,6 +97,22 @@ __device__ __forceinline__ void prefetch_range(const void* p, long bytes, int fi
   for (long o = (long)first * 128; o < bytes; o += (long)stride * 128) prefetch_l2(c + o);
 }
 
+// ------------------------------------------------------------ strided loads
+
+// Entries [0, N) of an FP64 array spread over NT threads (thread t takes
+// t, t + NT, ...), loaded into registers with all the loads in flight
+// together, for the caller to store afterwards: a loop that stores each
+// entry before it loads the next has the loads wait one after another.
+template <int N, int NT>
+__device__ __forceinline__ void load_spread(const double* __restrict__ src, int t, double (&v)[(N + NT - 1) / NT])
+{
+#pragma unroll
+  for (int k = 0; k < (N + NT - 1) / NT; ++k) {
+    const int i = t + k * NT;
+    v[k] = i < N ? src[i] : 0.;
+  }
+}
+
 // ------------------------------------------------------------ index helpers
 
 // node index from the coordinate along face axis a and the two tangential

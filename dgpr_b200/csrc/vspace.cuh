@@ -177,10 +177,14 @@ vtrace_kernel(long E, const double* __restrict__ V, const T* __restrict__ opsg, 
   T* sN = reinterpret_cast<T*>(smraw + L::oN);
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
-  const double* Ve = V + e * 5 * NB;
-  for (int i = tid; i < 5 * NB; i += blockDim.x) sV[i] = T(Ve[i]);
+  constexpr int NT = C::NTS, NL = (5 * NB + NT - 1) / NT;  // the launch has NTS threads
+  double vl[NL];
+  load_spread<5 * NB, NT>(V + e * 5 * NB, tid, vl);
+  for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += NT) sg[i] = T(geo[e * kGeoStride + i]);
+#pragma unroll
+  for (int k = 0; k < NL; ++k)
+    if (tid + k * NT < 5 * NB) sV[tid + k * NT] = T(vl[k]);
   __syncthreads();
   T* Te = Tr + e * 60 * NQF;
 #pragma unroll 1
@@ -435,10 +439,15 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3)
       prefetch_range(sa.acc + e * 5 * NB, 40L * NB, tid, nt);
   }
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = opsg[i];
-  for (int i = tid; i < kGeoStride; i += blockDim.x) sg[i] = T(geo[e * kGeoStride + i]);
   const double* Ve = Vs + e * 5 * NB;
-  for (int i = tid; i < 5 * NB; i += blockDim.x) V1[i] = T(Ve[i]);
+  constexpr int NT = C::NTS, NL = (5 * NB + NT - 1) / NT;  // the launch has NTS threads
+  double vl[NL];
+  load_spread<5 * NB, NT>(Ve, tid, vl);
+  for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
+  for (int i = tid; i < kGeoStride; i += NT) sg[i] = T(geo[e * kGeoStride + i]);
+#pragma unroll
+  for (int k = 0; k < NL; ++k)
+    if (tid + k * NT < 5 * NB) V1[tid + k * NT] = T(vl[k]);
   __syncthreads();
 
   const T* Dq = so + C::oDq;
@@ -500,8 +509,13 @@ __global__ void __launch_bounds__(Cfg<P>::NT) gauss_basis_kernel(long E, const d
   double* Bf = A + 5 * NB;
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
-  for (int i = tid; i < P * P; i += blockDim.x) M[i] = opsd[(INV ? C::oBi : C::oB) + i];
-  for (int i = tid; i < 5 * NB; i += blockDim.x) A[i] = in[e * 5 * NB + i];
+  constexpr int NT = C::NT, NL = (5 * NB + NT - 1) / NT;  // the launch has NT threads
+  double al[NL];
+  load_spread<5 * NB, NT>(in + e * 5 * NB, tid, al);
+  for (int i = tid; i < P * P; i += NT) M[i] = opsd[(INV ? C::oBi : C::oB) + i];
+#pragma unroll
+  for (int k = 0; k < NL; ++k)
+    if (tid + k * NT < 5 * NB) A[tid + k * NT] = al[k];
   __syncthreads();
   if (tid < NB) contract<P, 0, TR, false>(M, A, Bf, tid);
   __syncthreads();
@@ -579,10 +593,16 @@ vtrace2_kernel(long E, const double* __restrict__ V, const float* __restrict__ o
   f2* sN = reinterpret_cast<f2*>(smraw + L::oN);
   const long k = blockIdx.x, e0 = 2 * k, e1 = e0 + 1;
   const int tid = threadIdx.x;
-  for (int i = tid; i < C::OPS; i += blockDim.x) so[i] = f2(opsg[i]);
-  for (int i = tid; i < kGeoStride; i += blockDim.x)
+  constexpr int NT = C::NTS, NL = (5 * NB + NT - 1) / NT;  // the launch has NTS threads
+  double v0[NL], v1[NL];
+  load_spread<5 * NB, NT>(V + e0 * 5 * NB, tid, v0);
+  load_spread<5 * NB, NT>(V + e1 * 5 * NB, tid, v1);
+  for (int i = tid; i < C::OPS; i += NT) so[i] = f2(opsg[i]);
+  for (int i = tid; i < kGeoStride; i += NT)
     sg[i] = f2((float)geo[e0 * kGeoStride + i], (float)geo[e1 * kGeoStride + i]);
-  for (int i = tid; i < 5 * NB; i += blockDim.x) sV[i] = f2((float)V[e0 * 5 * NB + i], (float)V[e1 * 5 * NB + i]);
+#pragma unroll
+  for (int k = 0; k < NL; ++k)
+    if (tid + k * NT < 5 * NB) sV[tid + k * NT] = f2((float)v0[k], (float)v1[k]);
   __syncthreads();
   f2* Te = Tr2 + k * 60 * NQF;
 #pragma unroll 1
@@ -667,19 +687,25 @@ vstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
         prefetch_range(sa.acc + el[l] * 5 * NB, 40L * NB, tid, nt);
     }
   }
-  for (int i = tid; i < C::OPS; i += blockDim.x) {
+  const double* Ve0 = Vs + el[0] * 5 * NB;
+  const double* Ve1 = Vs + el[1] * 5 * NB;
+  constexpr int NT = C::NTS, NL = (5 * NB + NT - 1) / NT;  // the launch has NTS threads
+  double v0[NL], v1[NL];
+  load_spread<5 * NB, NT>(Ve0, tid, v0);
+  load_spread<5 * NB, NT>(Ve1, tid, v1);
+  for (int i = tid; i < C::OPS; i += NT) {
     so[i] = T(opsg[i]);
     sof[i] = opsg[i];
   }
-  for (int i = tid; i < kGeoStride; i += blockDim.x) {
+  for (int i = tid; i < kGeoStride; i += NT) {
     const float g0 = (float)geo[el[0] * kGeoStride + i], g1 = (float)geo[el[1] * kGeoStride + i];
     sg[i] = T(g0, g1);
     sgf[i] = g0;
     sgf[kGeoStride + i] = g1;
   }
-  const double* Ve0 = Vs + el[0] * 5 * NB;
-  const double* Ve1 = Vs + el[1] * 5 * NB;
-  for (int i = tid; i < 5 * NB; i += blockDim.x) V1[i] = T((float)Ve0[i], (float)Ve1[i]);
+#pragma unroll
+  for (int k = 0; k < NL; ++k)
+    if (tid + k * NT < 5 * NB) V1[tid + k * NT] = T((float)v0[k], (float)v1[k]);
   __syncthreads();
 
   const T* Dq = so + C::oDq;

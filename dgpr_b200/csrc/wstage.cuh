@@ -100,13 +100,9 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
     if (sa.acc && sa.mode >= MODE_RK4_1 && sa.mode <= MODE_RK4_3) prefetch_range(sa.acc + e * 5 * NB, 40L * NB, lt, GT);
   }
   const double* Ve = Vs + e * 5 * NB;
-  constexpr int NVL = (5 * NB + GT - 1) / GT;  // state entries per thread, all loads in flight together
+  constexpr int NVL = (5 * NB + GT - 1) / GT;  // state entries per thread
   double vl[NVL];
-#pragma unroll
-  for (int k = 0; k < NVL; ++k) {
-    const int i = lt + k * GT;
-    vl[k] = i < 5 * NB ? Ve[i] : 0.;
-  }
+  load_spread<5 * NB, GT>(Ve, lt, vl);
   for (int i = lt; i < kGeoStride; i += GT) sg[i] = T(geo[e * kGeoStride + i]);
 #pragma unroll
   for (int k = 0; k < NVL; ++k) {
