@@ -371,7 +371,8 @@ struct AdjASmem {
   static constexpr int NB = C::NB, NQF = C::NQF;
   static constexpr int oOps = 0;
   static constexpr int oGeo = (C::OPS + 1) & ~1;
-  static constexpr int oMu = oGeo + kGeoStride;  // mu [5][NB], alive through the face phase
+  static constexpr int oNb = oGeo + kGeoStride;   // the neighbours across the six faces (int)
+  static constexpr int oMu = oNb + 4;              // mu [5][NB], alive through the face phase
   static constexpr int oX = oMu + 5 * NB;          // scratch
   // volume: V0 V1 Sq [5NB each], G [15NB], N [15NB]
   static constexpr int VOL = 45 * NB;
@@ -410,6 +411,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
   double* Sq = sX + 10 * NB;
   double* G = sX + 15 * NB;
   double* N = sX + 30 * NB;
+  int* sNb = reinterpret_cast<int*>(sm + L::oNb);
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
   const bool node = tid < NB;
@@ -430,6 +432,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
         ul[k] = U[g];
       }
     }
+    if (tid < 6) sNb[tid] = nbr[e * 6 + tid];
     for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
     for (int i = tid; i < kGeoStride; i += NT) sg[i] = geo[e * kGeoStride + i];
 #pragma unroll
@@ -616,7 +619,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
     int nb = -1;
     double Uo[5], Un[5], lift_nb = 0.;
     if (tid < NH) {
-      nb = nbr[e * 6 + lf];
+      nb = sNb[lf];
       const double* To = Tr + ((e * 6 + lf) * 10) * NQF;
 #pragma unroll
       for (int r = 0; r < 5; ++r) Uo[r] = To[r * NQF + fq];
@@ -671,6 +674,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
       double* TAe = TA + ((e * 6 + lf) * 20) * NQF;
       if (nb >= 0) {
         double Unb[5] = {0., 0., 0., 0., 0.};
+        const double iro = 1. / Uo[0], irn = 1. / Un[0];  // once per side for all its VJPs
         {  // Roe flux.  The forward orients it (the high side is left) so that
            // both elements compute the same bits; as a function it is
            // f(Uo, Un, n_out) either way (antisymmetric under swapping the
@@ -679,7 +683,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
           double fb[5];
 #pragma unroll
           for (int r = 0; r < 5; ++r) fb[r] = fw * ab[r];
-          roe_flux_vjp(Uo, Un, n, gamma, fb, Uob, Unb);
+          roe_flux_vjp_r(Uo, Un, iro, irn, n, gamma, fb, Uob, Unb);
         }
 #pragma unroll
         for (int r = 0; r < 5; ++r) Qob[r] = -0.5 * fw * ab[r];
@@ -690,7 +694,7 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
           {
             double dcb[3][5];
             dual_bar(dcb);
-            visc_rank1_vjp(Uo, d, n, mu, dcb, Uob, dbar, kq);
+            visc_rank1_vjp_r(Uo, iro, d, n, mu, dcb, Uob, dbar, kq);
           }
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
@@ -707,8 +711,8 @@ adjA_kernel(long E, const double* __restrict__ U, const double* __restrict__ Tr,
             rob[r] = co * zb[r];
             rnb[r] = cn * zb[r];
           }
-          visc_jump_n_vjp(Uo, d, n, mu, rob, Uob, dbar, kq);
-          visc_jump_n_vjp(Un, d, n, mu, rnb, Unb, dbar, kq);
+          visc_jump_n_vjp_r(Uo, iro, d, n, mu, rob, Uob, dbar, kq);
+          visc_jump_n_vjp_r(Un, irn, d, n, mu, rnb, Unb, dbar, kq);
 #pragma unroll
           for (int r = 0; r < 5; ++r) {
             Uob[r] += dbar[r];
@@ -755,7 +759,8 @@ struct AdjBSmem {
   static constexpr int NB = C::NB, NQF = C::NQF;
   static constexpr int oOps = 0;
   static constexpr int oGeo = (C::OPS + 1) & ~1;
-  static constexpr int oU = oGeo + kGeoStride;
+  static constexpr int oNb = oGeo + kGeoStride;  // the neighbours across the six faces (int)
+  static constexpr int oU = oNb + 4;
   static constexpr int oX = oU + 5 * NB;
   // sN[3][10] sY[3][15] (then su[3][15] sc[3][10] in their place), sv[3][5], sgr[3][15]  (x NQF)
   static constexpr int TOTAL = oX + 75 * NQF + 60 * NQF;
@@ -782,6 +787,7 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
   double* sc = sX + 45 * NQF;
   double* sv = sX + 75 * NQF;
   double* sgr = sv + 15 * NQF;
+  int* sNb = reinterpret_cast<int*>(sm + L::oNb);
   const long e = blockIdx.x;
   const int tid = threadIdx.x;
   constexpr int NT = C::NT, NL = (5 * NB + NT - 1) / NT;  // the launch has NT threads
@@ -796,6 +802,7 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
 #pragma unroll
     for (int r = 0; r < 5; ++r) Racc[r] = Ubar_part[e * 5 * NB + r * NB + tid];
   }
+  if (tid < 6) sNb[tid] = nbr[e * 6 + tid];
   for (int i = tid; i < C::OPS; i += NT) so[i] = opsg[i];
   for (int i = tid; i < kGeoStride; i += NT) sg[i] = geo[e * kGeoStride + i];
 #pragma unroll
@@ -812,7 +819,7 @@ adjB_kernel(long E, const double* __restrict__ U, const double* __restrict__ TA,
     double vb[5], qb[5];
     if (tid < NH) {
       const int j = tid / NQF, lf = 3 * half + j, fq = tid % NQF;
-      const int nb = nbr[e * 6 + lf];
+      const int nb = sNb[lf];
       const double* TAo = TA + ((e * 6 + lf) * 20) * NQF;
 #pragma unroll
       for (int r = 0; r < 5; ++r) {

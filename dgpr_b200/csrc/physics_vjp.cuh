@@ -172,14 +172,15 @@ DGB_HD void rank1_tail_vjp(const T* S, const T* d, const T* v, T ir, const T* ab
   Sbar[0] += -irbar * ir * ir;
 }
 
-// Rank-one viscous flux Q = A(S, d n^T) (visc_rank1): Qbar[3][5] -> Sbar, dbar
+// Rank-one viscous flux Q = A(S, d n^T) (visc_rank1): Qbar[3][5] -> Sbar, dbar.
+// The _r forms take ir = 1 / S[0] from the caller, which divides once per
+// face state for all the VJPs that state enters.
 template <class T>
-DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qbar[3][5], T* Sbar, T* dbar,
-                           T kq = T(0))
+DGB_HD void visc_rank1_vjp_r(const T* S, T ir, const T* d, const T* n, T mu, const T Qbar[3][5], T* Sbar, T* dbar,
+                             T kq = T(0))
 {
   if (kq != T(0)) heat_y_vjp(S, d, kq * (Qbar[0][4] * n[0] + Qbar[1][4] * n[1] + Qbar[2][4] * n[2]), Sbar, dbar);
   const T lam = -(T(2) / T(3)) * mu;
-  const T ir = T(1) / S[0];
   const T v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
   T a[3];
 #pragma unroll
@@ -209,15 +210,21 @@ DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qba
   rank1_tail_vjp(S, d, v, ir, abar, vbar, T(0), Sbar, dbar);
 }
 
+template <class T>
+DGB_HD void visc_rank1_vjp(const T* S, const T* d, const T* n, T mu, const T Qbar[3][5], T* Sbar, T* dbar,
+                           T kq = T(0))
+{
+  visc_rank1_vjp_r(S, T(1) / S[0], d, n, mu, Qbar, Sbar, dbar, kq);
+}
+
 // Normal component A(S, d n^T).n (visc_jump_n): Qnbar[5] -> Sbar, dbar
 template <class T>
-DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Qnbar, T* Sbar, T* dbar,
-                            T kq = T(0))
+DGB_HD void visc_jump_n_vjp_r(const T* S, T ir, const T* d, const T* n, T mu, const T* Qnbar, T* Sbar, T* dbar,
+                              T kq = T(0))
 {
   if (kq != T(0))
     heat_y_vjp(S, d, kq * Qnbar[4] * (n[0] * n[0] + n[1] * n[1] + n[2] * n[2]), Sbar, dbar);
   const T lam = -(T(2) / T(3)) * mu;
-  const T ir = T(1) / S[0];
   const T v[3] = {S[1] * ir, S[2] * ir, S[3] * ir};
   T a[3];
 #pragma unroll
@@ -240,15 +247,21 @@ DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Q
   rank1_tail_vjp(S, d, v, ir, abar, vbar, T(0), Sbar, dbar);
 }
 
+template <class T>
+DGB_HD void visc_jump_n_vjp(const T* S, const T* d, const T* n, T mu, const T* Qnbar, T* Sbar, T* dbar,
+                            T kq = T(0))
+{
+  visc_jump_n_vjp_r(S, T(1) / S[0], d, n, mu, Qnbar, Sbar, dbar, kq);
+}
+
 // Normal Euler flux F(U).n of one side: Fnbar[5] -> Ubar (accumulated),
 // written out directly (no 3x5 intermediate).  With u = m / r, un = u.n,
 // q = |u|^2, p = (g - 1)(E - r q / 2), H = (E + p) / r:
-//   F = (r un, m un + p n, (E + p) un).
+//   F = (r un, m un + p n, (E + p) un).  ir = 1 / r from the caller.
 template <class T>
-DGB_HD void euler_normal_flux_vjp(const T* U, T g, const T* n, const T* fb, T* Ubar)
+DGB_HD void euler_normal_flux_vjp(const T* U, T ir, T g, const T* n, const T* fb, T* Ubar)
 {
   const T gm1 = g - T(1);
-  const T ir = T(1) / U[0];
   const T u[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
   const T un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
   const T q = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
@@ -269,23 +282,26 @@ DGB_HD void euler_normal_flux_vjp(const T* U, T g, const T* n, const T* fb, T* U
 // through the Roe average, and each side's share of the average is taken
 // from its own sqrt(rho), velocity and enthalpy.  Few values are live at a
 // time, which keeps the adjoint face kernel's registers down.
+// irl, irr: 1 / Ul[0], 1 / Ur[0] from the caller.  The reverse part divides
+// by nothing: 1 / (2 c) and 1 / (2 sqrt(r)) come from 1 / c and sqrt(r) / r.
 template <class T>
-DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fbar, T* Ulbar, T* Urbar)
+DGB_HD void roe_flux_vjp_r(const T* Ul, const T* Ur, T irl, T irr, const T* n, T g, const T* fbar, T* Ulbar,
+                           T* Urbar)
 {
   const T gm1 = g - T(1), h = T(0.5);
   {
     T hb[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) hb[k] = h * fbar[k];
-    euler_normal_flux_vjp(Ul, g, n, hb, Ulbar);
-    euler_normal_flux_vjp(Ur, g, n, hb, Urbar);
+    euler_normal_flux_vjp(Ul, irl, g, n, hb, Ulbar);
+    euler_normal_flux_vjp(Ur, irr, g, n, hb, Urbar);
   }
   // ---- forward of the dissipation
   T sq[2], us[2][3], Hs[2];
 #pragma unroll
   for (int s = 0; s < 2; ++s) {
     const T* U = s ? Ur : Ul;
-    const T ir = T(1) / U[0];
+    const T ir = s ? irr : irl;
 #pragma unroll
     for (int k = 0; k < 3; ++k) us[s][k] = U[1 + k] * ir;
     const T p = gm1 * (U[4] - T(0.5) * U[0] * (us[s][0] * us[s][0] + us[s][1] * us[s][1] + us[s][2] * us[s][2]));
@@ -373,7 +389,7 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   T cb = lb[0] - lb[1] + T(0.05) * epsb;
   // un = uk . n ; ic = 1/c ; c = sqrt(gm1 (H - q2/2)) ; q2 = |uk|^2
   cb += -icb * ic * ic;
-  const T c2b = cb / (T(2) * c);
+  const T c2b = cb * (h * ic);
   Hb += gm1 * c2b;
   q2b += -h * gm1 * c2b;
 #pragma unroll
@@ -395,7 +411,7 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
   for (int s = 0; s < 2; ++s) {
     const T* U = s ? Ur : Ul;
     T* Ub = s ? Urbar : Ulbar;
-    const T ir = T(1) / U[0], w = sq[s] * iden;
+    const T ir = s ? irr : irl, w = sq[s] * iden;
     T sqb = Hb * (Hs[s] - H), ub[3], qs = T(0), uub = T(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -408,8 +424,14 @@ DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fba
     Ub[4] += Hsb * g * ir;
 #pragma unroll
     for (int k = 0; k < 3; ++k) Ub[1 + k] += (ub[k] - Hsb * gm1 * us[s][k]) * ir;
-    Ub[0] += sqb * iden / (T(2) * sq[s]) + (-uub + Hsb * (gm1 * qs - g * U[4] * ir)) * ir;
+    Ub[0] += sqb * iden * (h * sq[s] * ir) + (-uub + Hsb * (gm1 * qs - g * U[4] * ir)) * ir;
   }
+}
+
+template <class T>
+DGB_HD void roe_flux_vjp(const T* Ul, const T* Ur, const T* n, T g, const T* fbar, T* Ulbar, T* Urbar)
+{
+  roe_flux_vjp_r(Ul, Ur, T(1) / Ul[0], T(1) / Ur[0], n, g, fbar, Ulbar, Urbar);
 }
 
 
