@@ -938,9 +938,9 @@ cudaError_t vlaunch_trace2_p(const KLaunch& L, const double* V, void* Tout, cuda
   return cudaGetLastError();
 }
 
-// The stages with a group of warps per element (one warp at p = 3, two at
-// p = 4) or per pair of elements (p = 4) (wstage.cuh, included at the end of
-// this header).
+// The stages with a group of warps per element or per pair of elements (one
+// warp at p = 3, two at p = 4) (wstage.cuh, included at the end of this
+// header).
 #ifndef DGB_WARP_STAGE
 #define DGB_WARP_STAGE 1
 #endif
@@ -964,7 +964,7 @@ template <int P, bool HT>
 cudaError_t vlaunch_stage2_p(const KLaunch& L, const double* Vs, const void* Tin, const StageArgs& sa,
                              cudaStream_t st)
 {
-  if constexpr (DGB_WARP_STAGE && P == 5) {  // (at p = 3 measured 1% slower than a CTA per pair)
+  if constexpr (DGB_WARP_STAGE && (P == 4 || P == 5)) {  // (a CTA per pair at other orders)
     const unsigned npair = (unsigned)((sa.ecount ? sa.ecount : L.E) / 2);
     wstage2_kernel<P, HT><<<(npair + kWarpElems - 1) / kWarpElems, WPairSmem<P>::GT * kWarpElems,
                             WPairSmem<P>::TOTAL, st>>>(

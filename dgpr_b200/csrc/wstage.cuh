@@ -310,8 +310,7 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 // The paired mixed stage (vstage2_kernel: two elements per thread in FP32x2)
 // with a group of warps per pair: a CTA holds two independent pairs, one per
 // group, sharing the operator tables.  Same arithmetic as vstage2_kernel.
-// Used at p = 4 (two warps a pair); at p = 3 one warp a pair measured 1%
-// slower than vstage2_kernel's CTA per pair.
+// Used at p = 3 (one warp a pair) and p = 4 (two warps a pair).
 template <int P>
 struct WPairSmem {
   using C = Cfg<P>;
@@ -380,15 +379,21 @@ wstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
         prefetch_range(sa.acc + el[l] * 5 * NB, 40L * NB, lt, GT);
     }
   }
+  const double* Ve0 = Vs + el[0] * 5 * NB;
+  const double* Ve1 = Vs + el[1] * 5 * NB;
+  constexpr int NVL = (5 * NB + GT - 1) / GT;  // state entries per thread and element
+  double v0[NVL], v1[NVL];
+  load_spread<5 * NB, GT>(Ve0, lt, v0);
+  load_spread<5 * NB, GT>(Ve1, lt, v1);
   for (int i = lt; i < kGeoStride; i += GT) {
     const float g0 = (float)geo[el[0] * kGeoStride + i], g1 = (float)geo[el[1] * kGeoStride + i];
     sg[i] = T(g0, g1);
     sgf[i] = g0;
     sgf[kGeoStride + i] = g1;
   }
-  const double* Ve0 = Vs + el[0] * 5 * NB;
-  const double* Ve1 = Vs + el[1] * 5 * NB;
-  for (int i = lt; i < 5 * NB; i += GT) V1[i] = T((float)Ve0[i], (float)Ve1[i]);
+#pragma unroll
+  for (int k = 0; k < NVL; ++k)
+    if (lt + k * GT < 5 * NB) V1[lt + k * GT] = T((float)v0[k], (float)v1[k]);
   group_sync<GT>(bar);
 
   const T* Dq = so + C::oDq;
