@@ -617,8 +617,8 @@ __device__ __forceinline__ double rk_stage_apply(const StageArgs& sa, long i, do
       if (sa.acc) sa.acc[i] = fma(2., fr, q.x);
       un = fma(dt, fr, q.ub);
       break;
-    case MODE_RK4_3:
-      un = fma((1. / 6.) * (q.x + fr), dt, q.ub);
+    case MODE_RK4_3:  // (an explicit add: fr is a product the compiler could otherwise fuse into it)
+      un = fma((1. / 6.) * __dadd_rn(q.x, fr), dt, q.ub);
       break;
     case MODE_TVD_0:
       un = fma(dt, fr, q.ub);

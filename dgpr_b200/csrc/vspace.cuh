@@ -103,17 +103,30 @@ struct VTraceSmem {
   static constexpr int TOTAL = oN + align16(10 * VF<P>::FN * C::NQF * ST);
 };
 
-// Traces of a Gauss-point state sV[5][NB] (shared memory) on the FN faces
-// lf = FN*half + j, into Te (this element's slice of the trace buffer), in
-// the trace format of trace_half.  Scratch sN[FN][10][NQF].  GT: the
-// element belongs to a group of GT threads of the CTA (32: a warp, ordered by
-// __syncwarp; more: named barrier gbar), 0: to the whole CTA.
-template <int P, class T, bool CV, int FN = VF<P>::FN, int GT = 0>
+// A Gauss-point tile in shared memory with its x-lines LS >= P entries
+// apart: point (x, y, z) of variable r at r * LS P^2 + x + LS (y + P z).
+// LS = P is the plain layout; LS = P + 1 at P = 4 spreads the lines over
+// the banks, so that the 16 face points of an x- or a y-face, read along
+// their normal lines by the lanes of a half-warp, fall in distinct banks
+// (plain, they are 32 or 128 bytes apart: 4-way conflicts).
+template <int P, int LS>
+__device__ __forceinline__ int tile_node(int a, int ia, int t1, int t2)
+{
+  return a == 0 ? ia + LS * (t1 + P * t2) : a == 1 ? t1 + LS * (ia + P * t2) : t1 + LS * (t2 + P * ia);
+}
+
+// Traces of a Gauss-point state sV[5][NB] (shared memory, x-lines LS apart)
+// on the FN faces lf = FN*half + j, into Te (this element's slice of the
+// trace buffer), in the trace format of trace_half.  Scratch
+// sN[FN][10][NQF].  GT: the element belongs to a group of GT threads of the
+// CTA (32: a warp, ordered by __syncwarp; more: named barrier gbar), 0: to
+// the whole CTA.
+template <int P, class T, bool CV, int FN = VF<P>::FN, int GT = 0, int LS = P>
 __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const T* so, const T* sg, T mu, T kq,
                                             T* __restrict__ Te, const double* __restrict__ gfe, int gbar = 0)
 {
   using C = Cfg<P>;
-  constexpr int NB = C::NB, NQF = C::NQF, NH = FN * NQF;
+  constexpr int NB = LS * P * P, NQF = C::NQF, NH = FN * NQF;  // NB: the tile's variable stride
   const int tid = GT ? (int)(threadIdx.x % GT) : (int)threadIdx.x;
   const int nt = GT ? GT : (int)blockDim.x;
 #pragma unroll 1
@@ -128,7 +141,7 @@ __device__ __forceinline__ void vtrace_half(int half, const T* sV, T* sN, const 
       T v = T(0), dn = T(0);
 #pragma unroll
       for (int qa = 0; qa < P; ++qa) {
-        const T u = sV[r * NB + face_node<P>(a, qa, t1, t2)];
+        const T u = sV[r * NB + tile_node<P, LS>(a, qa, t1, t2)];
         v = fma(Ev[qa], u, v);
         dn = fma(Dv[qa], u, dn);
       }

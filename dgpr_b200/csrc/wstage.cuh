@@ -29,12 +29,13 @@ struct WStageSmem {
   static constexpr int eR = eY + align16(5 * NB * ST);
   // R: gradients, then contravariant fluxes G[3][5][NB]; the face buffers
   // Fa[FPW][5][NQF] Fb[FPW][12][NQF] Gt[FPW][9][NQF]; the norm's two nodal
-  // buffers [2][5][NB]; the new state [5][NB] and the trace scratch
-  // [FPW][10][NQF]
+  // buffers [2][5][NB]; the new state [5][LS P^2] (x-lines LS apart,
+  // tile_node) and the trace scratch [FPW][10][NQF]
+  static constexpr int LS = P == 4 ? P + 1 : P;
   static constexpr int RG = 15 * NB * ST;
   static constexpr int RF = FPW * 26 * NQF * ST;
   static constexpr int RN = 10 * NB * ST;
-  static constexpr int RT = 5 * NB * ST + FPW * 10 * NQF * ST;
+  static constexpr int RT = 5 * LS * P * P * ST + FPW * 10 * NQF * ST;
   static constexpr int RMAX = RG > RF ? (RG > RN ? (RG > RT ? RG : RT) : (RN > RT ? RN : RT))
                                       : (RF > RN ? (RF > RT ? RF : RT) : (RN > RT ? RN : RT));
   static constexpr int eRed = eR + align16(RMAX);  // per-warp sums of the norm partial
@@ -257,6 +258,7 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 
   // ---------------- f_V = -Y / (w detJ) in FP64, RK update
   T* sVn = R;  // the new state for the epilogue traces
+  constexpr int LS = L::LS;
   constexpr int NPT = (NB + GT - 1) / GT;  // Gauss points per thread
   const long base = e * 5 * NB;
   const double* wd = opsd + C::oW;
@@ -285,11 +287,12 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
       const int o = lt + k * GT;
       if (o < NB) {
         const double sc = point_scale(o);
+        const int on = o + (LS - P) * (o / P);  // o in the tile with x-lines LS apart
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
           const double un = rk_stage_apply(sa, base + r * NB + o, double(Y[r * NB + o]) * sc, q[k][r]);
           sa.Uout[base + r * NB + o] = un;
-          sVn[r * NB + o] = T(un);
+          sVn[r * LS * P * P + on] = T(un);
         }
       }
     }
@@ -298,11 +301,11 @@ wstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
   if (sa.Tnext) {
     group_sync<GT>(bar);
     T* Te = reinterpret_cast<T*>(sa.Tnext) + e * 60 * NQF;
-    T* sN = R + 5 * NB;
+    T* sN = R + 5 * LS * P * P;
 #pragma unroll 1
     for (int pass = 0; pass < 6 / FPW; ++pass) {
       if (pass) group_sync<GT>(bar);
-      vtrace_half<P, T, CV, FPW, GT>(pass, sVn, sN, so, sg, mu, kq, Te, gfe, bar);
+      vtrace_half<P, T, CV, FPW, GT, LS>(pass, sVn, sN, so, sg, mu, kq, Te, gfe, bar);
     }
   }
 }
@@ -327,7 +330,8 @@ struct WPairSmem {
   static constexpr int RG = 15 * NB * 8;
   static constexpr int RF = FPW * 26 * NQF * 8;
   static constexpr int RN = 10 * NB * 8;
-  static constexpr int RT = 5 * NB * 8 + FPW * 10 * NQF * 8;
+  static constexpr int LS = P == 4 ? P + 1 : P;  // x-line stride of the new state's tile (tile_node)
+  static constexpr int RT = 5 * LS * P * P * 8 + FPW * 10 * NQF * 8;
   static constexpr int RMAX = RG > RF ? (RG > RN ? (RG > RT ? RG : RT) : (RN > RT ? RN : RT))
                                       : (RF > RN ? (RF > RT ? RF : RT) : (RN > RT ? RN : RT));
   static constexpr int eRed = eR + align16(RMAX);  // per-warp sums of the norm partials
@@ -566,18 +570,18 @@ wstage2_kernel(long E, const double* Vs, const f2* __restrict__ Tr2, const float
         const double un1 = rk_stage_apply(sa, b1 + r * NB, double(yv.lane(1)) * sc1, q1[r]);
         sa.Uout[b0 + r * NB] = un0;
         sa.Uout[b1 + r * NB] = un1;
-        sVn[r * NB + o] = T((float)un0, (float)un1);
+        sVn[r * L::LS * P * P + o + (L::LS - P) * (o / P)] = T((float)un0, (float)un1);
       }
     }
   }
   if (sa.Tnext) {
     group_sync<GT>(bar);
     T* Te = reinterpret_cast<T*>(sa.Tnext) + k * 60 * NQF;
-    T* sN = R + 5 * NB;
+    T* sN = R + 5 * L::LS * P * P;
 #pragma unroll 1
     for (int pass = 0; pass < 6 / FPW; ++pass) {
       if (pass) group_sync<GT>(bar);
-      vtrace_half<P, T, false, FPW, GT>(pass, sVn, sN, so, sg, mu, kq, Te, nullptr, bar);
+      vtrace_half<P, T, false, FPW, GT, L::LS>(pass, sVn, sN, so, sg, mu, kq, Te, nullptr, bar);
     }
   }
 }
