@@ -240,11 +240,16 @@ __device__ __forceinline__ void gface_value_grad(int half, const double* sVx, do
     const double* Ev = so + C::oEh + end * P;
     const double* Dv = so + C::oDh + end * P;
     double* out = sN + j * 10 * NQF;
+    // each face point walks its normal line from a different start, so the
+    // 16 face points a half-warp reads at once fall in distinct banks (in
+    // order along an x- or y-line they are 32 or 128 bytes apart)
+    const int q0 = t1 + t2;
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
       double v = 0., dn = 0.;
 #pragma unroll
-      for (int qa = 0; qa < P; ++qa) {
+      for (int k = 0; k < P; ++k) {
+        const int qa = (q0 + k) % P;
         const double u = sVx[r * NB + face_node<P>(a, qa, t1, t2)];
         v = fma(Ev[qa], u, v);
         dn = fma(Dv[qa], u, dn);
