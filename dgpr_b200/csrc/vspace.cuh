@@ -428,7 +428,7 @@ vstage_kernel(long E, const double* Vs, const T* __restrict__ Tr, const T* __res
 {
   using C = Cfg<P>;
   using L = VStageSmem<P, T>;
-  constexpr int NB = C::NB, NQF = C::NQF, FPP = VF<P>::FN, NH = FPP * NQF;
+  constexpr int NB = C::NB, NQF = C::NQF;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* so = reinterpret_cast<T*>(smraw + L::oOps);
   T* sg = reinterpret_cast<T*>(smraw + L::oGeo);
