@@ -341,6 +341,7 @@ def _adjoint_config(dg, torch, nsteps, budgets):
         s.forward_record(dg.RK4, dt, 2, 2, norms=False)
         s.backward(np.zeros(U0.numel()))
         grad = None
+        reps = 3  # host wall clock on a small mesh: the median of three runs
         for slots in budgets:
             # untimed recorded run first: allocates (or frees) the checkpoint buffers
             s.set_state(U0.cpu().numpy())
@@ -348,31 +349,40 @@ def _adjoint_config(dg, torch, nsteps, budgets):
                 s.forward_record_stages(dg.RK4, dt, nsteps, norms=False)
             else:
                 s.forward_record(dg.RK4, dt, nsteps, slots, norms=False)
-            a = a0.clone().requires_grad_(True)
-            Ua = modes.state(a)
+            tf, tb, same = [], [], True
+            for _ in range(reps):
+                a = a0.clone().requires_grad_(True)
+                Ua = modes.state(a)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                UN = dga.integrate(Ua, s, dg.RK4, dt, nsteps, slots=slots)
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                J = F.enstrophy(UN, quad)
+                J.backward()
+                torch.cuda.synchronize()
+                t2 = time.perf_counter()
+                tf.append(t1 - t0)
+                tb.append(t2 - t1)
+                fwd, rev, planned = s.adjoint_stats()
+                g = a.grad.cpu().numpy()
+                if grad is None:
+                    grad = g
+                same = same and bool(np.array_equal(g, grad))
+            out["budgets"].append({"slots": "every state and stage state" if slots == dga.STAGES else slots,
+                                   "recorded_forward_s": float(np.median(tf)), "backward_s": float(np.median(tb)),
+                                   "runs": reps, "recomputed_steps": fwd, "reversed_steps": rev,
+                                   "gradient_equal_to_first_budget": same})
+        # plain forward time of the same run (no recording), median of three
+        tp = []
+        for _ in range(reps):
+            s.set_state(U0.cpu().numpy())
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            UN = dga.integrate(Ua, s, dg.RK4, dt, nsteps, slots=slots)
+            s.step(dg.RK4, dt, nsteps, norms=False)
             torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            J = F.enstrophy(UN, quad)
-            J.backward()
-            torch.cuda.synchronize()
-            t2 = time.perf_counter()
-            fwd, rev, planned = s.adjoint_stats()
-            g = a.grad.cpu().numpy()
-            if grad is None:
-                grad = g
-            out["budgets"].append({"slots": "every state and stage state" if slots == dga.STAGES else slots,
-                                   "recorded_forward_s": t1 - t0, "backward_s": t2 - t1,
-                                   "recomputed_steps": fwd, "reversed_steps": rev,
-                                   "gradient_equal_to_first_budget": bool(np.array_equal(g, grad))})
-        # plain forward time of the same run (no recording)
-        s.set_state(U0.cpu().numpy())
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s.step(dg.RK4, dt, nsteps, norms=False)
-        out["plain_forward_s"] = time.perf_counter() - t0
+            tp.append(time.perf_counter() - t0)
+        out["plain_forward_s"] = float(np.median(tp))
         for b in out["budgets"]:
             b["backward_over_plain_forward"] = b["backward_s"] / out["plain_forward_s"]
         rng = np.random.default_rng(1)
